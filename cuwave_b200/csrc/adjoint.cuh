@@ -1,0 +1,350 @@
+// The transposed step and the gradient densities, marched along axis 0 like the step.
+//
+// MODE_STEP       lambda^n = 2 lambda^(n+1) - lambda^(n+2) + dt^2/m (W^-1 A^T W lambda^(n+1)),
+//                 the pml transpose gathered in: adjoint_kernel + pml_adjoint_kernel
+//                 (cuwave/kernels/scalar_sensitivity.cu:388-441, 545-597).
+// MODE_STEP_GRAD  the same, accumulating g_mass and g_stiff against u^n:
+//                 adjoint_gradient_kernel (scalar_sensitivity.cu:444-515).
+// MODE_GRAD       both densities of a forward triplet against lambda:
+//                 gradient_kernel (scalar_sensitivity.cu:303-350).
+//
+// The adjoint reads lambda, u and k through the node image, never a stored ghost,
+// lambda and u odd across a Dirichlet face and zero on its wall node
+// (`reflected`, scalar_sensitivity.cu:177-184); the queues and tiles hold the image
+// values and a tap landing on a held wall node is zeroed where it is read. The
+// transposed divergence is transposed_divergence_taps (scalar_sensitivity.cu:140-154)
+// and the stiffness density stiffness_gradient_taps (scalar_sensitivity.cu:119-135),
+// in their order of operations.
+#pragma once
+
+#include <type_traits>
+
+#include "params.cuh"
+
+namespace cwb {
+
+template <int NDIM, int R, int BX, int BY>
+struct AdjShape {
+  static constexpr int HY = NDIM == 3 ? R : 0;
+  static constexpr int TW = BX + 2 * R;
+  static constexpr int TH = BY + 2 * HY;
+  static constexpr int PLANE = TW * TH;
+};
+
+// fields an adjoint mode reads with taps: lambda always, u with gradients, k unless
+// uniform
+template <int MODE, bool UNIF>
+struct AdjFields {
+  static constexpr bool U = MODE != MODE_STEP;
+  static constexpr bool K = !UNIF;
+  static constexpr int COUNT = 1 + (U ? 1 : 0) + (K ? 1 : 0);
+};
+
+template <typename T, int NDIM, int R, bool UNIF, int MODE, int BX, int BY>
+__global__ void __launch_bounds__(BX *BY) adjoint_kernel(const AdjointParams<T> p) {
+  using S = AdjShape<NDIM, R, BX, BY>;
+  using FL = AdjFields<MODE, UNIF>;
+  constexpr int HY = S::HY, TW = S::TW, F = NDIM - 1;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T *tiles = reinterpret_cast<T *>(smem_raw);
+
+  const Geometry &g = p.g;
+  const int t = step_index(p.ctr);
+  // MODE_STEP*: l0 = lambda^(n+2) -> lambda^n, l1 = lambda^(n+1), u1 = u^n
+  // MODE_GRAD:  u0, u1, u2 the forward triplet, l1 = lambda
+  T *l0 = MODE == MODE_GRAD ? nullptr : level<T>(p.l0, t);
+  const T *__restrict__ l1 = level<T>(p.l1, t);
+  const T *__restrict__ u1 = FL::U ? level<T>(p.u1, t) : nullptr;
+  const T *__restrict__ u0 = MODE == MODE_GRAD ? level<T>(p.u0, t) : nullptr;
+  const T *__restrict__ u2 = MODE == MODE_GRAD ? level<T>(p.u2, t) : nullptr;
+  const T *__restrict__ stiff = p.stiff;
+
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int x0 = blockIdx.x * BX;
+  const int y0 = NDIM == 3 ? blockIdx.y * BY : 0;
+  const int cz = NDIM == 3 ? blockIdx.z : blockIdx.y;
+  const int N0 = g.n[0], NF = g.n[F], NM = NDIM == 3 ? g.n[1] : 1;
+  const int s0 = g.s[0], sM = NDIM == 3 ? g.s[1] : 0;
+  const int px = x0 + tx, py = y0 + ty;
+  const int c0 = 1 + cz * p.chunk;
+  const int c1 = min(N0 - 1, c0 + p.chunk);
+  // only an interior column keeps queues: a ghost column's cell holds its image
+  const bool inner = px >= 1 && px <= NF - 2 && (NDIM == 2 || (py >= 1 && py <= NM - 2));
+  const bool own = inner;
+  const int col = (NDIM == 3 ? py * sM : 0) + px;
+  const int dir0 = g.dir & 3;
+  const int dirM = NDIM == 3 ? (g.dir >> 2) & 3 : 0;
+  const int dirF = (g.dir >> (2 * F)) & 3;
+  const int flags = p.flags;
+
+  // field at row b of this column through the node image along axis 0
+  const auto row_val = [&](const T *f, const int b, const bool odd) -> T {
+    int sg;
+    const int m = node_image(b, N0, odd ? dir0 : 0, sg);
+    const T v = f[m * s0 + col];
+    return sg < 0 ? -v : v;
+  };
+  // field at in-plane node (bm, bf) of plane a0 through its images; out of reach zero
+  const auto plane_val = [&](const T *f, const int a0, const int bm, const int bf,
+                             const bool odd) -> T {
+    int sf, sm = 1, mm = 0;
+    const int mf = node_image(bf, NF, odd ? dirF : 0, sf);
+    if (NDIM == 3)
+      mm = node_image(bm, NM, odd ? dirM : 0, sm);
+    if (mf < 0 || mf > NF - 1 || mm < 0 || mm > NM - 1)
+      return (T)0;
+    const T v = f[a0 * s0 + mm * sM + mf];
+    return sf * sm < 0 ? -v : v;
+  };
+
+  // queues along axis 0: lambda, u, k on rows a0 - R .. a0 + R
+  T ql[2 * R + 1], qu[2 * R + 1], qk[2 * R + 1];
+  if (own && c0 < c1) {
+#pragma unroll
+    for (int k = 0; k < 2 * R; ++k) {
+      ql[k] = row_val(l1, c0 - R + k, true);
+      if constexpr (FL::U)
+        qu[k] = row_val(u1, c0 - R + k, true);
+      if constexpr (FL::K)
+        qk[k] = row_val(stiff, c0 - R + k, false);
+    }
+  }
+
+  for (int a0 = c0; a0 < c1; ++a0) {
+    T *tL = tiles + ((a0 - c0) & 1) * FL::COUNT * S::PLANE;
+    T *tU = tL + S::PLANE;
+    T *tK = tL + (FL::U ? 2 : 1) * S::PLANE;
+    if (own) {
+      ql[2 * R] = row_val(l1, a0 + R, true);
+      if constexpr (FL::U)
+        qu[2 * R] = row_val(u1, a0 + R, true);
+      if constexpr (FL::K)
+        qk[2 * R] = row_val(stiff, a0 + R, false);
+    }
+    const int cc = (ty + HY) * TW + tx + R;
+    tL[cc] = own ? ql[R] : plane_val(l1, a0, py, px, true);
+    if constexpr (FL::U)
+      tU[cc] = own ? qu[R] : plane_val(u1, a0, py, px, true);
+    if constexpr (FL::K)
+      tK[cc] = own ? qk[R] : plane_val(stiff, a0, py, px, false);
+    for (int e = tx; e < R; e += BX) {
+      const int cl = (ty + HY) * TW + e, cr = (ty + HY) * TW + BX + R + e;
+      tL[cl] = plane_val(l1, a0, py, x0 - R + e, true);
+      tL[cr] = plane_val(l1, a0, py, x0 + BX + e, true);
+      if constexpr (FL::U) {
+        tU[cl] = plane_val(u1, a0, py, x0 - R + e, true);
+        tU[cr] = plane_val(u1, a0, py, x0 + BX + e, true);
+      }
+      if constexpr (FL::K) {
+        tK[cl] = plane_val(stiff, a0, py, x0 - R + e, false);
+        tK[cr] = plane_val(stiff, a0, py, x0 + BX + e, false);
+      }
+    }
+    if (NDIM == 3) {
+      for (int e = ty; e < R; e += BY) {
+        const int ct = e * TW + tx + R, cb = (BY + HY + e) * TW + tx + R;
+        tL[ct] = plane_val(l1, a0, y0 - R + e, px, true);
+        tL[cb] = plane_val(l1, a0, y0 + BY + e, px, true);
+        if constexpr (FL::U) {
+          tU[ct] = plane_val(u1, a0, y0 - R + e, px, true);
+          tU[cb] = plane_val(u1, a0, y0 + BY + e, px, true);
+        }
+        if constexpr (FL::K) {
+          tK[ct] = plane_val(stiff, a0, y0 - R + e, px, false);
+          tK[cb] = plane_val(stiff, a0, y0 + BY + e, px, false);
+        }
+      }
+    }
+    __syncthreads();
+
+    if (inner) {
+      const int idx = a0 * s0 + col;
+      const int A[3] = {a0, NDIM == 3 ? py : px, px};
+      const int dirs[3] = {dir0, NDIM == 3 ? dirM : dirF, dirF};
+      const bool held = held_wall(a0, N0, dir0) || (NDIM == 3 && held_wall(py, NM, dirM)) ||
+                        held_wall(px, NF, dirF);
+      // whether a tap of this node can land on a held wall node
+      bool near = false;
+#pragma unroll
+      for (int d = 0; d < NDIM; ++d)
+        near |= ((dirs[d] & 1) && A[d] <= R + 1) || ((dirs[d] & 2) && A[d] >= g.n[d] - 2 - R);
+      const T sc = UNIF ? p.sconst : qk[R];
+      const T uc = FL::U ? qu[R] : (T)0;
+      const T lc = ql[R];
+      const T lw = held ? (T)0 : lc;
+
+      const auto body = [&](auto check) {
+        constexpr bool CHK = decltype(check)::value;
+        // the taps of axis d; lambda and u read zero on a held wall node
+        const auto tapL = [&](const int d, const int j) -> T {
+          T v = d == 0 ? ql[R + j] : (d == F ? tL[cc + j] : tL[cc + j * TW]);
+          if (CHK) {
+            const int b = A[d] + j;
+            if (((dirs[d] & 1) && b == 1) || ((dirs[d] & 2) && b == g.n[d] - 2))
+              v = (T)0;
+          }
+          return v;
+        };
+        const auto tapU = [&](const int d, const int j) -> T {
+          T v = d == 0 ? qu[R + j] : (d == F ? tU[cc + j] : tU[cc + j * TW]);
+          if (CHK) {
+            const int b = A[d] + j;
+            if (((dirs[d] & 1) && b == 1) || ((dirs[d] & 2) && b == g.n[d] - 2))
+              v = (T)0;
+          }
+          return v;
+        };
+        const auto tapK = [&](const int d, const int j) -> T {
+          if (UNIF)
+            return p.sconst;
+          return d == 0 ? qk[R + j] : (d == F ? tK[cc + j] : tK[cc + j * TW]);
+        };
+        // the stiffness density of one axis, its outer minus left to the caller
+        const auto stiff_density = [&](const int d) -> T {
+          T dgp, dgm;
+          if (UNIF) {
+            dgp = p.dgconst;
+            dgm = p.dgconst;
+          } else {
+            const T sp = tapK(d, 1), sm = tapK(d, -1);
+            dgp = sp * sp / ((sc + sp) * (sc + sp));
+            dgm = sm * sm / ((sc + sm) * (sc + sm));
+          }
+          T Dp = p.w[0] * (tapU(d, 1) - uc);
+          T Dm = p.w[0] * (uc - tapU(d, -1));
+#pragma unroll
+          for (int j = 2; j <= R; ++j) {
+            Dp += p.w[j - 1] * (tapU(d, j) - tapU(d, 1 - j));
+            Dm += p.w[j - 1] * (tapU(d, j - 1) - tapU(d, -j));
+          }
+          return p.f[d] * (dgp * Dp * (tapL(d, 1) - lw) + dgm * Dm * (lw - tapL(d, -1)));
+        };
+
+        if constexpr (MODE == MODE_GRAD) {
+          // dJ/dmass of the triplet, then dJ/dstiff (gradient_kernel)
+          p.g_mass[idx] -= p.mf * lc * (u2[idx] - (T)2 * uc + u0[idx]);
+          T gs = (T)0;
+#pragma unroll
+          for (int d = 0; d < NDIM; ++d)
+            gs += stiff_density(d);
+          p.g_stiff[idx] -= gs;
+        } else {
+          const T lo = l0[idx];
+          const T mi = (flags & K_DERIVE) ? (T)1 / sc : p.minv[idx];
+          T div_l = (T)0, gs = (T)0;
+#pragma unroll
+          for (int d = 0; d < NDIM; ++d) {
+            T div = (T)0, sh = sc, sl = sc, lh = lc, ll = lc;
+#pragma unroll
+            for (int j = 1; j <= R; ++j) {
+              const T sh1 = tapK(d, j), sl1 = tapK(d, -j);
+              const T lh1 = tapL(d, j), ll1 = tapL(d, -j);
+              T ghi, glo;
+              if (UNIF) {
+                ghi = p.gconst;
+                glo = p.gconst;
+              } else {
+                ghi = sh * sh1 / (sh + sh1);
+                glo = sl * sl1 / (sl + sl1);
+              }
+              div += p.w[j - 1] * (ghi * (lh1 - lh) - glo * (ll - ll1));
+              sh = sh1;
+              sl = sl1;
+              lh = lh1;
+              ll = ll1;
+            }
+            div_l += p.f[d] * div;
+            if constexpr (MODE == MODE_STEP_GRAD)
+              gs += stiff_density(d);
+          }
+          T ln;
+          if (flags & K_DAMP) {
+            const T beta = (T)0.5 * mi * p.damping[idx] * p.dt;
+            ln = ((T)2 * lc - lo * ((T)1 - beta) + mi * div_l) / ((T)1 + beta);
+          } else {
+            ln = -lo + (T)2 * lc + mi * div_l;
+          }
+          if (held)
+            ln = (T)0;
+          T gmass = (T)0, gstiff = (T)0;
+          if constexpr (MODE == MODE_STEP_GRAD) {
+            gmass = p.g_mass[idx] - p.mf * uc * (ln - (T)2 * lc + lo);
+            gstiff = p.g_stiff[idx] - p.mf * gs;
+          }
+
+          if (flags & K_PML) {
+            const T wcell = cell_weight<T>(g, A);
+#pragma unroll 1
+            for (int d = 0; d < NDIM; ++d) {
+              const int lo_d = g.lo[d], hi_d = g.hi[d];
+              if (!(lo_d + hi_d))
+                continue;
+              const int a = A[d], N = g.n[d];
+              const bool reached = (lo_d && a >= 1 && a <= lo_d + R) ||
+                                   (hi_d && a <= N - 2 && a >= N - 1 - (hi_d + R));
+              if (!reached)
+                continue;
+              const T *mem = p.mem[d];
+              const int sz = p.memrow[d];
+              int B[3] = {A[0], A[1], A[2]};
+              // what the memories of layer row ai give the node q rows off it
+              // (pml_tap, scalar_sensitivity.cu:237-251, its c+ and c- precomputed)
+              const auto tap = [&](const int ai, const int q) -> T {
+                const int r = slab_row(ai, N, lo_d, hi_d);
+                B[d] = ai;
+                const int i = slab_index(g, d, r, B);
+                return mem[3 * sz + i] * plus_tap<T, R>(p.w, q) +
+                       mem[4 * sz + i] * minus_tap<T, R>(p.w, q);
+              };
+              T sum = (T)0;
+#pragma unroll 1
+              for (int m = -R; m <= R; ++m)
+                if (slab_row(a + m, N, lo_d, hi_d) >= 0)
+                  sum += tap(a + m, -m);
+#pragma unroll 1
+              for (int high = 0; high < 2; ++high) {
+                // the reads past the wall that land on a, folded back, odd on a
+                // Dirichlet face
+                const int ghost = high ? 2 * (N - 2) - a : 2 - a;
+                if (high ? ghost < N - 1 : ghost > 0)
+                  continue;
+                T fold = (T)0;
+#pragma unroll 1
+                for (int k = 1; k <= R; ++k) {
+                  const int ai = high ? N - 1 - k : k;
+                  if (slab_row(ai, N, lo_d, hi_d) >= 0 && ghost - ai >= -R && ghost - ai <= R)
+                    fold += tap(ai, ghost - ai);
+                }
+                sum += ((g.dir >> (2 * d + high)) & 1) ? -fold : fold;
+              }
+              const T delta = mi * sum / wcell;
+              ln += delta;
+              if constexpr (MODE == MODE_STEP_GRAD)
+                gmass -= p.mf * uc * delta;
+            }
+          }
+          l0[idx] = ln;
+          if constexpr (MODE == MODE_STEP_GRAD) {
+            p.g_mass[idx] = gmass;
+            p.g_stiff[idx] = gstiff;
+          }
+        }
+      };
+      if (near)
+        body(std::true_type{});
+      else
+        body(std::false_type{});
+    }
+#pragma unroll
+    for (int k = 0; k < 2 * R; ++k) {
+      ql[k] = ql[k + 1];
+      if constexpr (FL::U)
+        qu[k] = qu[k + 1];
+      if constexpr (FL::K)
+        qk[k] = qk[k + 1];
+    }
+  }
+  finish_step(p.ctr, flags & K_ADV);
+}
+
+}  // namespace cwb

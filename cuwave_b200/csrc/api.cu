@@ -1,0 +1,676 @@
+// The C ABI: plans, and the march that runs an op list for a range of steps.
+#include <algorithm>
+#include <atomic>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <functional>
+#include <string>
+#include <vector>
+
+#include "cuwave_b200.h"
+#include "launch.cuh"
+
+namespace {
+
+thread_local std::string g_error;
+std::atomic<long long> g_launches{0};
+
+int fail(const int code, const std::string &what) {
+  g_error = what;
+  return code;
+}
+
+#define CWB_CUDA(call)                                                                   \
+  do {                                                                                   \
+    const cudaError_t e_ = (call);                                                       \
+    if (e_ != cudaSuccess)                                                               \
+      return fail(CWB_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));     \
+  } while (0)
+
+// steps a captured graph holds
+constexpr int GRAPH_STEPS = 32;
+
+struct Scratch {
+  int *start = nullptr;
+  int4 *entry = nullptr;
+  size_t start_cap = 0, entry_cap = 0;
+};
+
+}  // namespace
+
+struct cwb_plan {
+  cwb_grid grid;
+  cwb::Geometry geo;
+  int *ctr = nullptr;
+  cudaStream_t lane = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
+  int sms = 148;
+  int chunk_override = 0;
+  std::vector<Scratch> scratch;
+  long long pml_row[3] = {0, 0, 0};
+};
+
+namespace {
+
+using cwb::Geometry;
+
+bool lined(const cwb_plan *p, const int d) { return p->geo.lo[d] + p->geo.hi[d] > 0; }
+
+// planes of axis 0 a block marches: enough blocks to fill the device a few times over
+int chunk_for(const cwb_plan *p, const int plane_blocks) {
+  if (p->chunk_override > 0)
+    return p->chunk_override;
+  const int rows = p->geo.n[0] - 2;
+  if (p->geo.ndim == 3)
+    return std::min(rows, 128);
+  const long long want = 8LL * p->sms;
+  const long long chunk = (rows * (long long)plane_blocks + want - 1) / want;
+  return (int)std::max<long long>(8, std::min<long long>(rows, chunk));
+}
+
+void stencil_grid(const cwb_plan *p, dim3 &grid, int &chunk) {
+  int bx, by;
+  cwb::block_shape(p->geo.ndim, bx, by);
+  const Geometry &g = p->geo;
+  const int F = g.ndim - 1;
+  const int gx = (g.ext[F] + bx - 1) / bx;
+  const int gy = g.ndim == 3 ? (g.n[1] + by - 1) / by : 1;
+  chunk = chunk_for(p, gx * gy);
+  const int gz = (g.n[0] - 2 + chunk - 1) / chunk;
+  grid = g.ndim == 3 ? dim3(gx, gy, gz) : dim3(gx, gz, 1);
+}
+
+cwb::DLevel to_level(const cwb_level &L, const int bytes) {
+  cwb::DLevel d;
+  d.base = static_cast<char *>(L.base);
+  d.stride = L.stride * bytes;
+  d.mul = L.mul;
+  d.add = L.add;
+  d.period = L.period;
+  return d;
+}
+
+template <typename T>
+int fill_material(const cwb_plan *p, const cwb_material &m, const T **stiff, const T **minv,
+                  const T **damping, const T **prof, T &sconst, T &gconst, T &dgconst,
+                  int &flags, bool &uniform) {
+  uniform = m.stiff_uniform != 0;
+  *stiff = static_cast<const T *>(m.stiff);
+  *minv = static_cast<const T *>(m.minv);
+  *damping = static_cast<const T *>(m.damping);
+  if (!uniform && !m.stiff)
+    return fail(CWB_ERR_ARG, "a non-uniform stiffness needs the stiff field");
+  if (!m.derive_inertia && !m.minv)
+    return fail(CWB_ERR_ARG, "minv is required unless derive_inertia is set");
+  for (int d = 0; d < 3; ++d) {
+    prof[d] = static_cast<const T *>(m.profile[d]);
+    if (d < p->geo.ndim && lined(p, d) && !prof[d])
+      return fail(CWB_ERR_ARG, "a lined axis needs its pml profile");
+  }
+  sconst = (T)m.stiff_value;
+  const T s = sconst;
+  gconst = s * s / (s + s);
+  dgconst = s * s / ((s + s) * (s + s));
+  if (m.derive_inertia)
+    flags |= cwb::K_DERIVE;
+  if (m.damping)
+    flags |= cwb::K_DAMP;
+  return CWB_OK;
+}
+
+int check_level(const cwb_level &L, const char *what) {
+  if (!L.base)
+    return fail(CWB_ERR_ARG, std::string("op level ") + what + " has no base pointer");
+  if (L.period < 0)
+    return fail(CWB_ERR_ARG, std::string("op level ") + what + " has a negative period");
+  return CWB_OK;
+}
+
+using Launch = std::function<cudaError_t(cudaStream_t, bool)>;
+
+// the folded sources of a step, listed per block of its grid
+template <typename T>
+int build_sources(cwb_plan *p, const size_t slot, const cwb_points &pts, const dim3 grid,
+                  const int chunk, cudaStream_t stream, const int **start, const int4 **entry) {
+  const Geometry &g = p->geo;
+  const int nblocks = grid.x * grid.y * grid.z;
+  std::vector<int> lin(pts.num);
+  if (pts.num) {
+    CWB_CUDA(cudaMemcpyAsync(lin.data(), pts.lin, sizeof(int) * pts.num,
+                             cudaMemcpyDeviceToHost, stream));
+    CWB_CUDA(cudaStreamSynchronize(stream));
+  }
+  int bx, by;
+  cwb::block_shape(g.ndim, bx, by);
+  const int F = g.ndim - 1;
+  std::vector<std::vector<int4>> per(nblocks);
+  for (int j = 0; j < pts.num; ++j) {
+    int rest = lin[j], A[3] = {0, 0, 0};
+    for (int d = 0; d < g.ndim; ++d) {
+      A[d] = rest / g.s[d];
+      rest -= A[d] * g.s[d];
+    }
+    for (int d = 0; d < g.ndim; ++d)
+      if (A[d] < 1 || A[d] > g.n[d] - 2)
+        return fail(CWB_ERR_ARG, "a folded source must sit on an interior node");
+    const int gx = A[F] / bx, lx = A[F] % bx;
+    const int gy = g.ndim == 3 ? A[1] / by : 0, ly = g.ndim == 3 ? A[1] % by : 0;
+    const int gz = (A[0] - 1) / chunk;
+    const int blk = g.ndim == 3 ? gx + grid.x * (gy + grid.y * gz) : gx + grid.x * gz;
+    per[blk].push_back(make_int4(A[0], ly * bx + lx, j, 0));
+  }
+  std::vector<int> starts(nblocks + 1, 0);
+  std::vector<int4> entries;
+  entries.reserve(std::max(1, pts.num));
+  for (int b = 0; b < nblocks; ++b) {
+    std::stable_sort(per[b].begin(), per[b].end(), [](const int4 &x, const int4 &y) {
+      return x.x != y.x ? x.x < y.x : x.z < y.z;
+    });
+    entries.insert(entries.end(), per[b].begin(), per[b].end());
+    starts[b + 1] = (int)entries.size();
+  }
+  if (entries.empty())
+    entries.push_back(make_int4(-1, -1, 0, 0));
+  if (p->scratch.size() <= slot)
+    p->scratch.resize(slot + 1);
+  Scratch &sc = p->scratch[slot];
+  if (sc.start_cap < starts.size()) {
+    if (sc.start)
+      cudaFree(sc.start);
+    if (cudaMalloc(&sc.start, sizeof(int) * starts.size()) != cudaSuccess)
+      return fail(CWB_ERR_ALLOC, "source list allocation failed");
+    sc.start_cap = starts.size();
+  }
+  if (sc.entry_cap < entries.size()) {
+    if (sc.entry)
+      cudaFree(sc.entry);
+    if (cudaMalloc(&sc.entry, sizeof(int4) * entries.size()) != cudaSuccess)
+      return fail(CWB_ERR_ALLOC, "source list allocation failed");
+    sc.entry_cap = entries.size();
+  }
+  CWB_CUDA(cudaMemcpyAsync(sc.start, starts.data(), sizeof(int) * starts.size(),
+                           cudaMemcpyHostToDevice, stream));
+  CWB_CUDA(cudaMemcpyAsync(sc.entry, entries.data(), sizeof(int4) * entries.size(),
+                           cudaMemcpyHostToDevice, stream));
+  CWB_CUDA(cudaStreamSynchronize(stream));
+  *start = sc.start;
+  *entry = sc.entry;
+  return CWB_OK;
+}
+
+template <typename T, int NDIM>
+cudaError_t step_nd(const cwb::StepParams<T> &p, const int R, const bool u, const dim3 grid,
+                    cudaStream_t s) {
+  switch (R) {
+  case 1: return cwb::step_unit<T, NDIM, 1>(p, u, grid, s);
+  case 2: return cwb::step_unit<T, NDIM, 2>(p, u, grid, s);
+  case 3: return cwb::step_unit<T, NDIM, 3>(p, u, grid, s);
+  case 4: return cwb::step_unit<T, NDIM, 4>(p, u, grid, s);
+  case 5: return cwb::step_unit<T, NDIM, 5>(p, u, grid, s);
+  case 6: return cwb::step_unit<T, NDIM, 6>(p, u, grid, s);
+  case 7: return cwb::step_unit<T, NDIM, 7>(p, u, grid, s);
+  case 8: return cwb::step_unit<T, NDIM, 8>(p, u, grid, s);
+  }
+  return cudaErrorInvalidValue;
+}
+
+template <typename T, int NDIM>
+cudaError_t adjoint_nd(const cwb::AdjointParams<T> &p, const int R, const bool u,
+                       const int mode, const dim3 grid, cudaStream_t s) {
+  switch (R) {
+  case 1: return cwb::adjoint_unit<T, NDIM, 1>(p, u, mode, grid, s);
+  case 2: return cwb::adjoint_unit<T, NDIM, 2>(p, u, mode, grid, s);
+  case 3: return cwb::adjoint_unit<T, NDIM, 3>(p, u, mode, grid, s);
+  case 4: return cwb::adjoint_unit<T, NDIM, 4>(p, u, mode, grid, s);
+  case 5: return cwb::adjoint_unit<T, NDIM, 5>(p, u, mode, grid, s);
+  case 6: return cwb::adjoint_unit<T, NDIM, 6>(p, u, mode, grid, s);
+  case 7: return cwb::adjoint_unit<T, NDIM, 7>(p, u, mode, grid, s);
+  case 8: return cwb::adjoint_unit<T, NDIM, 8>(p, u, mode, grid, s);
+  }
+  return cudaErrorInvalidValue;
+}
+
+template <typename T>
+cudaError_t step_dispatch(const cwb::StepParams<T> &p, const int ndim, const int R,
+                          const bool u, const dim3 grid, cudaStream_t s) {
+  return ndim == 3 ? step_nd<T, 3>(p, R, u, grid, s) : step_nd<T, 2>(p, R, u, grid, s);
+}
+
+template <typename T>
+cudaError_t adjoint_dispatch(const cwb::AdjointParams<T> &p, const int ndim, const int R,
+                             const bool u, const int mode, const dim3 grid, cudaStream_t s) {
+  return ndim == 3 ? adjoint_nd<T, 3>(p, R, u, mode, grid, s)
+                   : adjoint_nd<T, 2>(p, R, u, mode, grid, s);
+}
+
+template <typename T>
+void fill_weights(const cwb_plan *p, T *w, T *f) {
+  for (int k = 0; k < cwb::MAXR; ++k)
+    w[k] = k < p->grid.radius ? (T)p->grid.coeffs[k] : (T)0;
+  for (int d = 0; d < 3; ++d)
+    f[d] = d < p->geo.ndim ? (T)p->grid.factors[d] : (T)0;
+}
+
+// the launches of one op, each taking (stream, advance)
+template <typename T>
+int translate(cwb_plan *p, const cwb_op &op, const size_t slot, cudaStream_t stream,
+              std::vector<Launch> &out) {
+  const Geometry &g = p->geo;
+  const int ndim = g.ndim, R = p->grid.radius;
+  const int bytes = sizeof(T);
+  int rc;
+  switch (op.kind) {
+  case CWB_OP_STEP: {
+    if ((rc = check_level(op.a, "a")) || (rc = check_level(op.b, "b")) ||
+        (rc = check_level(op.c, "c")))
+      return rc;
+    cwb::StepParams<T> sp;
+    std::memset(&sp, 0, sizeof sp);
+    sp.g = g;
+    fill_weights(p, sp.w, sp.f);
+    sp.dt = (T)p->grid.dt;
+    bool uniform;
+    int flags = 0;
+    T dgconst;
+    if ((rc = fill_material<T>(p, op.mat, &sp.stiff, &sp.minv, &sp.damping, sp.prof, sp.sconst,
+                               sp.gconst, dgconst, flags, uniform)))
+      return rc;
+    if (op.flags & CWB_PML) {
+      flags |= cwb::K_PML;
+      for (int d = 0; d < ndim; ++d) {
+        sp.aux[d] = static_cast<T *>(op.memory[d]);
+        sp.auxrow[d] = (int)p->pml_row[d];
+        if (lined(p, d) && !sp.aux[d])
+          return fail(CWB_ERR_ARG, "a lined axis needs its pml memory");
+      }
+    }
+    dim3 grid;
+    stencil_grid(p, grid, sp.chunk);
+    if (op.flags & CWB_FOLD_REFILL) {
+      flags |= cwb::K_REFILL;
+      sp.refill = p->grid.neumann | p->grid.dirichlet;
+    }
+    if ((op.flags & CWB_FOLD_SOURCES) && op.points.num > 0) {
+      flags |= cwb::K_SRC;
+      if (!op.points.weight || !op.points.record)
+        return fail(CWB_ERR_ARG, "folded sources need weights and a signal");
+      if ((rc = build_sources<T>(p, slot, op.points, grid, sp.chunk, stream, &sp.src_start,
+                                 &sp.src_entry)))
+        return rc;
+      sp.src_weight = static_cast<const T *>(op.points.weight);
+      sp.signal = static_cast<const T *>(op.points.record);
+      sp.nsrc = op.points.num;
+      sp.sig_mul = op.points.row_mul;
+      sp.sig_add = op.points.row_add;
+    }
+    sp.flags = flags;
+    sp.u0 = to_level(op.a, bytes);
+    sp.u1 = to_level(op.b, bytes);
+    sp.u2 = to_level(op.c, bytes);
+    sp.ctr = p->ctr;
+    out.push_back([sp, ndim, R, uniform, grid](cudaStream_t s, bool adv) {
+      cwb::StepParams<T> q = sp;
+      if (adv)
+        q.flags |= cwb::K_ADV;
+      return step_dispatch<T>(q, ndim, R, uniform, grid, s);
+    });
+    return CWB_OK;
+  }
+  case CWB_OP_ADJOINT:
+  case CWB_OP_GRADIENT: {
+    const bool grad_only = op.kind == CWB_OP_GRADIENT;
+    cwb::AdjointParams<T> ap;
+    std::memset(&ap, 0, sizeof ap);
+    ap.g = g;
+    fill_weights(p, ap.w, ap.f);
+    ap.dt = (T)p->grid.dt;
+    bool uniform;
+    int flags = 0;
+    const T *prof[3];
+    if ((rc = fill_material<T>(p, op.mat, &ap.stiff, &ap.minv, &ap.damping, prof, ap.sconst,
+                               ap.gconst, ap.dgconst, flags, uniform)))
+      return rc;
+    for (int d = 0; d < 3; ++d)
+      ap.prof[d] = prof[d];
+    ap.mf = (T)op.scale;
+    int mode;
+    if (grad_only) {
+      mode = cwb::MODE_GRAD;
+      if ((rc = check_level(op.a, "a")) || (rc = check_level(op.b, "b")) ||
+          (rc = check_level(op.c, "c")) || (rc = check_level(op.d, "d")))
+        return rc;
+      if (!op.g_mass || !op.g_stiff)
+        return fail(CWB_ERR_ARG, "the gradient op needs both accumulators");
+      ap.u0 = to_level(op.a, bytes);
+      ap.u1 = to_level(op.b, bytes);
+      ap.u2 = to_level(op.c, bytes);
+      ap.l1 = to_level(op.d, bytes);
+      for (int d = 0; d < 3; ++d)
+        ap.f[d] = d < ndim ? (T)op.factors[d] : (T)0;
+    } else {
+      if ((rc = check_level(op.a, "a")) || (rc = check_level(op.b, "b")))
+        return rc;
+      ap.l0 = to_level(op.a, bytes);
+      ap.l1 = to_level(op.b, bytes);
+      mode = cwb::MODE_STEP;
+      if (op.flags & CWB_GRAD) {
+        if ((rc = check_level(op.c, "c")))
+          return rc;
+        if (!op.g_mass || !op.g_stiff)
+          return fail(CWB_ERR_ARG, "gradients need both accumulators");
+        mode = cwb::MODE_STEP_GRAD;
+        ap.u1 = to_level(op.c, bytes);
+      }
+      if (op.flags & CWB_PML) {
+        flags |= cwb::K_PML;
+        for (int d = 0; d < ndim; ++d) {
+          ap.mem[d] = static_cast<T *>(op.memory[d]);
+          ap.memrow[d] = (int)p->pml_row[d];
+          if (lined(p, d) && !ap.mem[d])
+            return fail(CWB_ERR_ARG, "a lined axis needs its adjoint pml memory");
+        }
+      }
+    }
+    ap.g_mass = static_cast<T *>(op.g_mass);
+    ap.g_stiff = static_cast<T *>(op.g_stiff);
+    ap.flags = flags;
+    ap.ctr = p->ctr;
+    dim3 grid;
+    stencil_grid(p, grid, ap.chunk);
+    out.push_back([ap, ndim, R, uniform, mode, grid](cudaStream_t s, bool adv) {
+      cwb::AdjointParams<T> q = ap;
+      if (adv)
+        q.flags |= cwb::K_ADV;
+      return adjoint_dispatch<T>(q, ndim, R, uniform, mode, grid, s);
+    });
+    return CWB_OK;
+  }
+  case CWB_OP_PML_AUX: {
+    if ((rc = check_level(op.a, "a")))
+      return rc;
+    const T *stiff, *minv, *damping, *prof[3];
+    T sconst, gconst, dgconst;
+    bool uniform;
+    int flags = 0;
+    if ((rc = fill_material<T>(p, op.mat, &stiff, &minv, &damping, prof, sconst, gconst,
+                               dgconst, flags, uniform)))
+      return rc;
+    for (int d = 0; d < ndim; ++d) {
+      if (!lined(p, d))
+        continue;
+      cwb::PmlAuxParams<T> pa;
+      std::memset(&pa, 0, sizeof pa);
+      pa.g = g;
+      pa.f = (T)p->grid.factors[d];
+      pa.d = d;
+      pa.l1 = to_level(op.a, bytes);
+      pa.stiff = stiff;
+      pa.minv = minv;
+      pa.prof = prof[d];
+      pa.mem = static_cast<T *>(op.memory[d]);
+      if (!pa.mem)
+        return fail(CWB_ERR_ARG, "a lined axis needs its adjoint pml memory");
+      pa.memrow = (int)p->pml_row[d];
+      pa.sconst = sconst;
+      pa.uniform = uniform;
+      pa.ctr = p->ctr;
+      out.push_back([pa](cudaStream_t s, bool adv) {
+        cwb::PmlAuxParams<T> q = pa;
+        q.flags = adv ? cwb::K_ADV : 0;
+        return cwb::launch_pml_aux<T>(q, s);
+      });
+    }
+    return CWB_OK;
+  }
+  case CWB_OP_EXCITE:
+  case CWB_OP_LOAD:
+  case CWB_OP_RECORD:
+  case CWB_OP_REPLAY:
+  case CWB_OP_REFILL: {
+    if ((rc = check_level(op.a, "a")))
+      return rc;
+    cwb::TransferParams<T> tp;
+    std::memset(&tp, 0, sizeof tp);
+    tp.g = g;
+    tp.a = to_level(op.a, bytes);
+    tp.ctr = p->ctr;
+    int kind, total = 0, faces = 0;
+    T *g_mass = nullptr;
+    if (op.kind == CWB_OP_REFILL) {
+      kind = cwb::TR_REFILL;
+      faces = p->grid.neumann | p->grid.dirichlet;
+      for (int d = 0; d < ndim; ++d) {
+        int face = 1;
+        for (int e = 0; e < ndim; ++e)
+          if (e != d)
+            face *= g.n[e] - 2;
+        total += face * (((faces >> (2 * d)) & 1) + ((faces >> (2 * d + 1)) & 1));
+      }
+    } else {
+      const cwb_points &pt = op.points;
+      if (pt.num <= 0)
+        return CWB_OK;  // nothing to move
+      if (!pt.lin || !pt.record)
+        return fail(CWB_ERR_ARG, "a transfer needs indices and a record");
+      if (pt.store < 0 || pt.store > 2 || (pt.store == 2 && sizeof(T) == 4))
+        return fail(CWB_ERR_ARG, "unknown record storage");
+      tp.lin = pt.lin;
+      tp.weight = static_cast<const T *>(pt.weight);
+      tp.record = pt.record;
+      tp.num = pt.num;
+      tp.row_mul = pt.row_mul;
+      tp.row_add = pt.row_add;
+      tp.store = pt.store;
+      total = pt.num;
+      if (op.kind == CWB_OP_EXCITE || op.kind == CWB_OP_LOAD) {
+        if (!pt.weight)
+          return fail(CWB_ERR_ARG, "an excitation needs weights");
+      }
+      kind = op.kind == CWB_OP_EXCITE   ? cwb::TR_EXCITE
+             : op.kind == CWB_OP_LOAD   ? cwb::TR_LOAD
+             : op.kind == CWB_OP_RECORD ? cwb::TR_RECORD
+                                        : cwb::TR_REPLAY;
+      if (op.kind == CWB_OP_LOAD && op.g_mass) {
+        if ((rc = check_level(op.c, "c")))
+          return rc;
+        tp.flags |= cwb::K_MASS;
+        tp.c = to_level(op.c, bytes);
+        tp.scale = (T)op.scale;
+        g_mass = static_cast<T *>(op.g_mass);
+      }
+    }
+    if (total <= 0)
+      return CWB_OK;
+    out.push_back([tp, kind, g_mass, faces, total](cudaStream_t s, bool adv) {
+      cwb::TransferParams<T> q = tp;
+      if (adv)
+        q.flags |= cwb::K_ADV;
+      return cwb::launch_transfer<T>(kind, q, g_mass, faces, total, s);
+    });
+    return CWB_OK;
+  }
+  }
+  return fail(CWB_ERR_ARG, "unknown op kind " + std::to_string(op.kind));
+}
+
+int enqueue_step(const std::vector<Launch> &launches, cudaStream_t s) {
+  for (size_t i = 0; i < launches.size(); ++i) {
+    const cudaError_t e = launches[i](s, i + 1 == launches.size());
+    if (e != cudaSuccess)
+      return fail(CWB_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
+  }
+  g_launches += (long long)launches.size();
+  return CWB_OK;
+}
+
+template <typename T>
+int march(cwb_plan *p, const cwb_op *ops, const int nops, const int t0, const int steps,
+          const int graph, cudaStream_t user) {
+  std::vector<Launch> launches;
+  for (int i = 0; i < nops; ++i) {
+    const int rc = translate<T>(p, ops[i], (size_t)i, user, launches);
+    if (rc)
+      return rc;
+  }
+  if (launches.empty() || steps <= 0)
+    return CWB_OK;
+  // the march runs on the plan's own stream, ordered after and before the caller's
+  CWB_CUDA(cudaEventRecord(p->fork, user));
+  CWB_CUDA(cudaStreamWaitEvent(p->lane, p->fork, 0));
+  cudaStream_t s = p->lane;
+  CWB_CUDA(cwb::launch_set_counter(p->ctr, t0, s));
+  ++g_launches;
+  int done = 0;
+  if (graph && steps >= 2 * GRAPH_STEPS) {
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    CWB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    int rc = CWB_OK;
+    for (int k = 0; k < GRAPH_STEPS && !rc; ++k)
+      rc = enqueue_step(launches, s);
+    const cudaError_t ce = cudaStreamEndCapture(s, &g);
+    if (rc)
+      return rc;
+    if (ce != cudaSuccess)
+      return fail(CWB_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
+    g_launches -= (long long)GRAPH_STEPS * launches.size();  // captured, not run
+    CWB_CUDA(cudaGraphInstantiate(&exec, g, 0));
+    cudaGraphDestroy(g);
+    for (; done + GRAPH_STEPS <= steps; done += GRAPH_STEPS) {
+      const cudaError_t e = cudaGraphLaunch(exec, s);
+      if (e != cudaSuccess) {
+        cudaGraphExecDestroy(exec);
+        return fail(CWB_ERR_CUDA, std::string("graph launch: ") + cudaGetErrorString(e));
+      }
+      g_launches += (long long)GRAPH_STEPS * launches.size();
+    }
+    cudaGraphExecDestroy(exec);
+  }
+  for (; done < steps; ++done) {
+    const int rc = enqueue_step(launches, s);
+    if (rc)
+      return rc;
+  }
+  CWB_CUDA(cudaEventRecord(p->join, s));
+  CWB_CUDA(cudaStreamWaitEvent(user, p->join, 0));
+  return CWB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *cwb_last_error(void) { return g_error.c_str(); }
+
+int32_t cwb_version(void) { return 1; }
+
+int64_t cwb_launches(void) { return g_launches.load(); }
+
+int cwb_plan_create(const cwb_grid *grid, cwb_plan **out) {
+  if (!grid || !out)
+    return fail(CWB_ERR_ARG, "null argument");
+  *out = nullptr;
+  const cwb_grid &G = *grid;
+  if (G.ndim != 2 && G.ndim != 3)
+    return fail(CWB_ERR_UNSUPPORTED, "the steps are 2D and 3D");
+  if (G.radius < 1 || G.radius > CWB_MAX_RADIUS)
+    return fail(CWB_ERR_UNSUPPORTED, "radius runs 1 .. 8");
+  if (G.precision != 4 && G.precision != 8)
+    return fail(CWB_ERR_UNSUPPORTED, "precision is 4 or 8 bytes");
+  cwb::Geometry geo;
+  std::memset(&geo, 0, sizeof geo);
+  geo.ndim = G.ndim;
+  long long total = 1;
+  for (int d = 0; d < G.ndim; ++d) {
+    if (G.nx[d] < G.radius + 3)
+      return fail(CWB_ERR_ARG, "every axis needs at least radius + 3 nodes");
+    geo.n[d] = G.nx[d];
+    geo.ext[d] = d == G.ndim - 1 ? (G.nx[d] + 31) / 32 * 32 : G.nx[d];
+    total *= geo.ext[d];
+  }
+  if (total >= (1LL << 31))
+    return fail(CWB_ERR_ARG, "the padded grid overflows int32 flat indices");
+  geo.s[G.ndim - 1] = 1;
+  for (int d = G.ndim - 2; d >= 0; --d)
+    geo.s[d] = geo.s[d + 1] * geo.ext[d + 1];
+  geo.dir = G.dirichlet;
+  if ((G.dirichlet & G.neumann) != 0)
+    return fail(CWB_ERR_ARG, "a face is either Neumann or Dirichlet");
+  for (int d = 0; d < G.ndim; ++d) {
+    geo.lo[d] = G.pml_lo[d];
+    geo.hi[d] = G.pml_hi[d];
+    if (geo.lo[d] < 0 || geo.hi[d] < 0 ||
+        (geo.lo[d] + geo.hi[d] > 0 &&
+         (geo.lo[d] ? geo.lo[d] + G.radius : 0) + (geo.hi[d] ? geo.hi[d] + G.radius : 0) >=
+             G.nx[d] - 2))
+      return fail(CWB_ERR_ARG, "the pml layers and their reach leave no interior");
+  }
+  cwb_plan *p = new cwb_plan();
+  p->grid = G;
+  p->geo = geo;
+  for (int d = 0; d < G.ndim; ++d) {
+    if (geo.lo[d] + geo.hi[d] == 0)
+      continue;
+    long long row = 1;
+    for (int e = 0; e < G.ndim; ++e)
+      row *= e == d ? geo.lo[d] + geo.hi[d] : geo.ext[e];
+    p->pml_row[d] = row;
+  }
+  int dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&p->sms, cudaDevAttrMultiProcessorCount, dev);
+  if (const char *env = std::getenv("CWB_CHUNK"))
+    p->chunk_override = std::atoi(env);
+  if (cudaMalloc(&p->ctr, 2 * sizeof(int)) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&p->lane, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&p->fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&p->join, cudaEventDisableTiming) != cudaSuccess) {
+    cwb_plan_destroy(p);
+    return fail(CWB_ERR_ALLOC, std::string("plan resources: ") +
+                                   cudaGetErrorString(cudaGetLastError()));
+  }
+  cudaMemset(p->ctr, 0, 2 * sizeof(int));
+  *out = p;
+  return CWB_OK;
+}
+
+int cwb_plan_destroy(cwb_plan *p) {
+  if (!p)
+    return CWB_OK;
+  if (p->lane)
+    cudaStreamSynchronize(p->lane);
+  for (Scratch &s : p->scratch) {
+    if (s.start)
+      cudaFree(s.start);
+    if (s.entry)
+      cudaFree(s.entry);
+  }
+  if (p->ctr)
+    cudaFree(p->ctr);
+  if (p->fork)
+    cudaEventDestroy(p->fork);
+  if (p->join)
+    cudaEventDestroy(p->join);
+  if (p->lane)
+    cudaStreamDestroy(p->lane);
+  delete p;
+  return CWB_OK;
+}
+
+int64_t cwb_pml_row(const cwb_plan *p, const int32_t d) {
+  if (!p || d < 0 || d > 2)
+    return 0;
+  return p->pml_row[d];
+}
+
+int cwb_march(cwb_plan *p, const cwb_op *ops, const int32_t nops, const int32_t t0,
+              const int32_t steps, const int32_t graph, void *stream) {
+  if (!p || (!ops && nops > 0) || nops < 0)
+    return fail(CWB_ERR_ARG, "null argument");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  return p->grid.precision == 4 ? march<float>(p, ops, nops, t0, steps, graph, s)
+                                : march<double>(p, ops, nops, t0, steps, graph, s);
+}
+
+}  // extern "C"

@@ -1,0 +1,158 @@
+// Device helpers shared by the step, adjoint and transfer kernels.
+//
+// Arithmetic is written in the reference's own expression order and the library is
+// built with --fmad=false, so nothing is contracted that the reference's host build
+// (g++ -ffp-contract=off, cuwave/cpu.py) does not contract either; the explicit fused
+// operations of cuwave/kernels/common.cuh:11-19 (MUL_RN, FMA_RN) are kept as such.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace cwb {
+
+// op flags as the kernels read them
+enum : int {
+  K_PML = 1,      // step / adjoint: the lined axes carry memory terms
+  K_DAMP = 2,     // a damping field divides the update
+  K_DERIVE = 4,   // 1 / m = 1 / k
+  K_SRC = 8,      // step: sources folded in
+  K_REFILL = 16,  // step: face ghosts written from their mirrors
+  K_ADV = 32,     // this launch ends the step: the last block advances the counter
+  K_GRAD = 64,    // adjoint: accumulate g_mass, g_stiff
+  K_MASS = 128,   // load: the adjoint load's inertia share
+};
+
+struct DLevel {
+  char *base;
+  long long stride;  // bytes between levels
+  int mul, add, period;
+};
+
+template <typename T>
+__device__ __forceinline__ T *level(const DLevel &L, const int t) {
+  long long k = (long long)L.mul * t + L.add;
+  if (L.period > 0) {
+    k %= L.period;
+    if (k < 0)
+      k += L.period;
+  }
+  return reinterpret_cast<T *>(L.base + k * L.stride);
+}
+
+__device__ __forceinline__ int step_index(const int *ctr) {
+  return *reinterpret_cast<const volatile int *>(ctr);
+}
+
+// The launch that ends a time step advances the step counter once every block is
+// done: each block reads the counter when it starts, so the last to finish is past
+// every read. All threads of the block must reach this call.
+__device__ __forceinline__ void finish_step(int *ctr, const bool advance) {
+  if (!advance)
+    return;
+  __syncthreads();
+  if (threadIdx.x == 0 && threadIdx.y == 0 && threadIdx.z == 0) {
+    __threadfence();
+    const unsigned total = gridDim.x * gridDim.y * gridDim.z;
+    const unsigned prev = atomicAdd(reinterpret_cast<unsigned *>(ctr + 1), 1u);
+    if (prev == total - 1) {
+      ctr[1] = 0;
+      ctr[0] = ctr[0] + 1;
+      __threadfence();
+    }
+  }
+}
+
+// products and fused products the compiler keeps as written
+__device__ __forceinline__ float mul_rn(const float a, const float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mul_rn(const double a, const double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float fma_rn(const float a, const float b, const float c) {
+  return __fmaf_rn(a, b, c);
+}
+__device__ __forceinline__ double fma_rn(const double a, const double b, const double c) {
+  return __fma_rn(a, b, c);
+}
+
+// node b of an axis of N nodes as the forward step reads it: past the stored ghost
+// its mirror about the wall node, negated past a face of `odd` (cuwave common.cuh:50-54)
+__device__ __forceinline__ int mirror_node(const int b, const int N, const int odd, int &sign) {
+  sign = ((b < 0 && (odd & 1)) || (b > N - 1 && (odd & 2))) ? -1 : 1;
+  return b < 0 ? 2 - b : (b > N - 1 ? 2 * (N - 2) - b : b);
+}
+
+// node b past the wall node its image, as the adjoint reads a field no refill keeps:
+// the ghost itself is mirrored too (cuwave common.cuh:73-77)
+__device__ __forceinline__ int node_image(const int b, const int N, const int odd, int &sign) {
+  sign = ((b < 1 && (odd & 1)) || (b > N - 2 && (odd & 2))) ? -1 : 1;
+  return b < 1 ? 2 - b : (b > N - 2 ? 2 * (N - 2) - b : b);
+}
+
+// whether node a is the wall node of a Dirichlet face of `odd` (cuwave common.cuh:43-46)
+__device__ __forceinline__ bool held_wall(const int a, const int N, const int odd) {
+  return ((odd & 1) && a == 1) || ((odd & 2) && a == N - 2);
+}
+
+template <typename T>
+__device__ __forceinline__ T signed_value(const T v, const int sign) {
+  return sign > 0 ? v : (sign < 0 ? -v : (T)0);
+}
+
+// d(D+)/d(u at row q off the node) and d(D-)/d(u ...) at the full radius, the weights
+// the pml transpose scatters with (cuwave scalar_sensitivity.cu:221-234)
+template <typename T, int R>
+__device__ __forceinline__ T plus_tap(const T *w, const int q) {
+  if (q >= 1)
+    return q <= R ? w[q - 1] : (T)0;
+  return 1 - q <= R ? -w[-q] : (T)0;
+}
+template <typename T, int R>
+__device__ __forceinline__ T minus_tap(const T *w, const int q) {
+  if (q >= 0)
+    return q + 1 <= R ? w[q] : (T)0;
+  return -q <= R ? -w[-q - 1] : (T)0;
+}
+
+// ------------------------------------------------------------------ pml slabs
+// A lined axis d keeps its memory over the slab of its layer rows: row r < lo is node
+// 1 + r, row lo + k is node N - 1 - hi + k. The memory is laid out as the padded grid
+// with axis d replaced by those lo + hi rows, so a slab row along the march stays
+// contiguous in the fast axis.
+__device__ __forceinline__ int slab_row(const int a, const int N, const int lo, const int hi) {
+  if (lo && a >= 1 && a <= lo)
+    return a - 1;
+  if (hi && a >= N - 1 - hi && a <= N - 2)
+    return lo + a - (N - 1 - hi);
+  return -1;
+}
+
+struct Geometry {
+  int ndim;
+  int n[3];      // logical extents
+  int ext[3];    // padded extents (only the last differs)
+  int s[3];      // strides in elements
+  int lo[3], hi[3];
+  int dir;       // Dirichlet faces
+};
+
+// flat slab index of node A (its axis-d coordinate replaced by slab row r)
+__device__ __forceinline__ int slab_index(const Geometry &g, const int d, const int r,
+                                          const int *A) {
+  int idx = 0;
+  for (int e = 0; e < g.ndim; ++e) {
+    const int extent = e == d ? g.lo[d] + g.hi[d] : g.ext[e];
+    idx = idx * extent + (e == d ? r : A[e]);
+  }
+  return idx;
+}
+
+// the cell weight W of an interior node: 1/2 per axis on whose wall it sits
+template <typename T>
+__device__ __forceinline__ T cell_weight(const Geometry &g, const int *A) {
+  T w = (T)1;
+  for (int e = 0; e < g.ndim; ++e)
+    if (A[e] == 1 || A[e] == g.n[e] - 2)
+      w *= (T)0.5;
+  return w;
+}
+
+}  // namespace cwb

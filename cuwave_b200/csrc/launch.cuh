@@ -1,0 +1,34 @@
+// Host-side launchers of the kernel families. The stencil kernels are instantiated
+// one translation unit per (precision, dimension, radius), unit.cu compiled with
+// CWB_REAL / CWB_NDIM / CWB_RADIUS, so the build runs in parallel.
+#pragma once
+
+#include "params.cuh"
+
+namespace cwb {
+
+// block shapes: BX fast-axis nodes by BY axis-1 nodes (3D), BX nodes (2D)
+constexpr int STEP_BX3 = 32, STEP_BY3 = 8, STEP_BX2 = 128;
+constexpr int ADJ_BX3 = 32, ADJ_BY3 = 8, ADJ_BX2 = 128;
+
+inline void block_shape(const int ndim, int &bx, int &by) {
+  bx = ndim == 3 ? STEP_BX3 : STEP_BX2;
+  by = ndim == 3 ? STEP_BY3 : 1;
+}
+
+template <typename T, int NDIM, int R>
+cudaError_t step_unit(const StepParams<T> &p, bool uniform, dim3 grid, cudaStream_t stream);
+template <typename T, int NDIM, int R>
+cudaError_t adjoint_unit(const AdjointParams<T> &p, bool uniform, int mode, dim3 grid,
+                         cudaStream_t stream);
+
+template <typename T>
+cudaError_t launch_transfer(int kind, const TransferParams<T> &p, T *g_mass, int faces,
+                            int threads_total, cudaStream_t stream);
+template <typename T>
+cudaError_t launch_pml_aux(const PmlAuxParams<T> &p, cudaStream_t stream);
+cudaError_t launch_set_counter(int *ctr, int t0, cudaStream_t stream);
+
+enum : int { TR_EXCITE = 0, TR_LOAD = 1, TR_RECORD = 2, TR_REPLAY = 3, TR_REFILL = 4 };
+
+}  // namespace cwb

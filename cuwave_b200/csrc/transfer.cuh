@@ -1,0 +1,212 @@
+// Point transfers, the ghost refill and the adjoint pml memory step.
+#pragma once
+
+#include "params.cuh"
+
+namespace cwb {
+
+constexpr int TRANSFER_THREADS = 256;
+
+// float32 rounded to the nearest even bfloat16, as wave.narrow does it
+// (cuwave/wave.py:848-853): the high half after adding 0x7FFF plus the kept lsb
+__device__ __forceinline__ unsigned short narrow_bf16(const float v) {
+  const unsigned bits = __float_as_uint(v);
+  return (unsigned short)((bits + 0x7FFFu + ((bits >> 16) & 1u)) >> 16);
+}
+__device__ __forceinline__ float widen_bf16(const unsigned short b) {
+  return __uint_as_float(((unsigned)b) << 16);
+}
+
+template <typename T>
+__device__ __forceinline__ T record_read(const TransferParams<T> &p, const long long at) {
+  if (p.store == 1)
+    return (T)widen_bf16(reinterpret_cast<const unsigned short *>(p.record)[at]);
+  if (p.store == 2)
+    return (T)reinterpret_cast<const float *>(p.record)[at];
+  return reinterpret_cast<const T *>(p.record)[at];
+}
+
+template <typename T>
+__device__ __forceinline__ void record_write(const TransferParams<T> &p, const long long at,
+                                             const T v) {
+  if (p.store == 1)
+    reinterpret_cast<unsigned short *>(p.record)[at] = narrow_bf16((float)v);
+  else if (p.store == 2)
+    reinterpret_cast<float *>(p.record)[at] = (float)v;
+  else
+    reinterpret_cast<T *>(p.record)[at] = v;
+}
+
+// a[lin] += weight * record[row] (excitation_kernel, cuwave/kernels/common.cuh:456-464)
+template <typename T>
+__global__ void excite_kernel(const TransferParams<T> p) {
+  const int t = step_index(p.ctr);
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j < p.num) {
+    T *a = level<T>(p.a, t);
+    const long long row = (long long)p.row_mul * t + p.row_add;
+    atomicAdd(&a[p.lin[j]], p.weight[j] * record_read(p, row * p.num + j));
+  }
+  finish_step(p.ctr, p.flags & K_ADV);
+}
+
+// the adjoint load, and with K_MASS its share of the inertia gradient against c
+// (adjoint_excitation_kernel, common.cuh:467-480)
+template <typename T>
+__global__ void load_kernel(const TransferParams<T> p, T *g_mass) {
+  const int t = step_index(p.ctr);
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j < p.num) {
+    T *a = level<T>(p.a, t);
+    const long long row = (long long)p.row_mul * t + p.row_add;
+    const int n = p.lin[j];
+    const T load = p.weight[j] * record_read(p, row * p.num + j);
+    atomicAdd(&a[n], load);
+    if (p.flags & K_MASS) {
+      const T *u1 = level<T>(p.c, t);
+      atomicAdd(&g_mass[n], -p.scale * u1[n] * load);
+    }
+  }
+  finish_step(p.ctr, p.flags & K_ADV);
+}
+
+// record[row] = a[lin] (get_signal_kernel, common.cuh:483-491)
+template <typename T>
+__global__ void record_kernel(const TransferParams<T> p) {
+  const int t = step_index(p.ctr);
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j < p.num) {
+    const T *a = level<T>(p.a, t);
+    const long long row = (long long)p.row_mul * t + p.row_add;
+    record_write(p, row * p.num + j, a[p.lin[j]]);
+  }
+  finish_step(p.ctr, p.flags & K_ADV);
+}
+
+// a[lin] = record[row] (set_signal_kernel, common.cuh:494-503)
+template <typename T>
+__global__ void replay_kernel(const TransferParams<T> p) {
+  const int t = step_index(p.ctr);
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j < p.num) {
+    T *a = level<T>(p.a, t);
+    const long long row = (long long)p.row_mul * t + p.row_add;
+    a[p.lin[j]] = record_read(p, row * p.num + j);
+  }
+  finish_step(p.ctr, p.flags & K_ADV);
+}
+
+// One thread per face ghost, edges and corners excluded: the ghost takes its mirror
+// two nodes in, negated on a Dirichlet face whose wall node is zeroed
+// (homogeneous_neumann_kernel / homogeneous_dirichlet_kernel, scalar.cu:535-555).
+template <typename T>
+__global__ void refill_kernel(const TransferParams<T> p, const int faces) {
+  const int t = step_index(p.ctr);
+  const Geometry &g = p.g;
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  T *u = level<T>(p.a, t);
+  for (int d = 0; d < g.ndim; ++d) {
+    int face = 1;
+    for (int e = 0; e < g.ndim; ++e)
+      if (e != d)
+        face *= g.n[e] - 2;
+    for (int side = 0; side < 2; ++side) {
+      if (!((faces >> (2 * d + side)) & 1))
+        continue;
+      if (k >= 0 && k < face) {
+        int rest = k, off = 0;
+        for (int e = g.ndim - 1; e >= 0; --e)
+          if (e != d) {
+            off += (rest % (g.n[e] - 2) + 1) * g.s[e];
+            rest /= g.n[e] - 2;
+          }
+        const int ghost = off + (side ? g.n[d] - 1 : 0) * g.s[d];
+        const int normal = side ? -g.s[d] : g.s[d];
+        const bool odd = (g.dir >> (2 * d + side)) & 1;
+        const T v = u[ghost + 2 * normal];
+        u[ghost] = odd ? -v : v;
+        if (odd)
+          u[ghost + normal] = (T)0;
+      }
+      k -= face;
+    }
+  }
+  finish_step(p.ctr, p.flags & K_ADV);
+}
+
+// The adjoint pml memory of one lined axis from lambda^(n+1), then the coefficients
+// c+ and c- the transposed step gathers (pml_aux_kernel and pml_tap,
+// cuwave/kernels/scalar_sensitivity.cu:518-542, 237-251). One thread per slab node.
+template <typename T>
+__global__ void pml_aux_kernel(const PmlAuxParams<T> p) {
+  const int t = step_index(p.ctr);
+  const Geometry &g = p.g;
+  const int d = p.d;
+  const int lo = g.lo[d], hi = g.hi[d], N = g.n[d];
+  long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool active = k < p.memrow;
+  if (active) {
+    // decompose the slab index over the grid with axis d replaced by its rows
+    int A[3] = {0, 0, 0};
+    long long rest = k;
+    int r = 0;
+    for (int e = g.ndim - 1; e >= 0; --e) {
+      const int extent = e == d ? lo + hi : g.ext[e];
+      const int c = (int)(rest % extent);
+      rest /= extent;
+      if (e == d)
+        r = c;
+      else
+        A[e] = c;
+    }
+    const int a = r < lo ? 1 + r : N - 1 - hi + (r - lo);
+    A[d] = a;
+    bool interior = true;
+    for (int e = 0; e < g.ndim; ++e)
+      if (e != d && (A[e] < 1 || A[e] > g.n[e] - 2))
+        interior = false;
+    if (interior) {
+      const T *l1 = level<T>(p.l1, t);
+      int idx = 0;
+      bool held = false;
+      for (int e = 0; e < g.ndim; ++e) {
+        idx += A[e] * g.s[e];
+        held |= held_wall(A[e], g.n[e], (g.dir >> (2 * e)) & 3);
+      }
+      const int o = g.s[d];
+      T sc, sp, sm;
+      if (p.uniform) {
+        sc = sp = sm = p.sconst;
+      } else {
+        sc = p.stiff[idx];
+        sp = p.stiff[idx + o];
+        sm = p.stiff[idx - o];
+      }
+      const T gp = sc * sp / (sc + sp), gm = sc * sm / (sc + sm);
+      const T w = cell_weight<T>(g, A);
+      const T q = held ? (T)0 : w * l1[idx];
+      const T *an = p.prof, *bn = p.prof + N, *ah = p.prof + 2 * N, *bh = p.prof + 3 * N;
+      T *mem = p.mem;
+      const long long sz = p.memrow;
+      const T f = p.f;
+      const T ez = mem[2 * sz + k];
+      const T e0 = bh[a] * (mem[k] + an[a] * f * gp * ez) + f * gp * q;
+      const T e1 = bh[a - 1] * (mem[sz + k] - an[a] * f * gm * ez) - f * gm * q;
+      const T e2 = bn[a] * ez + q;
+      mem[k] = e0;
+      mem[sz + k] = e1;
+      mem[2 * sz + k] = e2;
+      const T ez2 = an[a] * f * e2;
+      mem[3 * sz + k] = ah[a] * e0 + gp * (1 + ah[a]) * ez2;
+      mem[4 * sz + k] = ah[a - 1] * e1 - gm * (1 + ah[a - 1]) * ez2;
+    }
+  }
+  finish_step(p.ctr, p.flags & K_ADV);
+}
+
+__global__ void set_counter_kernel(int *ctr, const int t0) {
+  ctr[0] = t0;
+  ctr[1] = 0;
+}
+
+}  // namespace cwb

@@ -1,0 +1,76 @@
+// One (precision, dimension, radius) of the step and adjoint kernels, selected by
+// CWB_REAL, CWB_NDIM and CWB_RADIUS at compile time.
+#include "adjoint.cuh"
+#include "launch.cuh"
+#include "step.cuh"
+
+#if !defined(CWB_REAL) || !defined(CWB_NDIM) || !defined(CWB_RADIUS)
+#error "unit.cu is compiled with CWB_REAL, CWB_NDIM and CWB_RADIUS"
+#endif
+
+namespace cwb {
+
+namespace {
+
+template <class Kernel>
+cudaError_t allow_smem(Kernel k, const size_t bytes) {
+  if (bytes <= 48 * 1024)
+    return cudaSuccess;
+  return cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+template <typename T, int NDIM, int R, bool U>
+cudaError_t step_one(const StepParams<T> &p, const dim3 grid, cudaStream_t s) {
+  constexpr int BX = NDIM == 3 ? STEP_BX3 : STEP_BX2;
+  constexpr int BY = NDIM == 3 ? STEP_BY3 : 1;
+  const size_t smem = 2 * StepShape<NDIM, R, BX, BY>::PLANE * sizeof(T);
+  const auto k = step_kernel<T, NDIM, R, U, BX, BY>;
+  cudaError_t e = allow_smem(k, smem);
+  if (e != cudaSuccess)
+    return e;
+  k<<<grid, dim3(BX, BY), smem, s>>>(p);
+  return cudaGetLastError();
+}
+
+template <typename T, int NDIM, int R, bool U, int MODE>
+cudaError_t adjoint_one(const AdjointParams<T> &p, const dim3 grid, cudaStream_t s) {
+  constexpr int BX = NDIM == 3 ? ADJ_BX3 : ADJ_BX2;
+  constexpr int BY = NDIM == 3 ? ADJ_BY3 : 1;
+  const size_t smem =
+      2 * AdjFields<MODE, U>::COUNT * AdjShape<NDIM, R, BX, BY>::PLANE * sizeof(T);
+  const auto k = adjoint_kernel<T, NDIM, R, U, MODE, BX, BY>;
+  cudaError_t e = allow_smem(k, smem);
+  if (e != cudaSuccess)
+    return e;
+  k<<<grid, dim3(BX, BY), smem, s>>>(p);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+template <typename T, int NDIM, int R>
+cudaError_t step_unit(const StepParams<T> &p, const bool uniform, const dim3 grid,
+                      cudaStream_t stream) {
+  return uniform ? step_one<T, NDIM, R, true>(p, grid, stream)
+                 : step_one<T, NDIM, R, false>(p, grid, stream);
+}
+
+template <typename T, int NDIM, int R>
+cudaError_t adjoint_unit(const AdjointParams<T> &p, const bool u, const int mode,
+                         const dim3 grid, cudaStream_t s) {
+  if (mode == MODE_STEP)
+    return u ? adjoint_one<T, NDIM, R, true, MODE_STEP>(p, grid, s)
+             : adjoint_one<T, NDIM, R, false, MODE_STEP>(p, grid, s);
+  if (mode == MODE_STEP_GRAD)
+    return u ? adjoint_one<T, NDIM, R, true, MODE_STEP_GRAD>(p, grid, s)
+             : adjoint_one<T, NDIM, R, false, MODE_STEP_GRAD>(p, grid, s);
+  return u ? adjoint_one<T, NDIM, R, true, MODE_GRAD>(p, grid, s)
+           : adjoint_one<T, NDIM, R, false, MODE_GRAD>(p, grid, s);
+}
+
+template cudaError_t step_unit<CWB_REAL, CWB_NDIM, CWB_RADIUS>(const StepParams<CWB_REAL> &,
+                                                               bool, dim3, cudaStream_t);
+template cudaError_t adjoint_unit<CWB_REAL, CWB_NDIM, CWB_RADIUS>(
+    const AdjointParams<CWB_REAL> &, bool, int, dim3, cudaStream_t);
+
+}  // namespace cwb

@@ -1,0 +1,174 @@
+/*
+ * cuwave_b200.h -- C ABI of the B200 scalar-wave hot path.
+ *
+ * One shared library, libcuwave_b200.so, steps the scalar (pressure) wave equation's
+ * leapfrog update with its perfectly matched layer, source injection, ghost refill and
+ * receiver recording, and the transposed (adjoint) update with the material-gradient
+ * accumulation, on one sm_100a GPU.
+ *
+ * Every pointer below is a DEVICE pointer unless its comment says otherwise. Fields are
+ * C-contiguous over the padded grid (nx[0], .., ceil32(nx[ndim-1])); a flat node index
+ * is sum_d i_d * stride_d over that grid, int32. Every call returns CWB_OK (0) or a
+ * negative CWB_ERR_* code, and cwb_last_error() then holds one line of text. Nothing is
+ * allocated outside a plan: a plan owns its scratch (counters, source lists, graphs).
+ *
+ * The reference (cmpmech/cuwave) launches one CUDA C kernel per operation from Python;
+ * on its host fallback each kernel is bound through the C ABI
+ *     extern "C" void launch_<kernel>(gx, gy, gz, bx, by, bz, void **args)
+ * (cuwave/kernels/cpu.hpp:93-98). The entry points here replace those launches, grouped
+ * per time step: see each op kind for the reference kernels it stands in for.
+ */
+#ifndef CUWAVE_B200_H
+#define CUWAVE_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CWB_OK 0
+#define CWB_ERR_ARG (-1)         /* an argument out of range or inconsistent */
+#define CWB_ERR_CUDA (-2)        /* a CUDA runtime call failed */
+#define CWB_ERR_UNSUPPORTED (-3) /* a configuration this build does not step */
+#define CWB_ERR_ALLOC (-4)       /* a plan could not allocate its scratch */
+
+#define CWB_MAX_RADIUS 8
+
+/* Grid geometry and the stencil, fixed for a plan.
+ * Replaces the compile-time configuration of cuwave/kernels/scalar.cu:1-12 (NDIM,
+ * USE_FLOAT, STENCIL_RADIUS, OP_COEFFS, DIRICHLET_FACES) and the geometry arguments
+ * of wave.axis_geometry (cuwave/wave.py:830-837). */
+typedef struct cwb_grid {
+  int32_t ndim;                  /* 2 or 3 */
+  int32_t nx[3];                 /* logical nodes per axis, ghost ring included */
+  int32_t radius;                /* R = space_order / 2, 1 .. 8 */
+  int32_t precision;             /* bytes per value: 4 (float32) or 8 (float64) */
+  double coeffs[CWB_MAX_RADIUS]; /* OP_W(R, 1..R), rounded to `precision` on use */
+  double factors[3];             /* the per-axis step factors f_d */
+  double dt;                     /* the time step, read by the damped update */
+  int32_t dirichlet;             /* faces held at zero, bit 2 * axis + side */
+  int32_t neumann;               /* faces refilled evenly, bit 2 * axis + side */
+  int32_t pml_lo[3], pml_hi[3];  /* layer depth behind each face, 0 for none */
+} cwb_grid;
+
+typedef struct cwb_plan cwb_plan;
+
+/* Where the field of time step t lives: base + ((mul * t + add) mod period) * stride
+ * elements (period 0: no wrap). Two slots rotate as period 2, a history as period 0. */
+typedef struct cwb_level {
+  void *base;
+  int64_t stride;
+  int32_t mul, add, period;
+} cwb_level;
+
+/* The material a step reads. Replaces PressureWave.step_kernel_args
+ * (cuwave/scalar.py:739-745) and the pml profiles (cuwave/boundary.py:327-361). */
+typedef struct cwb_material {
+  const void *stiff;       /* k over the padded grid; unread when stiff_uniform */
+  const void *minv;        /* 1 / m over the padded grid; unread when derive_inertia */
+  const void *damping;     /* d over the padded grid, or NULL for a lossless step */
+  const void *profile[3];  /* (4, nx[d]) rows a_node, b_node, a_half, b_half per lined axis */
+  int32_t derive_inertia;  /* 1 / m = 1 / k (ScalarWave) */
+  int32_t stiff_uniform;   /* k is stiff_value everywhere the step reads it */
+  double stiff_value;
+} cwb_material;
+
+/* A transfer list: `num` flat node indices, a per-point weight and a (rows, num)
+ * record whose row for step t is row_mul * t + row_add. */
+typedef struct cwb_points {
+  const int32_t *lin;
+  const void *weight;   /* per point, or NULL where the op reads none */
+  void *record;         /* (rows, num) values */
+  int32_t num;
+  int32_t row_mul, row_add;
+  int32_t store;        /* record elements: 0 the plan's precision, 1 bfloat16 bits
+                           (uint16, round to nearest even), 2 float32 under float64 */
+} cwb_points;
+
+/* Op kinds of a march step, run in order for every step t. */
+enum {
+  /* The leapfrog update u^t = 2u^(t-1) - u^(t-2) + dt^2/m div(k grad u^(t-1)) of the
+   * interior, its pml memory terms, and, per flags, the folded sources and ghost refill.
+   * a = u^(t-2) (read), b = u^(t-1) (read), c = u^t (written; may alias a).
+   * Replaces fd_kernel (cuwave/kernels/scalar.cu:347-496) and pml_kernel
+   * (scalar.cu:500-532), and with CWB_FOLD_* excitation_kernel
+   * (cuwave/kernels/common.cuh:456-464) and the refill kernels (scalar.cu:535-555). */
+  CWB_OP_STEP = 1,
+  /* a[lin] += weight * record[row], atomically. Replaces excitation_kernel
+   * (common.cuh:456-464). */
+  CWB_OP_EXCITE = 2,
+  /* a[lin] = record[row]. Replaces set_signal_kernel (common.cuh:494-503). */
+  CWB_OP_REPLAY = 3,
+  /* Ghosts of every face refilled from their mirror, negated and the wall node zeroed on
+   * a Dirichlet face. Replaces homogeneous_neumann_kernel / homogeneous_dirichlet_kernel
+   * (scalar.cu:535-555). */
+  CWB_OP_REFILL = 4,
+  /* record[row] = a[lin] (bfloat16-rounded when points.bf16). Replaces
+   * get_signal_kernel (common.cuh:483-491) and wave.narrow (cuwave/wave.py:848-853). */
+  CWB_OP_RECORD = 5,
+  /* The adjoint pml memory step from a = lambda^(n+1), before CWB_OP_ADJOINT reads it.
+   * Replaces pml_aux_kernel (cuwave/kernels/scalar_sensitivity.cu:518-542). */
+  CWB_OP_PML_AUX = 6,
+  /* The transposed update lambda^n from a = lambda^(n+2) (overwritten) and
+   * b = lambda^(n+1), with the pml transpose gathered in; with CWB_GRAD also
+   * g_mass and g_stiff against c = u^n. Replaces adjoint_kernel and
+   * adjoint_gradient_kernel (scalar_sensitivity.cu:388-515) and pml_adjoint_kernel
+   * (scalar_sensitivity.cu:545-597). */
+  CWB_OP_ADJOINT = 7,
+  /* The adjoint load a[lin] += weight * record[row]; with g_mass also
+   * g_mass[lin] -= scale * c[lin] * load. Replaces adjoint_excitation_kernel
+   * (common.cuh:467-480). */
+  CWB_OP_LOAD = 8,
+  /* Both gradient densities of one forward triplet a, b, c = u^(t-2), u^(t-1), u^t
+   * against d = lambda^t, with scale = 1 / dt^2 and factors F_d. Replaces
+   * gradient_kernel (scalar_sensitivity.cu:303-350). */
+  CWB_OP_GRADIENT = 9,
+};
+
+/* op flags */
+#define CWB_PML 1          /* STEP, ADJOINT: step the pml memory of the lined axes */
+#define CWB_FOLD_SOURCES 2 /* STEP: add `points` (interior nodes only) inside the step */
+#define CWB_FOLD_REFILL 4  /* STEP: write the face ghosts from their mirrors */
+#define CWB_GRAD 8         /* ADJOINT: accumulate g_mass and g_stiff */
+
+typedef struct cwb_op {
+  int32_t kind;
+  int32_t flags;
+  cwb_level a, b, c, d;
+  cwb_material mat;
+  cwb_points points;
+  void *memory[3];   /* pml memory per lined axis: 3 slab rows forward, 5 adjoint */
+  void *g_mass;
+  void *g_stiff;
+  double scale;      /* ADJOINT / LOAD: 1 / dt^2; GRADIENT: 1 / dt^2 */
+  double factors[3]; /* GRADIENT: F_d = f_d / dt^2 */
+} cwb_op;
+
+/* Create and destroy a plan. Replaces compile_kernels (cuwave/wave.py:637-647): one
+ * build serves every order, stencil and face layout, the table a runtime argument. */
+int cwb_plan_create(const cwb_grid *grid, cwb_plan **plan);
+int cwb_plan_destroy(cwb_plan *plan);
+
+/* Run `steps` steps t = t0 .. t0 + steps - 1 of the op list on `stream` (a
+ * cudaStream_t, NULL for the legacy stream). With `graph` nonzero, chunks of steps
+ * are captured once as a CUDA graph and replayed. Replaces wave.march
+ * (cuwave/wave.py:890-952) and the step closures handed to it. */
+int cwb_march(cwb_plan *plan, const cwb_op *ops, int32_t nops, int32_t t0,
+              int32_t steps, int32_t graph, void *stream);
+
+/* Elements per row of the pml memory of axis d (0 for an unlined axis); a forward
+ * memory holds 3 such rows, an adjoint one 5. */
+int64_t cwb_pml_row(const cwb_plan *plan, int32_t d);
+
+/* Kernels the library launched since it was loaded (a diagnostic counter). */
+int64_t cwb_launches(void);
+
+const char *cwb_last_error(void);
+int32_t cwb_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CUWAVE_B200_H */

@@ -1,0 +1,392 @@
+"""CPU ORACLE -- test infrastructure, not the product.
+
+Only tests/, `__graft_entry__.smoke()` and bench.py's cpu_baseline leg import this, and
+only as the checker the CUDA path is compared against. It restates cmpmech/cuwave's
+scalar-wave path on the CPU: the kernels in oracle_impl.h (plain C, one function per
+reference kernel launch) and, here in numpy, the setup and the drivers around them:
+
+    cell coefficients      cuwave/stencils.py:11-58
+    stable_dt              cuwave/wave.py:44-54
+    pml profiles           cuwave/boundary.py:327-361
+    materials              cuwave/scalar.py:407-415, 927-934 (+ wave.mirror_ghosts)
+    excitation weights     cuwave/scalar.py:858-872
+    simulate               cuwave/wave.py:1071-1163 (plain step order, 1119-1127)
+    sensitivity            cuwave/sensitivity.py:384-497 (fused adjoint, 468-480)
+    source_sensitivity     cuwave/sensitivity.py:1054-1111
+
+Pinned against the reference's own outputs: tests/golden/*.npz, produced by running
+the reference package itself (tests/golden/make_golden.py).
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from dataclasses import dataclass, field
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIBRARY = HERE / "liboracle.so"
+
+
+def build() -> Path:
+    """Compile liboracle.so from oracle.c when it is missing or older than its sources."""
+    sources = [HERE / "oracle.c", HERE / "oracle_impl.h"]
+    if LIBRARY.exists() and all(LIBRARY.stat().st_mtime >= s.stat().st_mtime for s in sources):
+        return LIBRARY
+    cc = os.environ.get("ORACLE_CC", "gcc")
+    tmp = LIBRARY.with_suffix(".tmp.so")
+    cmd = [cc, "-O2", "-ffp-contract=off", "-fopenmp", "-fPIC", "-shared",
+           str(HERE / "oracle.c"), "-o", str(tmp), "-lm"]
+    done = subprocess.run(cmd, capture_output=True, text=True)
+    if done.returncode:
+        raise RuntimeError(f"{' '.join(cmd)} failed:\n{done.stderr}")
+    os.replace(tmp, LIBRARY)
+    return LIBRARY
+
+
+class Geo(ctypes.Structure):
+    _fields_ = [
+        ("ndim", ctypes.c_int),
+        ("n", ctypes.c_int * 3),
+        ("ext", ctypes.c_int * 3),
+        ("s", ctypes.c_int * 3),
+        ("lo", ctypes.c_int * 3),
+        ("hi", ctypes.c_int * 3),
+        ("dir", ctypes.c_int),
+        ("R", ctypes.c_int),
+    ]
+
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        _lib = ctypes.CDLL(str(build()))
+        for sfx in ("_f32", "_f64"):
+            getattr(_lib, "orc_slab_size" + sfx).restype = ctypes.c_long
+    return _lib
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _r(dtype, v):
+    return ctypes.c_float(v) if dtype == np.float32 else ctypes.c_double(v)
+
+
+# ------------------------------------------------------------------------- setup
+def cell_coefficients(radius: int, stencil: str = "taylor") -> np.ndarray:
+    """Cell-flux weights w_1..w_R (cuwave stencils.py:11-58)."""
+    if stencil == "taylor":
+        x = np.arange(-radius, radius + 1)
+        A = x[None, :] ** np.arange(2 * radius + 1)[:, None]
+        rhs = np.zeros(2 * radius + 1)
+        rhs[2] = 2.0
+        w = np.linalg.solve(A, rhs)
+        return np.array([w[radius + 1 + k:].sum() for k in range(radius)])
+    k = np.arange(1, radius + 1)
+    for band in np.linspace(np.pi, 0.0, 400, endpoint=False):
+        theta = np.linspace(band / 400, band, 400)
+        G = 2.0 * np.sin(np.outer(theta, k - 0.5)) / theta[:, None]
+        G *= 2.0 * np.sin(theta / 2.0)[:, None] / theta[:, None]
+        cons = (2 * k - 1.0)[None]
+        K = np.block([[G.T @ G, cons.T], [cons, np.zeros((1, 1))]])
+        c = np.linalg.solve(K, np.append(G.sum(axis=0), 1.0))[:radius]
+        if np.abs(np.sqrt(G @ c) - 1.0).max() <= 1e-3:
+            return c
+    raise ValueError(radius)
+
+
+def stable_dt(dx, wavespeed, space_order=2, stencil="optimized") -> float:
+    c = cell_coefficients(space_order // 2, stencil)
+    lam = 4.0 * abs(float(c @ (-1.0) ** np.arange(len(c))))
+    return 2.0 / (wavespeed * float(np.sqrt(lam * sum(1.0 / d**2 for d in dx))))
+
+
+def padded(Nx):
+    return (*Nx[:-1], (Nx[-1] + 31) // 32 * 32)
+
+
+def mirror_ghosts(Nx, f):
+    for d in range(len(Nx)):
+        for ghost, mirror in ((0, 2), (Nx[d] - 1, Nx[d] - 3)):
+            dst = [slice(None)] * len(Nx)
+            src = [slice(None)] * len(Nx)
+            dst[d], src[d] = ghost, mirror
+            f[tuple(dst)] = f[tuple(src)]
+    return f
+
+
+def pml_profiles(Nx, dx, dt, widths, width, wavespeed, reflection, frequency, dtype):
+    """(4, Nx[d]) a_node, b_node, a_half, b_half per lined axis (cuwave boundary.py:327-361)."""
+    L = width - 1
+    out = []
+    for d, (lo, hi) in enumerate(widths):
+        if not lo + hi:
+            out.append(None)
+            continue
+        n = Nx[d]
+        damping = -3.0 * wavespeed * np.log(reflection) / (2.0 * L * dx[d])
+        rows = []
+        for shift in (0.0, 0.5):
+            position = np.arange(n) + shift
+            distance = np.full(n, np.inf)
+            if lo:
+                distance = np.minimum(distance, np.abs(position - 1))
+            if hi:
+                distance = np.minimum(distance, np.abs(n - 2 - position))
+            depth = np.clip((L - distance) / L, 0.0, 1.0)
+            d0 = damping * depth**2
+            alpha = np.pi * frequency
+            inside = depth > 0.0
+            b = np.where(inside, np.exp(-(d0 + alpha) * dt), 1.0)
+            a = np.where(inside, d0 / np.maximum(d0 + alpha, 1e-300) * (b - 1.0), 0.0)
+            rows += [a, b]
+        out.append(np.ascontiguousarray(np.stack(rows).astype(dtype)))
+    return out
+
+
+def acoustic_materials(Nx, indicator, rho1, rho2, kappa1, kappa2, dtype):
+    """(stiff, minv) of AcousticWave, ghosts mirrored (cuwave scalar.py:927-934, 407-415)."""
+    ind = np.asarray(indicator, dtype=dtype)
+    rho_inv = dtype(1 / rho1) + ind * dtype(1 / rho2 - 1 / rho1)
+    kappa_inv = dtype(1 / kappa1) + ind * dtype(1 / kappa2 - 1 / kappa1)
+    minv = dtype(1) / kappa_inv
+    return mirror_ghosts(Nx, rho_inv.astype(dtype)), mirror_ghosts(Nx, minv.astype(dtype))
+
+
+@dataclass
+class Case:
+    """One configuration of the scalar step and its inputs, all numpy."""
+
+    Nx: tuple
+    R: int
+    coeffs: np.ndarray        # w_1..w_R (float64; rounded to dtype on use)
+    factors: tuple            # f_d
+    dt: float
+    stiff: np.ndarray         # padded grid
+    minv: np.ndarray | None   # padded grid, None to derive 1 / stiff
+    dtype: type = np.float32
+    dirichlet: int = 0
+    neumann: int | None = None
+    damping: np.ndarray | None = None
+    widths: tuple | None = None   # ((lo, hi),) per axis of a pml
+    profiles: list | None = None  # per axis (4, Nx[d]) or None
+    source_lin: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int32))
+    source_weight: np.ndarray | None = None
+    signal: np.ndarray | None = None   # (N, nsrc)
+    sensor_lin: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int32))
+
+    def __post_init__(self):
+        self.ndim = len(self.Nx)
+        self.shape = padded(self.Nx)
+        if self.neumann is None:
+            self.neumann = ((1 << (2 * self.ndim)) - 1) & ~self.dirichlet
+        g = Geo()
+        g.ndim = self.ndim
+        strides = [1] * self.ndim
+        for d in range(self.ndim - 2, -1, -1):
+            strides[d] = strides[d + 1] * self.shape[d + 1]
+        for d in range(self.ndim):
+            g.n[d], g.ext[d], g.s[d] = self.Nx[d], self.shape[d], strides[d]
+            if self.widths is not None:
+                g.lo[d], g.hi[d] = self.widths[d]
+        g.dir = self.dirichlet
+        g.R = self.R
+        self.geo = g
+        self.strides = strides
+        self.sfx = "_f32" if self.dtype == np.float32 else "_f64"
+        self.w = np.zeros(8, self.dtype)
+        self.w[: self.R] = np.asarray(self.coeffs, np.float64).astype(self.dtype)
+        self.f = np.zeros(3, self.dtype)
+        self.f[: self.ndim] = np.asarray(self.factors, self.dtype)
+        self.derive = self.minv is None
+
+    def fn(self, name):
+        return getattr(lib(), name + self.sfx)
+
+    def slab_size(self, d):
+        return int(self.fn("orc_slab_size")(ctypes.byref(self.geo), d))
+
+    def lined(self):
+        return [d for d in range(self.ndim) if self.widths is not None and sum(self.widths[d])]
+
+    def excitation_weights(self, lin):
+        """dt^2 minv (/ (1 + beta)) at lin (cuwave scalar.py:858-872), source factor 1."""
+        field_ = self.stiff if self.derive else self.minv
+        w = field_.ravel()[lin]
+        if self.derive:
+            w = self.dtype(1) / w
+        if self.damping is not None:
+            beta = self.dtype(0.5) * w * self.damping.ravel()[lin] * self.dtype(self.dt)
+            w = w / (self.dtype(1) + beta)
+        return (self.dtype(self.dt**2) * w).astype(self.dtype)
+
+    # ------------------------------------------------------------ single launches
+    def step(self, u0, u1, u2):
+        self.fn("orc_step")(ctypes.byref(self.geo), _p(self.w), _p(self.f), _r(self.dtype, self.dt),
+                            _p(u0), _p(u1), _p(u2), _p(self.stiff), _p(self.minv),
+                            _p(self.damping), int(self.derive))
+
+    def pml(self, u1, u2, memory):
+        for d in self.lined():
+            self.fn("orc_pml")(ctypes.byref(self.geo), _p(self.w), d, _r(self.dtype, self.f[d]),
+                               _p(u1), _p(u2), _p(self.stiff), _p(self.minv), int(self.derive),
+                               _p(memory[d]), _p(self.profiles[d]))
+
+    def excite(self, u, lin, weight, row):
+        row = np.ascontiguousarray(row, self.dtype)
+        self.fn("orc_excite")(_p(u), _p(lin), _p(weight), _p(row), int(lin.size))
+
+    def refill(self, u):
+        self.fn("orc_refill")(ctypes.byref(self.geo), _p(u), self.neumann, self.dirichlet)
+
+    def memory(self):
+        return {d: np.zeros((3, self.slab_size(d)), self.dtype) for d in self.lined()}
+
+    # ------------------------------------------------------------------ drivers
+    def forward(self, N, history=False):
+        """N plain steps: fd, pml, excitation, refill, record (cuwave wave.py:1118-1127).
+
+        Returns (final field, (N, nsens) traces) and, with `history`, the (N + 2) levels
+        V with V[t + 2] = u^t as `sensitivity` stores them.
+        """
+        U = np.zeros((2, *self.shape), self.dtype)
+        V = np.zeros((N + 2, *self.shape), self.dtype) if history else None
+        mem = self.memory()
+        um = np.zeros((N, self.sensor_lin.size), self.dtype)
+        for t in range(N):
+            if history:
+                u0, u1, u2 = V[t], V[t + 1], V[t + 2]
+            else:
+                u0, u1, u2 = U[t % 2], U[1 - t % 2], U[t % 2]
+            self.step(u0, u1, u2)
+            self.pml(u1, u2, mem)
+            if self.source_lin.size:
+                self.excite(u2, self.source_lin, self.source_weight, self.signal[t])
+            self.refill(u2)
+            um[t] = u2.ravel()[self.sensor_lin]
+        final = V[N + 1] if history else U[(N - 1) % 2]
+        return (final, um, V) if history else (final, um)
+
+    def cell_weights(self, field_):
+        for d in range(self.ndim):
+            for index in (1, self.Nx[d] - 2):
+                face = [slice(None)] * self.ndim
+                face[d] = index
+                field_[tuple(face)] *= self.dtype(0.5)
+        return field_
+
+    def sensor_weights(self, lin):
+        """W at flat indices lin (cuwave wave.py:347-354)."""
+        w = np.ones(lin.size, self.dtype)
+        rest = lin.astype(np.int64)
+        coords = []
+        for d in range(self.ndim):
+            coords.append(rest // self.strides[d])
+            rest = rest - coords[-1] * self.strides[d]
+        for d in range(self.ndim):
+            for index in (1, self.Nx[d] - 2):
+                w = np.where(coords[d] == index, w * self.dtype(0.5), w)
+        return w
+
+    def pml_nodes(self):
+        inside = np.zeros(self.shape, bool)
+        for d in self.lined():
+            lo, hi = self.widths[d]
+            index = [slice(None)] * self.ndim
+            for rows in (slice(1, 1 + lo), slice(self.Nx[d] - 1 - hi, self.Nx[d] - 1)):
+                index[d] = rows
+                inside[tuple(index)] = True
+        interior = np.zeros(self.shape, bool)
+        interior[tuple(slice(1, n - 1) for n in self.Nx)] = True
+        return inside & interior
+
+    def adjoint_signal(self, dphi):
+        """dphi reversed over W (source factor 1) (cuwave sensitivity.py:272-292)."""
+        return np.ascontiguousarray(
+            np.asarray(dphi, self.dtype)[::-1] / self.sensor_weights(self.sensor_lin), self.dtype
+        )
+
+    def sensitivity(self, N, dphi_of):
+        """Fused adjoint with stored history (cuwave sensitivity.py:384-497).
+
+        `dphi_of(traces) -> (cost, dphi)`. Returns cost, {"mass", "stiff"}, traces.
+        """
+        _, um, V = self.forward(N, history=True)
+        cost, dphi = dphi_of(um)
+        signal = self.adjoint_signal(dphi)
+        weight = self.excitation_weights(self.sensor_lin)
+        g_mass = np.zeros(self.shape, self.dtype)
+        g_stiff = np.zeros(self.shape, self.dtype)
+        P = np.zeros((2, *self.shape), self.dtype)
+        eta = {d: np.zeros((3, self.slab_size(d)), self.dtype) for d in self.lined()}
+        mf = self.dtype(1.0 / self.dt**2)
+        geo = ctypes.byref(self.geo)
+        for m in range(N):
+            l0, l1 = P[m % 2], P[1 - m % 2]
+            u1 = V[N + 1 - m]
+            self.fn("orc_adjoint")(geo, _p(self.w), _p(self.f), _r(self.dtype, self.dt), _p(l0),
+                                   _p(l1), _p(l0), _p(u1), _p(g_mass), _p(g_stiff),
+                                   _p(self.stiff), _p(self.minv), _p(self.damping),
+                                   int(self.derive), _r(self.dtype, mf), 1)
+            for d in self.lined():
+                self.fn("orc_pml_aux")(geo, d, _r(self.dtype, self.f[d]), _p(l1), _p(self.stiff),
+                                       _p(eta[d]), _p(self.profiles[d]))
+                self.fn("orc_pml_adjoint")(geo, _p(self.w), d, _r(self.dtype, self.f[d]), _p(l0),
+                                           _p(g_mass), _p(u1), _r(self.dtype, mf), 1,
+                                           _p(self.stiff), _p(self.minv), int(self.derive),
+                                           _p(eta[d]), _p(self.profiles[d]))
+            row = np.ascontiguousarray(signal[m])
+            self.fn("orc_load")(_p(l0), _p(self.sensor_lin), _p(weight), _p(row),
+                                int(self.sensor_lin.size), _p(g_mass), _p(u1),
+                                _r(self.dtype, mf))
+        grads = {"mass": self.cell_weights(g_mass), "stiff": self.cell_weights(g_stiff)}
+        layer = self.pml_nodes()
+        for g in grads.values():
+            g[layer] = 0
+        return cost, grads, um
+
+    def source_sensitivity(self, N, dphi_of):
+        """d(cost)/d(signal) (cuwave sensitivity.py:1054-1111); source factor 1."""
+        _, um = self.forward(N)
+        cost, dphi = dphi_of(um)
+        signal = self.adjoint_signal(dphi)
+        weight = self.excitation_weights(self.sensor_lin)
+        P = np.zeros((2, *self.shape), self.dtype)
+        eta = {d: np.zeros((3, self.slab_size(d)), self.dtype) for d in self.lined()}
+        lam = np.zeros((N, self.source_lin.size), self.dtype)
+        geo = ctypes.byref(self.geo)
+        for m in range(N):
+            l0, l1 = P[m % 2], P[1 - m % 2]
+            self.fn("orc_adjoint")(geo, _p(self.w), _p(self.f), _r(self.dtype, self.dt), _p(l0),
+                                   _p(l1), _p(l0), None, None, None, _p(self.stiff),
+                                   _p(self.minv), _p(self.damping), int(self.derive),
+                                   _r(self.dtype, 0.0), 0)
+            for d in self.lined():
+                self.fn("orc_pml_aux")(geo, d, _r(self.dtype, self.f[d]), _p(l1), _p(self.stiff),
+                                       _p(eta[d]), _p(self.profiles[d]))
+                self.fn("orc_pml_adjoint")(geo, _p(self.w), d, _r(self.dtype, self.f[d]), _p(l0),
+                                           None, None, _r(self.dtype, 0.0), 0, _p(self.stiff),
+                                           _p(self.minv), int(self.derive), _p(eta[d]),
+                                           _p(self.profiles[d]))
+            self.excite(l0, self.sensor_lin, weight, signal[m])
+            self.refill(l0)
+            lam[m] = l0.ravel()[self.source_lin]
+        gradient = lam[::-1] * self.sensor_weights(self.source_lin)
+        return cost, np.ascontiguousarray(gradient), um
+
+
+def l2(observed):
+    """The least-squares objective (cuwave sensitivity.py:93-100)."""
+    def objective(traces):
+        residual = traces - observed
+        return 0.5 * float(np.sum(residual**2)), residual
+    return objective

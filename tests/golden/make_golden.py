@@ -1,0 +1,238 @@
+"""Generate the golden fixtures by running the reference package itself.
+
+Runs cmpmech/cuwave from its source tree on its CPU fallback (the same scalar.cu /
+scalar_sensitivity.cu kernels, compiled for the host by g++ with OpenMP) on small
+seeded cases, and stores the inputs with the outputs in tests/golden/*.npz. The tests
+rebuild each case from the stored inputs and compare the oracle (and, on a GPU, the
+CUDA path) against the stored outputs.
+
+    python tests/golden/make_golden.py [--reference PATH]
+
+Needs the reference source tree; nothing at test time reads it.
+"""
+
+from __future__ import annotations
+
+import argparse
+import os
+import sys
+import tempfile
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+
+
+def setup(reference: str) -> None:
+    os.environ["CUWAVE_DEVICE"] = "cpu"
+    # the image default CXX lacks libgomp; the system g++ has it
+    os.environ["CXX"] = os.environ.get("GOLDEN_CXX", "/usr/bin/g++")
+    os.environ.setdefault("XDG_CACHE_HOME", tempfile.mkdtemp(prefix="cuwave-golden-"))
+    os.environ.setdefault("OMP_NUM_THREADS", "8")
+    sys.path.insert(0, reference)
+
+
+def smooth_indicator(rng, shape, blobs=4):
+    """A smooth field in [0, 1]: a few Gaussian bumps."""
+    grids = np.meshgrid(*[np.arange(n, dtype=np.float64) for n in shape], indexing="ij")
+    out = np.zeros(shape)
+    for _ in range(blobs):
+        centre = [rng.uniform(0, n) for n in shape]
+        sigma = rng.uniform(2.0, max(3.0, min(shape) / 4))
+        r2 = sum((g - c) ** 2 for g, c in zip(grids, centre))
+        out += rng.uniform(0.3, 1.0) * np.exp(-r2 / (2 * sigma**2))
+    return np.clip(out / max(out.max(), 1e-12), 0.0, 1.0)
+
+
+def stencil_tables():
+    from cuwave.stencils import cell_coefficients
+    from cuwave.wave import stable_dt
+
+    out = {}
+    for R in range(1, 9):
+        for stencil in ("taylor", "optimized"):
+            out[f"coeffs_{stencil}_{R}"] = cell_coefficients(R, stencil)
+            out[f"stable_dt_{stencil}_{R}"] = np.array(
+                stable_dt((1.0, 0.5), 1.7, 2 * R, stencil)
+            )
+    return out
+
+
+def build_case(name, ndim, Nx, order, N, *, faces="neumann", pml=None, damping=False,
+               stencil="optimized", scalar=False, precision="float32", nsens=3, seed=0):
+    """Inputs of one run: a dict of arrays and scalars, rebuildable without the reference."""
+    from cuwave.wave import padded_shape
+    from cuwave.signals import ricker
+    from cuwave.stencils import cell_coefficients
+
+    rng = np.random.default_rng(seed)
+    shape = padded_shape(Nx)
+    indicator = np.zeros(shape)
+    indicator[tuple(slice(0, n) for n in Nx)] = smooth_indicator(rng, Nx)
+    c = cell_coefficients(order // 2, stencil)
+    lam = 4.0 * abs(float(c @ (-1.0) ** np.arange(len(c))))
+    cmax = 1.0 if scalar else 1.3
+    dx = tuple(1.0 for _ in Nx)
+    dt = 0.5 * 2.0 / (cmax * np.sqrt(lam * sum(1.0 / d**2 for d in dx)))
+    t = np.arange(N) * dt
+    freq = 1.0 / (20.0 * dx[0])
+    src = np.array([[n // 2] for n in Nx], dtype=np.int32)
+    sens = np.stack(
+        [rng.integers(2, n - 2, size=nsens) for n in Nx]
+    ).astype(np.int32)
+    signal = ricker(t, 1.0, freq)[:, None].astype(precision)
+    case = dict(
+        name=name, ndim=ndim, Nx=np.array(Nx), order=order, N=N, dt=dt, stencil=stencil,
+        faces=faces, scalar=scalar, precision=precision, indicator=indicator,
+        source=src, signal=signal, sensors=sens, kappa2=1.0 / 1.69,
+        pml=np.array(pml if pml is not None else [0, 0.0]), damping=damping,
+    )
+    return case
+
+
+def make_sim(case):
+    from cuwave.boundary import Dirichlet, Neumann, Pml, sponge
+    from cuwave.scalar import AcousticWave, ScalarWave
+
+    Nx = tuple(int(n) for n in case["Nx"])
+    ndim = len(Nx)
+    if case["faces"] == "neumann":
+        boundary = Neumann
+    elif case["faces"] == "dirichlet":
+        boundary = Dirichlet
+    else:  # mixed: Dirichlet on the low face of axis 0 and the high face of the last axis
+        boundary = [[Neumann, Neumann] for _ in range(ndim)]
+        boundary[0][0] = Dirichlet
+        boundary[-1][1] = Dirichlet
+        boundary = tuple(tuple(p) for p in boundary)
+    pml = None
+    if case["pml"][0] > 0:
+        pml = Pml(width=int(case["pml"][0]), wavespeed=float(case["pml"][1]))
+    common = dict(
+        Nx=Nx, dx=tuple(1.0 for _ in Nx), N=int(case["N"]), dt=float(case["dt"]),
+        threads=(8,) * (ndim - 1) + (32,), precision=str(case["precision"]),
+        space_order=int(case["order"]), stencil=str(case["stencil"]), boundary=boundary,
+        pml=pml,
+    )
+    if case["scalar"]:
+        sim = ScalarWave(**common, wavespeed=1.0, density=1.0)
+    else:
+        sim = AcousticWave(**common, rho1=1.0, rho2=1.0, kappa1=1.0, kappa2=float(case["kappa2"]))
+    if case["damping"]:
+        from dataclasses import replace
+
+        ind = case["indicator"].astype(sim.dtype) if not case["scalar"] else 1.0 + case["indicator"].astype(sim.dtype)
+        damping = sponge(sim, ind.copy(), width=4, beta=0.3)
+        sim = replace(sim, damping=damping)
+    return sim
+
+
+def design(case, sim):
+    ind = case["indicator"].astype(sim.dtype)
+    return (1.0 + ind) if case["scalar"] else ind
+
+
+def run_forward(case):
+    from cuwave.wave import Source, simulate
+
+    sim = make_sim(case)
+    source = Source(case["source"].copy(), case["signal"].astype(sim.dtype))
+    field, um = simulate(sim, source, design(case, sim).copy(), case["sensors"].copy())
+    out = dict(case)
+    out["field"] = np.asarray(field)
+    out["traces"] = np.asarray(um)
+    if sim.damping is not None:
+        out["damping_field"] = np.asarray(sim.damping)
+    return out
+
+
+def run_gradients(case):
+    from cuwave.sensitivity import (
+        l2_misfit,
+        reconstruction_sensitivity,
+        sensitivity,
+        source_sensitivity,
+    )
+    from cuwave.wave import Source, simulate
+
+    sim = make_sim(case)
+    source = Source(case["source"].copy(), case["signal"].astype(sim.dtype))
+    # observed traces from a perturbed design
+    perturbed = design(case, sim).copy()
+    perturbed *= 0.95
+    _, observed = simulate(sim, source, perturbed, case["sensors"].copy())
+    observed = np.asarray(observed)
+    objective = l2_misfit(observed)
+    cost, grads, um, _ = sensitivity(sim, source, design(case, sim).copy(), case["sensors"].copy(), objective)
+    scost, sgrad, _, _ = source_sensitivity(sim, source, design(case, sim).copy(), case["sensors"].copy(), objective)
+    rcost, rgrads, _, info = reconstruction_sensitivity(
+        sim, source, design(case, sim).copy(), case["sensors"].copy(), objective, checkpoints=2
+    )
+    out = dict(case)
+    out.update(
+        observed=observed, cost=np.array(cost), g_mass=np.asarray(grads["mass"]),
+        g_stiff=np.asarray(grads["stiff"]), traces=np.asarray(um), source_cost=np.array(scost),
+        source_gradient=np.asarray(sgrad), rec_cost=np.array(rcost),
+        rec_g_mass=np.asarray(rgrads["mass"]), rec_g_stiff=np.asarray(rgrads["stiff"]),
+        rec_strip=np.array(info["strip"]), rec_segment=np.array(info["segment"]),
+        rec_sweeps=np.array(info["sweeps"]),
+    )
+    if sim.damping is not None:
+        out["damping_field"] = np.asarray(sim.damping)
+    return out
+
+
+FORWARD = [
+    dict(name="fwd2d_r1", ndim=2, Nx=(30, 37), order=2, N=80),
+    dict(name="fwd2d_r2_mixed", ndim=2, Nx=(30, 40), order=4, N=80, faces="mixed"),
+    dict(name="fwd2d_r4", ndim=2, Nx=(40, 46), order=8, N=100),
+    dict(name="fwd2d_r4_taylor_dir", ndim=2, Nx=(33, 35), order=8, N=70, faces="dirichlet",
+         stencil="taylor"),
+    dict(name="fwd2d_r8", ndim=2, Nx=(36, 44), order=16, N=60),
+    dict(name="fwd2d_r4_damped", ndim=2, Nx=(34, 38), order=8, N=70, damping=True),
+    dict(name="fwd2d_r4_pml", ndim=2, Nx=(44, 50), order=8, N=120, pml=(8, 1.3)),
+    dict(name="fwd2d_r3_pml_mixed", ndim=2, Nx=(40, 42), order=6, N=90, pml=(6, 1.3),
+         faces="mixed"),
+    dict(name="fwd2d_scalar_r2", ndim=2, Nx=(30, 33), order=4, N=60, scalar=True),
+    dict(name="fwd3d_r1", ndim=3, Nx=(16, 18, 20), order=2, N=40),
+    dict(name="fwd3d_r4_pml", ndim=3, Nx=(26, 24, 28), order=8, N=50, pml=(5, 1.3)),
+    dict(name="fwd3d_r2_mixed", ndim=3, Nx=(18, 17, 21), order=4, N=40, faces="mixed"),
+    dict(name="fwd2d_r4_f64", ndim=2, Nx=(34, 38), order=8, N=70, precision="float64"),
+]
+
+GRADIENTS = [
+    dict(name="grad2d_r4", ndim=2, Nx=(34, 38), order=8, N=70),
+    dict(name="grad2d_r4_pml", ndim=2, Nx=(44, 46), order=8, N=90, pml=(8, 1.3)),
+    dict(name="grad2d_r2_mixed", ndim=2, Nx=(30, 33), order=4, N=60, faces="mixed"),
+    dict(name="grad2d_r4_damped", ndim=2, Nx=(34, 36), order=8, N=60, damping=True),
+    dict(name="grad3d_r2_pml", ndim=3, Nx=(22, 20, 24), order=4, N=40, pml=(5, 1.3)),
+    dict(name="grad2d_r4_pml_f64", ndim=2, Nx=(40, 42), order=8, N=70, pml=(7, 1.3),
+         precision="float64"),
+]
+
+
+def main(argv=None) -> int:
+    parser = argparse.ArgumentParser(description=__doc__)
+    parser.add_argument("--reference", default="/root/reference")
+    parser.add_argument("--only", default=None)
+    args = parser.parse_args(argv)
+    setup(args.reference)
+    np.savez_compressed(HERE / "stencils.npz", **stencil_tables())
+    for spec in FORWARD:
+        if args.only and args.only not in spec["name"]:
+            continue
+        out = run_forward(build_case(**spec))
+        np.savez_compressed(HERE / f"{spec['name']}.npz", **out)
+        print(spec["name"], "ok", flush=True)
+    for spec in GRADIENTS:
+        if args.only and args.only not in spec["name"]:
+            continue
+        out = run_gradients(build_case(**spec))
+        np.savez_compressed(HERE / f"{spec['name']}.npz", **out)
+        print(spec["name"], "ok", flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())
