@@ -1,0 +1,410 @@
+#!/usr/bin/env python
+"""Benchmark of the scalar-wave hot path: the 3D forward with PML.
+
+Workload (one bench step = one whole job): AcousticWave on a 512^3 grid (ghosts
+included), fp32, radius-4 optimized stencil, 20-cell PML on every face, 4000 leapfrog
+steps at CFL 0.5, six seeded horizontal layers of speed in [1.0, 2.5] with a +-5% random
+perturbation, a Ricker source at node (22, 256, 256), and a 128 x 128 receiver plane on
+row 30 (stride-4 columns). Data are synthetic (seeded), inputs larger than L2.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+`value` is Gpt-updates/s (interior nodes x time steps / job time) with the inputs
+resident in HBM; `e2e` is the same through the public `simulate` call with host
+buffers (pinned host -> device copies of the inputs and device -> host copies of the
+traces and the final field inside the timed region). Multi-GPU runs are replicas (the
+path does not shard across GPUs here): every rank runs the whole job on its own GPU.
+`--impl reference` times the reference's own kernels compiled for the host cores
+(oracle/_ref) on a bounded sample of the same workload.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "Gpt-updates/s + % HBM roofline; learned-vs-plain time at 1e-2 rel. trace error"
+UNIT = "Gpt-updates/s"
+BYTES_PER_UPDATE = 16  # read u^(t-1), u^(t-2), 1/m; write u^t (stiffness uniform)
+PML_BYTES = 24  # read + write of psi+, psi-, zeta per slab node per lined axis
+
+
+def workload(size: int = 512, steps: int = 4000, width: int = 20, seed: int = 0) -> dict:
+    """The seeded inputs of the layered 3D job, all numpy."""
+    rng = np.random.default_rng(seed)
+    Nx = (size, size, size)
+    shape = (size, size, (size + 31) // 32 * 32)
+    # six layers along axis 0, speeds sorted upwards in depth
+    speeds = np.sort(rng.uniform(1.0, 2.5, 6))
+    cuts = np.sort(rng.choice(np.arange(2, size - 2), 5, replace=False))
+    layer = np.searchsorted(cuts, np.arange(size), side="right")
+    c = speeds[layer][:, None, None] * (1.0 + rng.uniform(-0.05, 0.05, Nx))
+    c_max = float(c.max())
+    kappa2 = 2.5**2
+    # AcousticWave with rho1 = rho2 = kappa1 = 1: minv = kappa(gamma) = c^2
+    indicator = np.zeros(shape, np.float32)
+    indicator[:, :, :size] = ((1.0 / c**2 - 1.0) / (1.0 / kappa2 - 1.0)).astype(np.float32)
+    from cuwave_b200.stencils import stable_dt
+
+    dt = 0.5 * stable_dt((1.0, 1.0, 1.0), c_max, 8, "optimized")
+    from cuwave_b200.signals import ricker
+
+    freq = float(c.min()) / 20.0
+    signal = ricker(np.arange(steps) * dt, 1.0, freq)[:, None].astype(np.float32)
+    source = np.array([[22], [size // 2], [size // 2]], np.int32)
+    cols = 2 + 4 * np.arange(min(128, (size - 4) // 4))
+    a1, a2 = np.meshgrid(cols, cols, indexing="ij")
+    sensors = np.stack([np.full(a1.size, 30), a1.ravel(), a2.ravel()]).astype(np.int32)
+    return dict(Nx=Nx, steps=steps, width=width, dt=dt, c_max=c_max, kappa2=kappa2,
+                indicator=indicator, signal=signal, source=source, sensors=sensors)
+
+
+def make_sim(w: dict):
+    from cuwave_b200 import AcousticWave, Pml
+
+    return AcousticWave(
+        Nx=w["Nx"], dx=(1.0, 1.0, 1.0), N=w["steps"], dt=w["dt"], precision="float32",
+        space_order=8, stencil="optimized", pml=Pml(width=w["width"], wavespeed=w["c_max"]),
+        rho1=1.0, rho2=1.0, kappa1=1.0, kappa2=w["kappa2"],
+    )
+
+
+def interior_updates(w: dict) -> int:
+    return int(np.prod([n - 2 for n in w["Nx"]]))
+
+
+def algorithmic_bytes(w: dict) -> int:
+    """Compulsory HBM bytes of one time step: 16 B per interior update plus 24 B per pml
+    slab node per lined axis."""
+    n = [x - 2 for x in w["Nx"]]
+    slab = sum(2 * w["width"] * int(np.prod([n[e] for e in range(3) if e != d])) for d in range(3))
+    return BYTES_PER_UPDATE * interior_updates(w) + PML_BYTES * slab
+
+
+# ------------------------------------------------------------------- clocks
+REASONS = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+
+
+class ClockSampler:
+    """nvidia-smi clock and throttle-reason samples during the timed region."""
+
+    def __init__(self, index: int):
+        self.path = Path(tempfile.mkstemp(suffix=".csv")[1])
+        query = "index,clocks.sm,clocks.max.sm,power.draw," + ",".join(
+            f"clocks_event_reasons.{r}" for r in REASONS
+        )
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(index), f"--query-gpu={query}", "--format=csv,noheader,nounits",
+                 "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL,
+            )
+        except FileNotFoundError:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        self.proc.wait()
+        rows = [r.split(", ") for r in self.path.read_text().splitlines() if r.strip()]
+        self.path.unlink(missing_ok=True)
+        sm = [float(r[1]) for r in rows if len(r) >= 8 and r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if len(r) >= 8 and r[2].replace(".", "").isdigit()]
+        reasons = sorted({REASONS[i] for r in rows if len(r) >= 8 for i in range(4)
+                          if r[4 + i].strip().lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+# ------------------------------------------------------------------- helpers
+def dist_setup():
+    """(rank, world, local_rank) from the torchrun environment; a gloo/nccl group when > 1."""
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    return rank, world, local
+
+
+def cpu_baseline(w: dict, sample_steps: int, cores: int | None = None) -> dict:
+    """The reference's own kernels (oracle/_ref, built from its sources) on the host cores,
+    a bounded sample of `sample_steps` steps of the same job."""
+    from oracle import oracle as o
+
+    path = o.ref_library(3, 4, "optimized", "float32")
+    if not path.exists():
+        return {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
+                "sample": f"unavailable: {path.name} not built (oracle/ref_build.py)"}
+    cores = cores or os.cpu_count() or 1
+    case = reference_case(w)
+    o.ref_simulate_3d(case, 1, threads=cores)  # page in, spawn the OpenMP team
+    t0 = time.perf_counter()
+    o.ref_simulate_3d(case, sample_steps, threads=cores)
+    elapsed = time.perf_counter() - t0
+    value = interior_updates(w) * sample_steps / elapsed / 1e9
+    return {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
+            "sample": f"{sample_steps} of {w['steps']} steps of the full {w['Nx'][0]}^3 job "
+                      f"({elapsed:.1f} s), reference kernels via oracle/_ref, OpenMP"}
+
+
+def reference_case(w: dict):
+    """The job as an oracle case: the same materials, tables and source weights."""
+    from oracle import oracle as o
+
+    Nx = w["Nx"]
+    stiff, minv = o.acoustic_materials(Nx, w["indicator"], 1.0, 1.0, 1.0, w["kappa2"], np.float32)
+    widths = tuple((w["width"], w["width"]) for _ in range(3))
+    profiles = o.pml_profiles(Nx, (1.0,) * 3, w["dt"], widths, w["width"], w["c_max"], 1e-6, 0.0,
+                              np.float32)
+    flat = lambda p: (p[0].astype(np.int64) * Nx[1] * ((Nx[2] + 31) // 32 * 32)  # noqa: E731
+                      + p[1].astype(np.int64) * ((Nx[2] + 31) // 32 * 32) + p[2]).astype(np.int32)
+    case = o.Case(Nx=Nx, R=4, coeffs=o.cell_coefficients(4, "optimized"),
+                  factors=[np.float32(2.0 * w["dt"] ** 2)] * 3, dt=w["dt"], stiff=stiff, minv=minv,
+                  widths=widths, profiles=profiles, source_lin=flat(w["source"]),
+                  signal=w["signal"], sensor_lin=flat(w["sensors"]))
+    case.source_weight = case.excitation_weights(case.source_lin)
+    return case
+
+
+def run_reference(args) -> int:
+    rank, world, _ = dist_setup()
+    if rank != 0:
+        return 0
+    w = workload(args.size, args.nt)
+    sample = args.ref_sample
+    times = []
+    from oracle import oracle as o
+
+    path = o.ref_library(3, 4, "optimized", "float32")
+    if not path.exists():
+        print(json.dumps({"impl": "reference", "unavailable": f"{path.name} was not built"}))
+        return 0
+    case = reference_case(w)
+    cores = os.cpu_count() or 1
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        o.ref_simulate_3d(case, sample, threads=cores)
+        if i >= args.warmup:
+            times.append(time.perf_counter() - t0)
+    per = sum(times) / len(times)
+    value = interior_updates(w) * sample / per / 1e9
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": per * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded layered model)",
+        "config": config_line(w, args),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
+                         "sample": f"{sample} of {w['steps']} steps of the full job per bench step"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def config_line(w: dict, args) -> dict:
+    return {"workload": "3D scalar forward with PML (layered 512^3, radius 4, 20-cell PML, "
+                        "4000 steps, 128x128 receiver plane)" if w["Nx"][0] == 512 and w["steps"] == 4000
+            else f"3D scalar forward with PML ({w['Nx'][0]}^3, radius 4, {w['width']}-cell PML, "
+                 f"{w['steps']} steps)",
+            "grid": list(w["Nx"]), "space_order": 8, "pml": w["width"], "time_steps": w["steps"],
+            "receivers": int(w["sensors"].shape[1]), "precision": "float32",
+            "parallelism": f"replicas x{args.gpus}", "l2": "inputs larger than L2 (512 MiB per field)"}
+
+
+# ------------------------------------------------------------------- our arm
+def step_kernel_ms(sim, mat_inputs, steps: int) -> float:
+    """Average duration of the dominant kernel (the fused step: fd + pml + sources +
+    refill) over `steps` back-to-back launches on the stream it runs on, by CUDA events."""
+    import torch
+
+    from cuwave_b200 import _native as nat
+    from cuwave_b200.wave import forward_ops, pml_memory, prepare_shot
+
+    dev = torch.device("cuda")
+    indicator, position, signal = mat_inputs
+    mat = sim.build_materials(indicator.clone())
+    shot = prepare_shot(sim, mat, position, signal)
+    U = torch.zeros((2, *sim.Nx_padded), dtype=sim.dtype, device=dev)
+    memory = pml_memory(sim, 3, dev)
+    ops = forward_ops(sim, mat, nat.level(U, add=0, period=2), nat.level(U, add=1, period=2),
+                      nat.level(U, add=0, period=2), shot, memory)
+    assert len(ops) == 1 and ops[0].kind == nat.OP_STEP
+    plan = sim.plan()
+    plan.march(ops, 0, 8)
+    stream = torch.cuda.current_stream()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    a.record(stream)
+    plan.march(ops, 8, steps)
+    b.record(stream)
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) / steps
+
+
+def run_ours(args) -> int:
+    import torch
+    import torch.distributed as dist
+
+    from cuwave_b200 import Source, _native as nat, simulate
+
+    rank, world, local = dist_setup()
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    w = workload(args.size, args.nt)
+    sim = make_sim(w)
+    dev = torch.device("cuda", local)
+    indicator = torch.as_tensor(w["indicator"], device=dev)
+    position = torch.as_tensor(w["source"], device=dev)
+    signal = torch.as_tensor(w["signal"], device=dev)
+    sensors = torch.as_tensor(w["sensors"], device=dev)
+    source = Source(position, signal)
+
+    def job():
+        return simulate(sim, source, indicator.clone(), sensors)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t)
+
+    for _ in range(args.warmup):
+        job()
+    barrier()
+    clocks = ClockSampler(local)
+    launches0 = nat.launches()
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        field, traces = job()
+    e1.record(stream)
+    barrier()
+    clock = clocks.stop()
+    launches = nat.launches() - launches0
+    ms = max_over_ranks(e0.elapsed_time(e1) / args.steps)
+    updates = interior_updates(w) * w["steps"]
+    value = world * updates / (ms / 1e3) / 1e9
+
+    # e2e: the public call from pinned host buffers, results copied back, every step
+    host_ind = torch.as_tensor(w["indicator"]).pin_memory()
+    host_pos = torch.as_tensor(w["source"]).pin_memory()
+    host_sig = torch.as_tensor(w["signal"]).pin_memory()
+    host_sens = torch.as_tensor(w["sensors"]).pin_memory()
+    out_field = torch.empty(tuple(w["Nx"]), dtype=torch.float32).pin_memory()
+    out_traces = torch.empty((w["steps"], w["sensors"].shape[1]), dtype=torch.float32).pin_memory()
+    h2d = sum(t.numel() * t.element_size() for t in (host_ind, host_pos, host_sig, host_sens))
+    d2h = sum(t.numel() * t.element_size() for t in (out_field, out_traces))
+
+    def e2e_job():
+        f, um = simulate(sim, Source(host_pos, host_sig), host_ind, host_sens)
+        out_field.copy_(f, non_blocking=True)
+        out_traces.copy_(um, non_blocking=True)
+
+    e2e_job()
+    barrier()
+    e2e_steps = max(1, min(args.steps, 3))
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        e2e_job()
+    e1.record(stream)
+    barrier()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1) / e2e_steps)
+    e2e_value = world * updates / (e2e_ms / 1e3) / 1e9
+
+    # the dominant kernel against the HBM roofline
+    kernel_ms = step_kernel_ms(sim, (indicator, position, signal), args.kernel_steps)
+    kernel_ms = max_over_ranks(kernel_ms)
+    bytes_per_launch = algorithmic_bytes(w)
+    achieved = bytes_per_launch / (kernel_ms / 1e3) / 1e9
+    peak, peak_kind = hbm_peak()
+    traffic = profile_traffic(w)
+
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    baseline = cpu_baseline(w, args.cpu_sample) if not args.no_cpu else None
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded layered model)",
+        "config": config_line(w, args),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
+                     "kernel": "step_kernel<float,3,4,uniform> (fd + pml + sources + refill)",
+                     "kernel_ms": kernel_ms, "algorithmic_bytes_per_launch": bytes_per_launch},
+        "cpu_baseline": baseline,
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms},
+        "gpu_launches": launches,
+        "clocks": clock,
+        "kernel_updates_per_s": interior_updates(w) / (kernel_ms / 1e3) / 1e9,
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def hbm_peak() -> tuple[float, str]:
+    path = ROOT / "MEASURED_PEAKS.json"
+    if path.exists():
+        return float(json.loads(path.read_text())["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    return 6650.0, "fallback 6.65 TB/s"
+
+
+def profile_traffic(w: dict):
+    """DRAM bytes per launch of the step kernel from the committed ncu summary, scaled to
+    this workload's units, or None when no capture was summarised."""
+    path = ROOT / "profiles" / "traffic.json"
+    if not path.exists():
+        return None
+    data = json.loads(path.read_text())
+    per_update = data.get("dram_bytes_per_interior_update")
+    return None if per_update is None else per_update * interior_updates(w)
+
+
+def main(argv=None) -> int:
+    parser = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    parser.add_argument("--gpus", type=int, default=1)
+    parser.add_argument("--steps", type=int, default=5)
+    parser.add_argument("--warmup", type=int, default=3)
+    parser.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    parser.add_argument("--size", type=int, default=512, help="grid nodes per axis (ghosts included)")
+    parser.add_argument("--nt", type=int, default=4000, help="time steps of one job")
+    parser.add_argument("--kernel-steps", type=int, default=400)
+    parser.add_argument("--cpu-sample", type=int, default=6, help="time steps the CPU baseline runs")
+    parser.add_argument("--ref-sample", type=int, default=3, help="time steps per reference bench step")
+    parser.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    args = parser.parse_args(argv)
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

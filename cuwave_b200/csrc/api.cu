@@ -94,7 +94,7 @@ cwb::DLevel to_level(const cwb_level &L, const int bytes) {
 template <typename T>
 int fill_material(const cwb_plan *p, const cwb_material &m, const T **stiff, const T **minv,
                   const T **damping, const T **prof, T &sconst, T &gconst, T &dgconst,
-                  int &flags, bool &uniform) {
+                  int &flags, bool &uniform, const bool pml) {
   uniform = m.stiff_uniform != 0;
   *stiff = static_cast<const T *>(m.stiff);
   *minv = static_cast<const T *>(m.minv);
@@ -105,7 +105,7 @@ int fill_material(const cwb_plan *p, const cwb_material &m, const T **stiff, con
     return fail(CWB_ERR_ARG, "minv is required unless derive_inertia is set");
   for (int d = 0; d < 3; ++d) {
     prof[d] = static_cast<const T *>(m.profile[d]);
-    if (d < p->geo.ndim && lined(p, d) && !prof[d])
+    if (pml && d < p->geo.ndim && lined(p, d) && !prof[d])
       return fail(CWB_ERR_ARG, "a lined axis needs its pml profile");
   }
   sconst = (T)m.stiff_value;
@@ -274,7 +274,7 @@ int translate(cwb_plan *p, const cwb_op &op, const size_t slot, cudaStream_t str
     int flags = 0;
     T dgconst;
     if ((rc = fill_material<T>(p, op.mat, &sp.stiff, &sp.minv, &sp.damping, sp.prof, sp.sconst,
-                               sp.gconst, dgconst, flags, uniform)))
+                               sp.gconst, dgconst, flags, uniform, op.flags & CWB_PML)))
       return rc;
     if (op.flags & CWB_PML) {
       flags |= cwb::K_PML;
@@ -329,7 +329,8 @@ int translate(cwb_plan *p, const cwb_op &op, const size_t slot, cudaStream_t str
     int flags = 0;
     const T *prof[3];
     if ((rc = fill_material<T>(p, op.mat, &ap.stiff, &ap.minv, &ap.damping, prof, ap.sconst,
-                               ap.gconst, ap.dgconst, flags, uniform)))
+                               ap.gconst, ap.dgconst, flags, uniform,
+                               !grad_only && (op.flags & CWB_PML))))
       return rc;
     for (int d = 0; d < 3; ++d)
       ap.prof[d] = prof[d];
@@ -394,7 +395,7 @@ int translate(cwb_plan *p, const cwb_op &op, const size_t slot, cudaStream_t str
     bool uniform;
     int flags = 0;
     if ((rc = fill_material<T>(p, op.mat, &stiff, &minv, &damping, prof, sconst, gconst,
-                               dgconst, flags, uniform)))
+                               dgconst, flags, uniform, true)))
       return rc;
     for (int d = 0; d < ndim; ++d) {
       if (!lined(p, d))

@@ -1,0 +1,472 @@
+"""Adjoint sensitivities: `sensitivity`, `reconstruction_sensitivity`, `source_sensitivity`.
+
+Same arguments and returns as cuwave `sensitivity.py` (384-497, 500-750, 1054-1111):
+`(cost, {"mass": dJ/dm, "stiff": dJ/dk}, traces, info)` with the gradients over the
+padded grid, cell-weighted and zeroed in a pml layer, or `(cost, dJ/dsignal, traces,
+info)` for the source. The adjoint marches run in the native library: the transposed
+step with the gradients fused in (CWB_OP_ADJOINT), the pml transpose (CWB_OP_PML_AUX and
+the gather inside the step) and the adjoint load (CWB_OP_LOAD).
+"""
+
+from __future__ import annotations
+
+import math
+from collections.abc import Callable
+from dataclasses import replace
+
+import numpy as np
+import torch
+
+from . import _native as nat
+from .boundary import pml_nodes
+from .wave import (
+    BFLOAT16,
+    Simulation,
+    Source,
+    as_device,
+    as_position,
+    device,
+    flatten_indices,
+    forward_ops,
+    grid_rows,
+    narrow,
+    pml_memory,
+    prepare_shot,
+    require_off_held_walls,
+    simulate,
+)
+
+# what `strip_dtype` stores the strip as, per (strip_dtype, precision) (cuwave sensitivity.py:54-58)
+STRIP_DTYPES = {
+    ("float32", "float64"): torch.float32,
+    ("bfloat16", "float32"): BFLOAT16,
+    ("bfloat16", "float64"): BFLOAT16,
+}
+# round-off growth past which a damped node is recorded rather than run backwards
+REVERSIBLE_GROWTH = {"float32": 1e2, "float64": 1e6}
+
+
+def l2_misfit(observed) -> Callable:
+    """Objective factory: J = 1/2 sum (traces - observed)^2 and its derivative (cuwave sensitivity.py:93-100)."""
+
+    def objective(traces):
+        residual = traces - as_device(observed, traces.dtype)
+        return 0.5 * float(torch.sum(residual**2)), residual
+
+    return objective
+
+
+def windowed_misfit(observed, window) -> Callable:
+    """`l2_misfit` restricted to a time window (cuwave sensitivity.py:68-84)."""
+
+    def objective(traces):
+        w = as_device(window, traces.dtype)
+        residual = w * (traces - as_device(observed, traces.dtype))
+        return 0.5 * float(torch.sum(residual**2)), w * residual
+
+    return objective
+
+
+def require_interior(sim: Simulation, position, what: str) -> None:
+    """Raise if a node of `position` sits on a ghost (cuwave sensitivity.py:103-118)."""
+    rows = grid_rows(sim, as_position(sim, position))
+    if rows.numel() == 0:
+        return
+    lo = int(rows.min())
+    if lo < 1:
+        raise ValueError(f"{what} on a ghost node: index {lo} < 1")
+    for d in range(sim.ndim):
+        hi = int(rows[d].max())
+        if hi > sim.Nx[d] - 2:
+            raise ValueError(
+                f"{what} on a ghost node: axis {d} index {hi} exceeds Nx[{d}] - 2 = {sim.Nx[d] - 2}"
+            )
+
+
+def frozen(sim: Simulation, grads: dict) -> dict:
+    """`grads` zeroed in the pml layer, assigned so a NaN cannot survive (cuwave sensitivity.py:198-205)."""
+    if sim.pml is not None:
+        layer = torch.as_tensor(pml_nodes(sim), device=next(iter(grads.values())).device)
+        for f in grads.values():
+            f[layer] = 0.0
+    return grads
+
+
+def adjoint_signal(sim: Simulation, dphi, sensors, scale: float = 1.0, delay: int = 0):
+    """dphi reversed in time over W and the source factor (cuwave sensitivity.py:272-292)."""
+    sensors = as_position(sim, sensors)
+    signal = as_device(dphi, sim.dtype).flip(0) / sim.adjoint_weights(sensors)
+    if delay:
+        signal = torch.cat((signal[delay:], torch.zeros_like(signal[:delay])))
+    return (torch.tensor(scale, dtype=sim.dtype, device=signal.device) * signal).contiguous()
+
+
+def _objective(objective, um):
+    cost, dphi = objective(um)
+    return float(cost), dphi
+
+
+def _adjoint_ops(sim, mat, P, eta, *, u_level=None, grads=None, load=None, probe=None):
+    """One adjoint step lambda^n in P[m % 2] from P[(m + 1) % 2]: pml memory, the
+    transposed update (gradients fused against `u_level` when `grads`), the load, and a
+    probe of lambda after the load."""
+    material = sim.material(mat)
+    l0 = nat.level(P, add=0, period=2)
+    l1 = nat.level(P, add=1, period=2)
+    ops = []
+    flags = 0
+    if sim.pml is not None:
+        ops.append(nat.op(nat.OP_PML_AUX, a=l1, mat=material, memory=eta))
+        flags |= nat.PML
+    fields = dict(a=l0, b=l1, mat=material, memory=eta, scale=sim.adjoint_mass_factor())
+    if grads is not None:
+        flags |= nat.GRAD
+        fields.update(c=u_level, g_mass=grads["mass"], g_stiff=grads["stiff"])
+    ops.append(nat.op(nat.OP_ADJOINT, flags=flags, **fields))
+    if load is not None:
+        lin, signal, weight = load
+        pts = nat.points(lin, signal, weight=weight)
+        if grads is not None:
+            ops.append(nat.op(nat.OP_LOAD, a=l0, c=u_level, points=pts, g_mass=grads["mass"],
+                              scale=sim.adjoint_mass_factor()))
+        else:
+            ops.append(nat.op(nat.OP_EXCITE, a=l0, points=pts))
+    if probe is not None:
+        lin, record = probe
+        ops.append(nat.op(nat.OP_RECORD, a=l0, points=nat.points(lin, record)))
+    return ops
+
+
+def sensitivity(sim: Simulation, source: Source, indicator, sensors, objective: Callable):
+    """Cost and d(cost)/d(mass, stiff) with the forward history stored (cuwave sensitivity.py:384-497).
+
+    The forward march writes every level into an (N + 2)-level history V, V[t + 2] = u^t;
+    the adjoint march steps lambda with the gradients fused against V reversed.
+    """
+    require_interior(sim, sensors, "sensor")
+    require_interior(sim, source.position, "source")
+    dev = device()
+    mat = sim.build_materials(indicator)
+    shot = prepare_shot(sim, mat, source.position, source.signal)
+    require_off_held_walls(sim, shot.position)
+    plan = sim.plan()
+    N = sim.N
+
+    # ---------------------------------------------------------------- forward pass
+    V = torch.zeros((N + 2, *sim.Nx_padded), dtype=sim.dtype, device=dev)
+    memory = pml_memory(sim, 3, dev)
+    ops = forward_ops(sim, mat, nat.level(V, add=0), nat.level(V, add=1), nat.level(V, add=2),
+                      shot, memory)
+    plan.march(ops, 0, N)
+    del memory
+    sensor_lin = flatten_indices(sim, sensors)
+    um = V[2:].reshape(N, -1)[:, sensor_lin.long()]
+    cost, dphi = _objective(objective, um)
+
+    # --------------------------------------------------------------- backward pass
+    signal = adjoint_signal(sim, dphi, sensors)
+    weight = sim.excitation_weights(mat, sensor_lin)
+    grads = sim.gradient_fields(mat)
+    P = torch.zeros((2, *sim.Nx_padded), dtype=sim.dtype, device=dev)
+    eta = pml_memory(sim, 5, dev)
+    # adjoint step m pairs lambda^n, n = N - 1 - m, with u^n = V[N + 1 - m]
+    u_level = nat.level(V, mul=-1, add=N + 1)
+    ops = _adjoint_ops(sim, mat, P, eta, u_level=u_level, grads=grads,
+                       load=(sensor_lin, signal, weight))
+    plan.march(ops, 0, N)
+    return cost, frozen(sim, sim.finalize_gradients(grads)), um, {}
+
+
+def source_sensitivity(sim: Simulation, source: Source, indicator, sensors, objective: Callable):
+    """Cost and d(cost)/d(source.signal) (cuwave sensitivity.py:1054-1111).
+
+    No forward field is stored: the gradient is lambda at the sources, reversed, times
+    the adjoint weights.
+    """
+    require_interior(sim, sensors, "sensor")
+    require_interior(sim, source.position, "source")
+    dev = device()
+    um = simulate(sim, source, indicator, sensors)[1]
+    cost, dphi = _objective(objective, um)
+    mat = sim.build_materials(indicator)
+    plan = sim.plan()
+    signal = adjoint_signal(sim, dphi, sensors)
+    sensor_lin = flatten_indices(sim, sensors)
+    weight = sim.excitation_weights(mat, sensor_lin)
+    position = as_position(sim, source.position)
+    source_lin = flatten_indices(sim, position)
+    P = torch.zeros((2, *sim.Nx_padded), dtype=sim.dtype, device=dev)
+    eta = pml_memory(sim, 5, dev)
+    lam = torch.zeros((sim.N, source_lin.numel()), dtype=sim.dtype, device=dev)
+    ops = _adjoint_ops(sim, mat, P, eta, load=(sensor_lin, signal, weight),
+                       probe=(source_lin, lam))
+    plan.march(ops, 0, sim.N)
+    gradient = lam.flip(0) * sim.adjoint_weights(position)
+    return cost, gradient.contiguous(), um, {}
+
+
+# ------------------------------------------------------------------- reconstruction
+def reversible_damping(sim: Simulation, indicator, span: int) -> np.ndarray:
+    """Damped nodes a reverse march of `span` steps can run backwards (cuwave sensitivity.py:139-157)."""
+    from scipy import ndimage
+
+    if sim.damping is None:
+        return np.zeros(sim.Nx_padded, dtype=bool)
+    minv = sim.inverse_inertia(indicator).cpu().numpy()
+    minv = ndimage.maximum_filter(minv, size=3)
+    damping = np.asarray(as_device(sim.damping, sim.dtype).cpu().numpy())
+    dt = sim.np_dtype
+    beta = dt(0.5) * dt(sim.dt) * damping * minv
+    tiny = np.finfo(sim.np_dtype).tiny
+    growth = dt(span) * np.log((dt(1.0) + beta) / np.maximum(dt(1.0) - beta, tiny))
+    bound = math.log(REVERSIBLE_GROWTH[sim.precision])
+    return (damping > 0) & (beta < 1.0) & (growth <= bound)
+
+
+def reconstruction_nodes(sim: Simulation, indicator, span: int | None = None):
+    """(strip, valid): the nodes a reverse march replays, and where it is exact (cuwave sensitivity.py:160-195).
+
+    Irreversible are the pml nodes and the damped nodes too lossy to run backwards; the
+    strip is the irreversible interior within `reach` (a Chebyshev dilation) of the
+    reversible set, in C order.
+    """
+    from scipy import ndimage
+
+    interior = np.zeros(sim.Nx_padded, dtype=bool)
+    interior[tuple(slice(1, n - 1) for n in sim.Nx)] = True
+    dev = device()
+    if sim.damping is None and sim.pml is None:
+        return torch.zeros((sim.ndim, 0), dtype=torch.int32, device=dev), torch.as_tensor(interior, device=dev)
+    reversible = interior & ~pml_nodes(sim)
+    if sim.damping is not None:
+        span = sim.N if span is None else span
+        damping = as_device(sim.damping, sim.dtype).cpu().numpy()
+        reversible &= ~(damping > 0) | reversible_damping(sim, indicator, span)
+    square = ndimage.generate_binary_structure(sim.ndim, sim.ndim)
+    reach = ndimage.binary_dilation(reversible, structure=square, iterations=sim.reach, brute_force=True)
+    strip = np.stack(np.nonzero(interior & ~reversible & reach)).astype(np.int32)
+    return torch.as_tensor(strip, device=dev), torch.as_tensor(reversible, device=dev)
+
+
+def segment_split(lo: int, hi: int, free: int) -> int:
+    """Where to snapshot segments lo .. hi with `free` slots: the binomial treeverse split
+    of Griewank & Walther (2000) (cuwave sensitivity.py:229-240)."""
+    r = 0
+    while math.comb(free + r, free) < hi - lo:
+        r += 1
+    return max(lo + 1, hi - math.comb(free - 1 + r, free - 1))
+
+
+def checkpoint_schedule(segments: int, slots: int) -> list[tuple]:
+    """Treeverse over `segments` with `slots` snapshots past the initial state (cuwave sensitivity.py:243-269).
+
+    Actions in order: ("restore", k), ("store", k), ("drop", k), ("advance", a, b) and
+    ("leaf", k), which replays segment k forwards and reverses it.
+    """
+    actions = []
+
+    def reverse(lo, hi, free):
+        while hi - lo > 1:
+            if free == 0:
+                for k in range(hi - 1, lo, -1):
+                    actions.extend((("restore", lo), ("advance", lo, k), ("leaf", k)))
+                break
+            mid = segment_split(lo, hi, free)
+            actions.extend((("restore", lo), ("advance", lo, mid), ("store", mid)))
+            reverse(mid, hi, free - 1)
+            actions.append(("drop", mid))
+            hi = mid
+        actions.extend((("restore", lo), ("leaf", lo)))
+
+    reverse(0, segments, slots)
+    return actions
+
+
+def _store_code(sim: Simulation, stored) -> int:
+    if stored == sim.dtype:
+        return nat.STORE_NATIVE
+    return nat.STORE_BF16 if stored == BFLOAT16 else nat.STORE_F32
+
+
+def reconstruction_sensitivity(sim: Simulation, source: Source, indicator, sensors,
+                               objective: Callable, strip_dtype: str | None = None,
+                               checkpoints: int | None = None):
+    """Cost and gradients as `sensitivity`, marching the forward field backwards behind a
+    recorded strip instead of storing it (cuwave sensitivity.py:500-750).
+
+    The lossless recursion run with its outer slots swapped steps the field backwards
+    (a reversible damping negated); the nodes it cannot reverse (the pml layer, strong
+    damping) are recorded each step over the strip that shields the rest, and replayed
+    on the way back. With `checkpoints` the run is cut into segments replayed from
+    snapshots on the treeverse schedule, so memory no longer grows with N.
+
+    Returns (cost, grads, traces, info) with info = {"strip", "drift", "segment", "sweeps"}.
+    """
+    require_interior(sim, sensors, "sensor")
+    require_interior(sim, source.position, "source")
+    if checkpoints is not None and checkpoints < 0:
+        raise ValueError(f"checkpoints must be non-negative: {checkpoints}")
+    stored = STRIP_DTYPES.get((strip_dtype, sim.precision), sim.dtype)
+    if strip_dtype is not None and stored == sim.dtype:
+        raise ValueError(
+            f"strip_dtype {strip_dtype!r} is not narrower than {sim.precision}: "
+            f"use 'bfloat16', or 'float32' under float64"
+        )
+    dev = device()
+    N = sim.N
+    mat = sim.build_materials(indicator)
+    shot = prepare_shot(sim, mat, source.position, source.signal)
+    require_off_held_walls(sim, shot.position)
+    plan = sim.plan()
+    itemsize = torch.empty(0, dtype=sim.dtype).element_size()
+    stored_size = torch.empty(0, dtype=stored).element_size()
+
+    U = torch.zeros((3, *sim.Nx_padded), dtype=sim.dtype, device=dev)
+    memory = pml_memory(sim, 3, dev)
+    memory_list = [m for m in memory if m is not None]
+    snapshot_bytes = 2 * U[0].numel() * itemsize + sum(m.numel() * itemsize for m in memory_list)
+    strip, valid = reconstruction_nodes(sim, indicator)
+    segment = N
+    if checkpoints is not None and strip.shape[1]:
+        row_bytes = 2 * strip.shape[1] * stored_size
+        segment = min(N, max(2, snapshot_bytes // row_bytes))
+    if segment < N:
+        strip, valid = reconstruction_nodes(sim, indicator, segment)
+    if not bool(valid.any()):
+        raise ValueError(
+            "damping too strong to reverse covers every interior node, so there is nothing "
+            "to reconstruct; set checkpoints, damp only the faces with sponge, or use sensitivity"
+        )
+    num_strip = int(strip.shape[1])
+    starts = list(range(0, N, segment)) + [N]
+    lin_strip = flatten_indices(sim, strip) if num_strip else None
+    store = _store_code(sim, stored)
+
+    # backwards the layer sits behind the strip, and a reversible damping is negated
+    back = replace(sim, pml=None)
+    back_mat = dict(mat)
+    if sim.damping is not None:
+        back_mat["damping"] = torch.where(valid, -mat["damping"], mat["damping"]).contiguous()
+    back_mat["profiles"] = [None, None, None]
+    back_weight = back.excitation_weights(back_mat, shot.lin)
+    back_shot = replace(shot, weight=back_weight)
+
+    sensor_lin = flatten_indices(sim, sensors)
+    sensor_weight = sim.excitation_weights(mat, sensor_lin)
+    um = torch.zeros((N, sensor_lin.numel()), dtype=sim.dtype, device=dev)
+    P = torch.zeros((2, *sim.Nx_padded), dtype=sim.dtype, device=dev)
+    eta = pml_memory(sim, 5, dev)
+    grads = sim.gradient_fields(mat)
+    snapshots = {}
+    state = {"recorded": 0, "steps": 0}
+    grad_factors = [float(sim.np_dtype(float(f) / sim.dt**2)) for f in sim.step_factors()]
+
+    def slot(i, mul=1, add=0):
+        return nat.level(U, mul=mul, add=add, period=3)
+
+    # ------------------------------------------------------------ forward pass
+    def advance(a, b, buffer=None):
+        records = []
+        if a == state["recorded"]:
+            records.append((sensor_lin, um, 1, 0, nat.STORE_NATIVE))
+            state["recorded"] = b
+        if buffer is not None:
+            # buffer row r holds u^(seg_start - 2 + r); step t writes row t - seg_start + 2
+            records.append((lin_strip, buffer[0], 1, buffer[1], store))
+        ops = forward_ops(sim, mat, slot(0, add=0), slot(0, add=1), slot(0, add=2), shot,
+                          memory, records=records)
+        state["steps"] += b - a
+        plan.march(ops, a, b - a)
+
+    def slots_at(t):
+        return U[t % 3], U[(t + 1) % 3]
+
+    def store_snapshot(k):
+        snapshots[k] = [f.clone() for f in (*slots_at(starts[k]), *memory_list)]
+
+    def restore(k):
+        for f, saved in zip((*slots_at(starts[k]), *memory_list), snapshots.get(k, ())):
+            f.copy_(saved)
+        if k == 0:
+            for f in (*slots_at(0), *memory_list):
+                f.zero_()
+
+    # ----------------------------------------------------------- backward pass
+    # triplet(m) = (u^(n-2), u^(n-1), u^n), n = N - 1 - m, sit in U[(N + 2 - m) % 3],
+    # U[(N - m) % 3], U[(N + 1 - m) % 3]
+    material = sim.material(mat)
+    back_material = back.material(back_mat)
+
+    def adjoint_ops(offset):
+        """Adjoint step m + offset: lambda in P[(m + offset) % 2]."""
+        l0 = nat.level(P, add=offset, period=2)
+        l1 = nat.level(P, add=offset + 1, period=2)
+        ops = []
+        flags = 0
+        if sim.pml is not None:
+            ops.append(nat.op(nat.OP_PML_AUX, a=l1, mat=material, memory=eta))
+            flags = nat.PML
+        ops.append(nat.op(nat.OP_ADJOINT, flags=flags, a=l0, b=l1, mat=material, memory=eta,
+                          scale=sim.adjoint_mass_factor()))
+        ops.append(nat.op(nat.OP_EXCITE, a=l0,
+                          points=nat.points(sensor_lin, state["signal"], weight=sensor_weight,
+                                            row_add=offset)))
+        # the triplet of step m + offset and the lambda just stepped
+        o_ = offset
+        ops.append(nat.op(nat.OP_GRADIENT, a=slot(0, mul=-1, add=N + 2 - o_),
+                          b=slot(0, mul=-1, add=N - o_), c=slot(0, mul=-1, add=N + 1 - o_),
+                          d=l0, mat=material, g_mass=grads["mass"], g_stiff=grads["stiff"],
+                          scale=sim.adjoint_mass_factor(), factors=grad_factors))
+        return ops
+
+    def leaf(k):
+        s, e = starts[k], starts[k + 1]
+        buffer = None
+        if num_strip:
+            buf = torch.zeros((e - s + 2, num_strip), dtype=stored, device=dev)
+            if s:
+                for row, f in enumerate(slots_at(s)):
+                    buf[row] = narrow(f.reshape(-1)[lin_strip.long()], stored)
+            buffer = (buf, 2 - s)
+        advance(s, e, buffer)
+        if "signal" not in state:
+            state["cost"], dphi = _objective(objective, um)
+            state["signal"] = adjoint_signal(sim, dphi, sensors)
+        m0, m1 = N - e, N - s
+        if not s:
+            state["seed"] = float(torch.linalg.vector_norm(U[(N + 1 - m0) % 3] * valid))
+        plan.march(adjoint_ops(0), m0, 1)
+        if e - s > 1:
+            # reverse step m beside adjoint step m + 1 (sequential here: they meet only
+            # in the gradient)
+            replay = None
+            if num_strip:
+                # u^(n-3), n = N - 1 - m, sits in row N - 2 - m - s of the buffer
+                replay = nat.points(lin_strip, buf, row_mul=-1, row_add=N - 2 - s, store=store)
+            ops = forward_ops(back, back_mat, slot(0, mul=-1, add=N), slot(0, mul=-1, add=N + 2),
+                              slot(0, mul=-1, add=N + 1), back_shot, [None, None, None],
+                              replay=replay, source_row=(-1, N - 2), fold=False)
+            ops[0].mat = back_material
+            ops += adjoint_ops(1)
+            plan.march(ops, m0, e - s - 1)
+
+    for action, *segs in checkpoint_schedule(len(starts) - 1, checkpoints or 0):
+        if action == "advance":
+            advance(starts[segs[0]], starts[segs[1]])
+        elif action == "store":
+            store_snapshot(segs[0])
+        elif action == "restore":
+            restore(segs[0])
+        elif action == "drop":
+            del snapshots[segs[0]]
+        else:
+            leaf(segs[0])
+
+    grads = sim.finalize_gradients(grads)
+    outside = ~valid
+    for f in grads.values():
+        f[outside] = 0.0
+    seed = state["seed"]
+    drift = float(torch.linalg.vector_norm(U[0] * valid)) / seed if seed > 0.0 else float("inf")
+    info = {"strip": num_strip, "drift": drift, "segment": segment, "sweeps": state["steps"] / N}
+    return state["cost"], grads, um, info

@@ -151,6 +151,8 @@ class Simulation:
 
     def pml_slabs(self) -> list[tuple]:
         """(d, lo, hi, profile) per lined axis (cuwave wave.py:587-595)."""
+        if self.pml is None:
+            return []
         widths, profiles = pml_widths(self), pml_profiles(self)
         return [
             (d, lo, hi, profile)
@@ -237,6 +239,16 @@ def as_position(sim: Simulation, position) -> torch.Tensor:
         raise ValueError(
             f"position needs {sim.node_rows} rows in {sim.ndim}D, not {tuple(pos.shape)}"
         )
+    if pos.numel():
+        # every node a kernel reads or writes through a flat index must be on the grid
+        lo = pos.amin(dim=1).cpu()
+        hi = pos.amax(dim=1).cpu()
+        for d in range(sim.ndim):
+            if int(lo[d]) < 0 or int(hi[d]) > sim.Nx[d] - 1:
+                raise ValueError(
+                    f"position off the grid on axis {d}: [{int(lo[d])}, {int(hi[d])}] "
+                    f"outside [0, {sim.Nx[d] - 1}]"
+                )
     return pos
 
 

@@ -390,3 +390,46 @@ def l2(observed):
         residual = traces - observed
         return 0.5 * float(np.sum(residual**2)), residual
     return objective
+
+
+# ------------------------------------------------------ the reference's own kernels
+REF_DIR = HERE / "_ref"
+
+
+def ref_library(ndim=3, radius=4, stencil="optimized", precision="float32") -> Path:
+    tag = "f32" if precision == "float32" else "f64"
+    return REF_DIR / f"libref{ndim}d_r{radius}_{stencil}_{tag}.so"
+
+
+def ref_simulate_3d(case: "Case", N: int, threads: int | None = None):
+    """The reference's own fd/pml/excitation/refill/record kernels (built by ref_build.py
+    from its sources) stepped N times on a 3D Neumann case; returns (field, traces)."""
+    path = ref_library(3, case.R, "optimized", "float32" if case.dtype == np.float32 else "float64")
+    if not path.exists():
+        raise FileNotFoundError(f"{path.name} is not built: run oracle/ref_build.py")
+    if threads is not None:
+        os.environ["OMP_NUM_THREADS"] = str(threads)
+    lib = ctypes.CDLL(str(path))
+    n0, n1, n2 = case.Nx
+    U = np.zeros((2, *case.shape), case.dtype)
+    lo = hi = 0
+    aux_parts, prof_parts = [], []
+    if case.widths is not None:
+        lo, hi = case.widths[0]
+        for d in range(3):
+            plane = int(np.prod([case.shape[e] for e in range(3) if e != d]))
+            aux_parts.append(np.zeros(3 * (lo + hi) * plane, case.dtype))
+            prof_parts.append(case.profiles[d].ravel())
+    aux = np.concatenate(aux_parts) if aux_parts else np.zeros(1, case.dtype)
+    prof = np.concatenate(prof_parts) if prof_parts else np.zeros(1, case.dtype)
+    um = np.zeros((N, case.sensor_lin.size), case.dtype)
+    f = np.ascontiguousarray(case.f[:3])
+    signal = np.ascontiguousarray(case.signal[:N], case.dtype)
+    rc = lib.ref_simulate_3d(
+        n0, n1, n2, case.shape[2], _p(U), _p(case.stiff), _p(case.minv), int(case.derive), _p(f),
+        lo, hi, _p(aux), _p(prof), _p(case.source_lin), _p(case.source_weight), _p(signal),
+        int(case.source_lin.size), _p(case.sensor_lin), _p(um), int(case.sensor_lin.size), N,
+    )
+    if rc:
+        raise RuntimeError("ref_simulate_3d refused the case")
+    return U[(N - 1) % 2], um

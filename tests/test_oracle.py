@@ -1,0 +1,57 @@
+"""The CPU oracle against the reference's own outputs (tests/golden, make_golden.py).
+
+The oracle restates the reference's kernels in C and its drivers in numpy; run here
+it reproduces the reference's CPU fallback bit for bit, forward and adjoint.
+"""
+
+import numpy as np
+import pytest
+
+import cases
+from oracle import oracle as o
+
+
+@pytest.mark.parametrize("name", cases.FORWARD)
+def test_forward_matches_reference(name):
+    fx = cases.load(name)
+    case = cases.oracle_case(fx)
+    field, traces = case.forward(int(fx["N"]))
+    Nx = tuple(int(n) for n in fx["Nx"])
+    np.testing.assert_array_equal(field[tuple(slice(0, n) for n in Nx)], fx["field"])
+    np.testing.assert_array_equal(traces, fx["traces"])
+
+
+@pytest.mark.parametrize("name", cases.GRADIENT)
+def test_gradients_match_reference(name):
+    fx = cases.load(name)
+    case = cases.oracle_case(fx)
+    objective = o.l2(fx["observed"])
+    cost, grads, traces = case.sensitivity(int(fx["N"]), objective)
+    np.testing.assert_array_equal(traces, fx["traces"])
+    np.testing.assert_array_equal(grads["mass"], fx["g_mass"])
+    np.testing.assert_array_equal(grads["stiff"], fx["g_stiff"])
+    assert cost == pytest.approx(float(fx["cost"]), rel=1e-5)
+    _, gradient, _ = case.source_sensitivity(int(fx["N"]), objective)
+    np.testing.assert_array_equal(gradient, fx["source_gradient"])
+
+
+def test_oracle_tables_match_reference():
+    tables = np.load(cases.GOLDEN / "stencils.npz")
+    for R in range(1, 9):
+        for stencil in ("taylor", "optimized"):
+            np.testing.assert_allclose(
+                o.cell_coefficients(R, stencil), tables[f"coeffs_{stencil}_{R}"], rtol=1e-12, atol=1e-15
+            )
+            assert o.stable_dt((1.0, 0.5), 1.7, 2 * R, stencil) == pytest.approx(
+                float(tables[f"stable_dt_{stencil}_{R}"]), rel=1e-12
+            )
+
+
+def test_planted_error_is_caught():
+    """A checker that cannot fail proves nothing: a wrong coefficient must show."""
+    fx = cases.load("fwd2d_r4")
+    case = cases.oracle_case(fx)
+    case.w[1] *= 1.001
+    field, _ = case.forward(int(fx["N"]))
+    Nx = tuple(int(n) for n in fx["Nx"])
+    assert not np.array_equal(field[tuple(slice(0, n) for n in Nx)], fx["field"])
