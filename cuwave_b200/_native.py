@@ -45,6 +45,7 @@ class Level(ctypes.Structure):
         ("mul", ctypes.c_int32),
         ("add", ctypes.c_int32),
         ("period", ctypes.c_int32),
+        ("count", ctypes.c_int32),
     ]
 
 
@@ -181,12 +182,13 @@ def ptr(tensor: torch.Tensor | None) -> int | None:
 
 def level(stack: torch.Tensor, *, mul: int = 1, add: int = 0, period: int = 0) -> Level:
     """Level `(mul * t + add) mod period` (no wrap for period 0) of a stack of fields."""
-    return Level(stack.data_ptr(), int(stack[0].numel()), int(mul), int(add), int(period))
+    return Level(stack.data_ptr(), int(stack[0].numel()), int(mul), int(add), int(period),
+                 int(stack.shape[0]))
 
 
 def fixed(field: torch.Tensor) -> Level:
     """A level that is the same field every step."""
-    return Level(field.data_ptr(), 0, 0, 0, 0)
+    return Level(field.data_ptr(), 0, 0, 0, 0, 1)
 
 
 def points(lin: torch.Tensor | None, record: torch.Tensor | None, *, weight=None,

@@ -8,8 +8,12 @@
 #include <string>
 #include <vector>
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include "cuwave_b200.h"
 #include "launch.cuh"
+#include "step_tma.cuh"
 
 namespace {
 
@@ -43,6 +47,8 @@ struct cwb_plan {
   cwb_grid grid;
   cwb::Geometry geo;
   int *ctr = nullptr;
+  int *err = nullptr;  // raised by a kernel whose bounded wait ran out
+  bool tma = true;     // stage planes with tensor-map copies where the layout allows
   cudaStream_t lane = nullptr;
   cudaEvent_t fork = nullptr, join = nullptr;
   int sms = 148;
@@ -72,6 +78,17 @@ int chunk_for(const cwb_plan *p, const int plane_blocks) {
 void stencil_grid(const cwb_plan *p, dim3 &grid, int &chunk) {
   int bx, by;
   cwb::block_shape(p->geo.ndim, bx, by);
+  const Geometry &g = p->geo;
+  const int F = g.ndim - 1;
+  const int gx = (g.ext[F] + bx - 1) / bx;
+  const int gy = g.ndim == 3 ? (g.n[1] + by - 1) / by : 1;
+  chunk = chunk_for(p, gx * gy);
+  const int gz = (g.n[0] - 2 + chunk - 1) / chunk;
+  grid = g.ndim == 3 ? dim3(gx, gy, gz) : dim3(gx, gz, 1);
+}
+
+// the TMA step's grid: BX x BY tiles of the plane, chunks of axis 0
+void tma_grid(const cwb_plan *p, const int bx, const int by, dim3 &grid, int &chunk) {
   const Geometry &g = p->geo;
   const int F = g.ndim - 1;
   const int gx = (g.ext[F] + bx - 1) / bx;
@@ -132,7 +149,8 @@ using Launch = std::function<cudaError_t(cudaStream_t, bool)>;
 // the folded sources of a step, listed per block of its grid
 template <typename T>
 int build_sources(cwb_plan *p, const size_t slot, const cwb_points &pts, const dim3 grid,
-                  const int chunk, cudaStream_t stream, const int **start, const int4 **entry) {
+                  const int chunk, const int bx, const int by, cudaStream_t stream,
+                  const int **start, const int4 **entry) {
   const Geometry &g = p->geo;
   const int nblocks = grid.x * grid.y * grid.z;
   std::vector<int> lin(pts.num);
@@ -141,8 +159,6 @@ int build_sources(cwb_plan *p, const size_t slot, const cwb_points &pts, const d
                              cudaMemcpyDeviceToHost, stream));
     CWB_CUDA(cudaStreamSynchronize(stream));
   }
-  int bx, by;
-  cwb::block_shape(g.ndim, bx, by);
   const int F = g.ndim - 1;
   std::vector<std::vector<int4>> per(nblocks);
   for (int j = 0; j < pts.num; ++j) {
@@ -199,6 +215,116 @@ int build_sources(cwb_plan *p, const size_t slot, const cwb_points &pts, const d
   return CWB_OK;
 }
 
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void *ptr = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(ptr);
+  }
+  return fn;
+}
+
+// a tiled tensor map, dims fastest first, strides in bytes of dims 1 .. rank - 1
+template <typename T>
+bool encode_map(CUtensorMap *map, const void *base, const int rank, const cuuint64_t *dims,
+                const cuuint64_t *strides, const cuuint32_t *box) {
+  const auto fn = encode_fn();
+  if (!fn || (reinterpret_cast<uintptr_t>(base) & 15))
+    return false;
+  for (int i = 0; i < rank - 1; ++i)
+    if (strides[i] % 16 || strides[i] >= (1ULL << 40))
+      return false;
+  const cuuint32_t elem[5] = {1, 1, 1, 1, 1};
+  const CUresult r = fn(map, sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64,
+                        rank, const_cast<void *>(base), dims, strides, box, elem,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                        CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
+template <typename T, int NDIM>
+int tma_halo_nd(const int R) {
+  switch (R) {
+  case 1: return cwb::step_tma_halo<T, NDIM, 1>();
+  case 2: return cwb::step_tma_halo<T, NDIM, 2>();
+  case 3: return cwb::step_tma_halo<T, NDIM, 3>();
+  case 4: return cwb::step_tma_halo<T, NDIM, 4>();
+  case 5: return cwb::step_tma_halo<T, NDIM, 5>();
+  case 6: return cwb::step_tma_halo<T, NDIM, 6>();
+  case 7: return cwb::step_tma_halo<T, NDIM, 7>();
+  default: return cwb::step_tma_halo<T, NDIM, 8>();
+  }
+}
+
+template <typename T, int NDIM>
+cudaError_t step_tma_nd(const cwb::StepTmaParams<T> &p, const int R, const bool u,
+                        const dim3 grid, cudaStream_t s) {
+  switch (R) {
+  case 1: return cwb::step_tma_unit<T, NDIM, 1>(p, u, grid, s);
+  case 2: return cwb::step_tma_unit<T, NDIM, 2>(p, u, grid, s);
+  case 3: return cwb::step_tma_unit<T, NDIM, 3>(p, u, grid, s);
+  case 4: return cwb::step_tma_unit<T, NDIM, 4>(p, u, grid, s);
+  case 5: return cwb::step_tma_unit<T, NDIM, 5>(p, u, grid, s);
+  case 6: return cwb::step_tma_unit<T, NDIM, 6>(p, u, grid, s);
+  case 7: return cwb::step_tma_unit<T, NDIM, 7>(p, u, grid, s);
+  case 8: return cwb::step_tma_unit<T, NDIM, 8>(p, u, grid, s);
+  }
+  return cudaErrorInvalidValue;
+}
+
+// The tensor maps of a TMA step: the level stacks of operands b (box with halo) and a,
+// and 1/m. False where the layout does not allow tensor-map copies.
+template <typename T>
+bool tma_maps(const cwb_plan *p, const cwb_op &op, const bool derive, const T *minv,
+              cwb::StepTmaParams<T> &tp) {
+  const cwb::Geometry &g = p->geo;
+  const int nd = g.ndim, F = nd - 1, R = p->grid.radius;
+  const int H = nd == 3 ? tma_halo_nd<T, 3>(R) : tma_halo_nd<T, 2>(R);
+  const cuuint64_t ext = g.ext[F], nm = nd == 3 ? g.n[1] : 1, n0 = g.n[0];
+  const cuuint64_t row = ext * sizeof(T), plane = row * nm;
+  const int bx = nd == 3 ? cwb::TMA_BX3 : cwb::TMA_BX2, by = nd == 3 ? cwb::TMA_BY3 : 1;
+  const int hy = nd == 3 ? R : 0;
+  for (const cwb_level *L : {&op.b, &op.a})
+    if (L->count < 1 || (L->period > 0 && L->period > L->count))
+      return false;
+  {
+    const cuuint64_t dims[4] = {ext, nm, n0, (cuuint64_t)op.b.count};
+    const cuuint64_t strides[3] = {row, plane, (cuuint64_t)op.b.stride * sizeof(T)};
+    const cuuint32_t box[4] = {(cuuint32_t)(bx + 2 * H), (cuuint32_t)(by + 2 * hy), 1, 1};
+    if (op.b.count > 1 && op.b.stride * (long long)sizeof(T) < (long long)(plane * n0))
+      return false;
+    if (!encode_map<T>(&tp.map_u1, op.b.base, 4, dims, strides, box))
+      return false;
+  }
+  {
+    const cuuint64_t dims[4] = {ext, nm, n0, (cuuint64_t)op.a.count};
+    const cuuint64_t strides[3] = {row, plane, (cuuint64_t)op.a.stride * sizeof(T)};
+    const cuuint32_t box[4] = {(cuuint32_t)bx, (cuuint32_t)by, 1, 1};
+    if (op.a.count > 1 && op.a.stride * (long long)sizeof(T) < (long long)(plane * n0))
+      return false;
+    if (!encode_map<T>(&tp.map_u0, op.a.base, 4, dims, strides, box))
+      return false;
+  }
+  if (!derive) {
+    const cuuint64_t dims[3] = {ext, nm, n0};
+    const cuuint64_t strides[2] = {row, plane};
+    const cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)by, 1};
+    if (!encode_map<T>(&tp.map_minv, minv, 3, dims, strides, box))
+      return false;
+  } else {
+    tp.map_minv = tp.map_u0;  // never read
+  }
+  tp.level_u1[0] = op.b.mul, tp.level_u1[1] = op.b.add, tp.level_u1[2] = op.b.period;
+  tp.level_u0[0] = op.a.mul, tp.level_u0[1] = op.a.add, tp.level_u0[2] = op.a.period;
+  return true;
+}
+
 template <typename T, int NDIM>
 cudaError_t step_nd(const cwb::StepParams<T> &p, const int R, const bool u, const dim3 grid,
                     cudaStream_t s) {
@@ -238,6 +364,12 @@ cudaError_t step_dispatch(const cwb::StepParams<T> &p, const int ndim, const int
 }
 
 template <typename T>
+cudaError_t step_tma_dispatch(const cwb::StepTmaParams<T> &p, const int ndim, const int R,
+                              const bool u, const dim3 grid, cudaStream_t s) {
+  return ndim == 3 ? step_tma_nd<T, 3>(p, R, u, grid, s) : step_tma_nd<T, 2>(p, R, u, grid, s);
+}
+
+template <typename T>
 cudaError_t adjoint_dispatch(const cwb::AdjointParams<T> &p, const int ndim, const int R,
                              const bool u, const int mode, const dim3 grid, cudaStream_t s) {
   return ndim == 3 ? adjoint_nd<T, 3>(p, R, u, mode, grid, s)
@@ -265,8 +397,9 @@ int translate(cwb_plan *p, const cwb_op &op, const size_t slot, cudaStream_t str
     if ((rc = check_level(op.a, "a")) || (rc = check_level(op.b, "b")) ||
         (rc = check_level(op.c, "c")))
       return rc;
-    cwb::StepParams<T> sp;
-    std::memset(&sp, 0, sizeof sp);
+    cwb::StepTmaParams<T> tp;
+    std::memset(&tp, 0, sizeof tp);
+    cwb::StepParams<T> &sp = tp.s;
     sp.g = g;
     fill_weights(p, sp.w, sp.f);
     sp.dt = (T)p->grid.dt;
@@ -285,8 +418,17 @@ int translate(cwb_plan *p, const cwb_op &op, const size_t slot, cudaStream_t str
           return fail(CWB_ERR_ARG, "a lined axis needs its pml memory");
       }
     }
+    const bool tma = p->tma && tma_maps<T>(p, op, flags & cwb::K_DERIVE, sp.minv, tp);
     dim3 grid;
-    stencil_grid(p, grid, sp.chunk);
+    int bx, by;
+    if (tma) {
+      bx = ndim == 3 ? cwb::TMA_BX3 : cwb::TMA_BX2;
+      by = ndim == 3 ? cwb::TMA_BY3 : 1;
+      tma_grid(p, bx, by, grid, sp.chunk);
+    } else {
+      cwb::block_shape(ndim, bx, by);
+      stencil_grid(p, grid, sp.chunk);
+    }
     if (op.flags & CWB_FOLD_REFILL) {
       flags |= cwb::K_REFILL;
       sp.refill = p->grid.neumann | p->grid.dirichlet;
@@ -295,8 +437,8 @@ int translate(cwb_plan *p, const cwb_op &op, const size_t slot, cudaStream_t str
       flags |= cwb::K_SRC;
       if (!op.points.weight || !op.points.record)
         return fail(CWB_ERR_ARG, "folded sources need weights and a signal");
-      if ((rc = build_sources<T>(p, slot, op.points, grid, sp.chunk, stream, &sp.src_start,
-                                 &sp.src_entry)))
+      if ((rc = build_sources<T>(p, slot, op.points, grid, sp.chunk, bx, by, stream,
+                                 &sp.src_start, &sp.src_entry)))
         return rc;
       sp.src_weight = static_cast<const T *>(op.points.weight);
       sp.signal = static_cast<const T *>(op.points.record);
@@ -309,12 +451,22 @@ int translate(cwb_plan *p, const cwb_op &op, const size_t slot, cudaStream_t str
     sp.u1 = to_level(op.b, bytes);
     sp.u2 = to_level(op.c, bytes);
     sp.ctr = p->ctr;
-    out.push_back([sp, ndim, R, uniform, grid](cudaStream_t s, bool adv) {
-      cwb::StepParams<T> q = sp;
-      if (adv)
-        q.flags |= cwb::K_ADV;
-      return step_dispatch<T>(q, ndim, R, uniform, grid, s);
-    });
+    tp.err = p->err;
+    if (tma) {
+      out.push_back([tp, ndim, R, uniform, grid](cudaStream_t s, bool adv) {
+        cwb::StepTmaParams<T> q = tp;
+        if (adv)
+          q.s.flags |= cwb::K_ADV;
+        return step_tma_dispatch<T>(q, ndim, R, uniform, grid, s);
+      });
+    } else {
+      out.push_back([sp, ndim, R, uniform, grid](cudaStream_t s, bool adv) {
+        cwb::StepParams<T> q = sp;
+        if (adv)
+          q.flags |= cwb::K_ADV;
+        return step_dispatch<T>(q, ndim, R, uniform, grid, s);
+      });
+    }
     return CWB_OK;
   }
   case CWB_OP_ADJOINT:
@@ -520,6 +672,7 @@ int march(cwb_plan *p, const cwb_op *ops, const int nops, const int t0, const in
   CWB_CUDA(cudaEventRecord(p->fork, user));
   CWB_CUDA(cudaStreamWaitEvent(p->lane, p->fork, 0));
   cudaStream_t s = p->lane;
+  CWB_CUDA(cudaMemsetAsync(p->err, 0, sizeof(int), s));
   CWB_CUDA(cwb::launch_set_counter(p->ctr, t0, s));
   ++g_launches;
   int done = 0;
@@ -555,6 +708,12 @@ int march(cwb_plan *p, const cwb_op *ops, const int nops, const int t0, const in
   }
   CWB_CUDA(cudaEventRecord(p->join, s));
   CWB_CUDA(cudaStreamWaitEvent(user, p->join, 0));
+  // a bounded wait that ran out leaves its step incomplete: report it
+  int err = 0;
+  CWB_CUDA(cudaMemcpyAsync(&err, p->err, sizeof(int), cudaMemcpyDeviceToHost, s));
+  CWB_CUDA(cudaStreamSynchronize(s));
+  if (err)
+    return fail(CWB_ERR_CUDA, "a staged tile never arrived: the step was abandoned");
   return CWB_OK;
 }
 
@@ -623,7 +782,10 @@ int cwb_plan_create(const cwb_grid *grid, cwb_plan **out) {
   cudaDeviceGetAttribute(&p->sms, cudaDevAttrMultiProcessorCount, dev);
   if (const char *env = std::getenv("CWB_CHUNK"))
     p->chunk_override = std::atoi(env);
+  if (const char *env = std::getenv("CWB_NO_TMA"))
+    p->tma = std::atoi(env) == 0;
   if (cudaMalloc(&p->ctr, 2 * sizeof(int)) != cudaSuccess ||
+      cudaMalloc(&p->err, sizeof(int)) != cudaSuccess ||
       cudaStreamCreateWithFlags(&p->lane, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreateWithFlags(&p->fork, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&p->join, cudaEventDisableTiming) != cudaSuccess) {
@@ -632,6 +794,7 @@ int cwb_plan_create(const cwb_grid *grid, cwb_plan **out) {
                                    cudaGetErrorString(cudaGetLastError()));
   }
   cudaMemset(p->ctr, 0, 2 * sizeof(int));
+  cudaMemset(p->err, 0, sizeof(int));
   *out = p;
   return CWB_OK;
 }
@@ -649,6 +812,8 @@ int cwb_plan_destroy(cwb_plan *p) {
   }
   if (p->ctr)
     cudaFree(p->ctr);
+  if (p->err)
+    cudaFree(p->err);
   if (p->fork)
     cudaEventDestroy(p->fork);
   if (p->join)

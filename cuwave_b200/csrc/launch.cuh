@@ -18,6 +18,18 @@ inline void block_shape(const int ndim, int &bx, int &by) {
 
 template <typename T, int NDIM, int R>
 cudaError_t step_unit(const StepParams<T> &p, bool uniform, dim3 grid, cudaStream_t stream);
+template <typename T>
+struct StepTmaParams;
+
+// the TMA step: BX x BY tile, each thread RY rows (3D); a BX-wide row (2D)
+constexpr int TMA_BX3 = 32, TMA_BY3 = 16, TMA_RY3 = 2, TMA_BX2 = 128;
+
+template <typename T, int NDIM, int R>
+cudaError_t step_tma_unit(const StepTmaParams<T> &p, bool uniform, dim3 grid,
+                          cudaStream_t stream);
+template <typename T, int NDIM, int R>
+int step_tma_halo();  // the x halo of the staged box, a multiple of 16 bytes
+
 template <typename T, int NDIM, int R>
 cudaError_t adjoint_unit(const AdjointParams<T> &p, bool uniform, int mode, dim3 grid,
                          cudaStream_t stream);

@@ -3,6 +3,7 @@
 #include "adjoint.cuh"
 #include "launch.cuh"
 #include "step.cuh"
+#include "step_tma.cuh"
 
 #if !defined(CWB_REAL) || !defined(CWB_NDIM) || !defined(CWB_RADIUS)
 #error "unit.cu is compiled with CWB_REAL, CWB_NDIM and CWB_RADIUS"
@@ -48,6 +49,32 @@ cudaError_t adjoint_one(const AdjointParams<T> &p, const dim3 grid, cudaStream_t
 
 }  // namespace
 
+template <typename T, int NDIM, int R, bool U>
+cudaError_t step_tma_one(const StepTmaParams<T> &p, const dim3 grid, cudaStream_t s) {
+  constexpr int BX = NDIM == 3 ? TMA_BX3 : TMA_BX2;
+  constexpr int BY = NDIM == 3 ? TMA_BY3 : 1;
+  constexpr int RY = NDIM == 3 ? TMA_RY3 : 1;
+  const size_t smem = TmaShape<T, NDIM, R, BX, BY>::SMEM;
+  const auto k = step_tma_kernel<T, NDIM, R, U, BX, BY, RY>;
+  cudaError_t e = allow_smem(k, smem);
+  if (e != cudaSuccess)
+    return e;
+  k<<<grid, dim3(BX, BY / RY), smem, s>>>(p);
+  return cudaGetLastError();
+}
+
+template <typename T, int NDIM, int R>
+cudaError_t step_tma_unit(const StepTmaParams<T> &p, const bool uniform, const dim3 grid,
+                          cudaStream_t stream) {
+  return uniform ? step_tma_one<T, NDIM, R, true>(p, grid, stream)
+                 : step_tma_one<T, NDIM, R, false>(p, grid, stream);
+}
+
+template <typename T, int NDIM, int R>
+int step_tma_halo() {
+  return TmaShape<T, NDIM, R, 32, 1>::H;
+}
+
 template <typename T, int NDIM, int R>
 cudaError_t step_unit(const StepParams<T> &p, const bool uniform, const dim3 grid,
                       cudaStream_t stream) {
@@ -70,6 +97,9 @@ cudaError_t adjoint_unit(const AdjointParams<T> &p, const bool u, const int mode
 
 template cudaError_t step_unit<CWB_REAL, CWB_NDIM, CWB_RADIUS>(const StepParams<CWB_REAL> &,
                                                                bool, dim3, cudaStream_t);
+template cudaError_t step_tma_unit<CWB_REAL, CWB_NDIM, CWB_RADIUS>(
+    const StepTmaParams<CWB_REAL> &, bool, dim3, cudaStream_t);
+template int step_tma_halo<CWB_REAL, CWB_NDIM, CWB_RADIUS>();
 template cudaError_t adjoint_unit<CWB_REAL, CWB_NDIM, CWB_RADIUS>(
     const AdjointParams<CWB_REAL> &, bool, int, dim3, cudaStream_t);
 

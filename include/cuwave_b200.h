@@ -55,11 +55,13 @@ typedef struct cwb_grid {
 typedef struct cwb_plan cwb_plan;
 
 /* Where the field of time step t lives: base + ((mul * t + add) mod period) * stride
- * elements (period 0: no wrap). Two slots rotate as period 2, a history as period 0. */
+ * elements (period 0: no wrap), one of `count` levels stacked from `base`. Two slots
+ * rotate as period 2, a history as period 0. */
 typedef struct cwb_level {
   void *base;
   int64_t stride;
   int32_t mul, add, period;
+  int32_t count; /* levels in the stack; every step's index must fall in 0 .. count - 1 */
 } cwb_level;
 
 /* The material a step reads. Replaces PressureWave.step_kernel_args
@@ -104,7 +106,7 @@ enum {
    * a Dirichlet face. Replaces homogeneous_neumann_kernel / homogeneous_dirichlet_kernel
    * (scalar.cu:535-555). */
   CWB_OP_REFILL = 4,
-  /* record[row] = a[lin] (bfloat16-rounded when points.bf16). Replaces
+  /* record[row] = a[lin], narrowed as points.store asks. Replaces
    * get_signal_kernel (common.cuh:483-491) and wave.narrow (cuwave/wave.py:848-853). */
   CWB_OP_RECORD = 5,
   /* The adjoint pml memory step from a = lambda^(n+1), before CWB_OP_ADJOINT reads it.
