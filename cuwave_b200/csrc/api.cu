@@ -55,6 +55,10 @@ struct cwb_plan {
   int chunk_override = 0;
   std::vector<Scratch> scratch;
   long long pml_row[3] = {0, 0, 0};
+  // a march run without a plan keeps its source lists in the library's static device
+  // array (cwb_march_static) instead of the plan's scratch
+  unsigned char *fixed = nullptr;
+  size_t fixed_cap = 0, fixed_used = 0;
 };
 
 namespace {
@@ -188,6 +192,27 @@ int build_sources(cwb_plan *p, const size_t slot, const cwb_points &pts, const d
   }
   if (entries.empty())
     entries.push_back(make_int4(-1, -1, 0, 0));
+  if (p->fixed) {
+    // no allocation: both lists go into the caller-less static region, 16-byte aligned
+    const size_t off = (p->fixed_used + 15) / 16 * 16;
+    const size_t start_bytes = (sizeof(int) * starts.size() + 15) / 16 * 16;
+    const size_t need = off + start_bytes + sizeof(int4) * entries.size();
+    if (need > p->fixed_cap)
+      return fail(CWB_ERR_ARG, "the folded sources need " + std::to_string(need) +
+                                   " bytes of static scratch, more than the " +
+                                   std::to_string(p->fixed_cap) + " it holds");
+    int *sdev = reinterpret_cast<int *>(p->fixed + off);
+    int4 *edev = reinterpret_cast<int4 *>(p->fixed + off + start_bytes);
+    CWB_CUDA(cudaMemcpyAsync(sdev, starts.data(), sizeof(int) * starts.size(),
+                             cudaMemcpyHostToDevice, stream));
+    CWB_CUDA(cudaMemcpyAsync(edev, entries.data(), sizeof(int4) * entries.size(),
+                             cudaMemcpyHostToDevice, stream));
+    CWB_CUDA(cudaStreamSynchronize(stream));
+    p->fixed_used = need;
+    *start = sdev;
+    *entry = edev;
+    return CWB_OK;
+  }
   if (p->scratch.size() <= slot)
     p->scratch.resize(slot + 1);
   Scratch &sc = p->scratch[slot];
@@ -840,3 +865,143 @@ int cwb_march(cwb_plan *p, const cwb_op *ops, const int32_t nops, const int32_t 
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------- march without allocation
+// Some callers cannot let a library allocate device memory: a host application (an
+// inference server, or a service embedding this library through its C ABI) that owns
+// the whole GPU through its own memory pool and forbids allocations behind its back,
+// or that budgets every byte of a device shared with other work. For them
+// cwb_march_static runs the same op list as cwb_march with no plan at all: its step
+// counter, its error flag and its folded-source lists live in g_static_scratch, a
+// fixed array every GPU that loads this library holds until the process exits.
+namespace {
+
+// 16 bytes of counter and flag, the rest for folded-source lists
+__device__ __align__(256) unsigned char g_static_scratch[CWB_STATIC_SCRATCH_BYTES];
+
+constexpr int MAX_DEVICES = 64;
+void *g_static_ptr[MAX_DEVICES] = {};
+
+// The device address of g_static_scratch on the current device. In host code the
+// symbol's name is only a host-side stand-in, so the address is asked from the runtime
+// once per device, with that device current, and cached.
+int static_scratch(void **out) {
+  int dev = 0;
+  CWB_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= MAX_DEVICES)
+    return fail(CWB_ERR_UNSUPPORTED, "device ordinal past the static scratch table");
+  if (!g_static_ptr[dev]) {
+    void *ptr = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&ptr, g_static_scratch);
+    if (e != cudaSuccess)
+      return fail(CWB_ERR_CUDA,
+                  std::string("cudaGetSymbolAddress(g_static_scratch): ") + cudaGetErrorString(e));
+    g_static_ptr[dev] = ptr;
+  }
+  *out = g_static_ptr[dev];
+  return CWB_OK;
+}
+
+// the plan fields a march reads, validated as cwb_plan_create validates them
+int static_geometry(const cwb_grid &G, cwb_plan &p) {
+  if (G.ndim != 2 && G.ndim != 3)
+    return fail(CWB_ERR_UNSUPPORTED, "the steps are 2D and 3D");
+  if (G.radius < 1 || G.radius > CWB_MAX_RADIUS)
+    return fail(CWB_ERR_UNSUPPORTED, "radius runs 1 .. 8");
+  if (G.precision != 4 && G.precision != 8)
+    return fail(CWB_ERR_UNSUPPORTED, "precision is 4 or 8 bytes");
+  if ((G.dirichlet & G.neumann) != 0)
+    return fail(CWB_ERR_ARG, "a face is either Neumann or Dirichlet");
+  cwb::Geometry &geo = p.geo;
+  std::memset(&geo, 0, sizeof geo);
+  geo.ndim = G.ndim;
+  long long total = 1;
+  for (int d = 0; d < G.ndim; ++d) {
+    if (G.nx[d] < G.radius + 3)
+      return fail(CWB_ERR_ARG, "every axis needs at least radius + 3 nodes");
+    geo.n[d] = G.nx[d];
+    geo.ext[d] = d == G.ndim - 1 ? (G.nx[d] + 31) / 32 * 32 : G.nx[d];
+    total *= geo.ext[d];
+  }
+  if (total >= (1LL << 31))
+    return fail(CWB_ERR_ARG, "the padded grid overflows int32 flat indices");
+  geo.s[G.ndim - 1] = 1;
+  for (int d = G.ndim - 2; d >= 0; --d)
+    geo.s[d] = geo.s[d + 1] * geo.ext[d + 1];
+  geo.dir = G.dirichlet;
+  for (int d = 0; d < G.ndim; ++d) {
+    geo.lo[d] = G.pml_lo[d];
+    geo.hi[d] = G.pml_hi[d];
+    if (geo.lo[d] < 0 || geo.hi[d] < 0 ||
+        (geo.lo[d] + geo.hi[d] > 0 &&
+         (geo.lo[d] ? geo.lo[d] + G.radius : 0) + (geo.hi[d] ? geo.hi[d] + G.radius : 0) >=
+             G.nx[d] - 2))
+      return fail(CWB_ERR_ARG, "the pml layers and their reach leave no interior");
+    if (geo.lo[d] + geo.hi[d] == 0)
+      continue;
+    long long row = 1;
+    for (int e = 0; e < G.ndim; ++e)
+      row *= e == d ? geo.lo[d] + geo.hi[d] : geo.ext[e];
+    p.pml_row[d] = row;
+  }
+  p.grid = G;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&p.sms, cudaDevAttrMultiProcessorCount, dev);
+  if (const char *env = std::getenv("CWB_CHUNK"))
+    p.chunk_override = std::atoi(env);
+  if (const char *env = std::getenv("CWB_NO_TMA"))
+    p.tma = std::atoi(env) == 0;
+  return CWB_OK;
+}
+
+template <typename T>
+int march_static(cwb_plan &p, const cwb_op *ops, const int nops, const int t0, const int steps,
+                 cudaStream_t s) {
+  std::vector<Launch> launches;
+  for (int i = 0; i < nops; ++i) {
+    const int rc = translate<T>(&p, ops[i], (size_t)i, s, launches);
+    if (rc)
+      return rc;
+  }
+  if (launches.empty() || steps <= 0)
+    return CWB_OK;
+  // the counter and the flag start at zero every call; the lists were written above
+  CWB_CUDA(cudaMemsetAsync(p.err, 0, sizeof(int), s));
+  CWB_CUDA(cwb::launch_set_counter(p.ctr, t0, s));
+  ++g_launches;
+  for (int k = 0; k < steps; ++k) {
+    const int rc = enqueue_step(launches, s);
+    if (rc)
+      return rc;
+  }
+  int err = 0;
+  CWB_CUDA(cudaMemcpyAsync(&err, p.err, sizeof(int), cudaMemcpyDeviceToHost, s));
+  CWB_CUDA(cudaStreamSynchronize(s));
+  if (err)
+    return fail(CWB_ERR_CUDA, "a staged tile never arrived: the step was abandoned");
+  return CWB_OK;
+}
+
+}  // namespace
+
+extern "C" int cwb_march_static(const cwb_grid *grid, const cwb_op *ops, const int32_t nops,
+                                const int32_t t0, const int32_t steps, void *stream) {
+  if (!grid || (!ops && nops > 0) || nops < 0)
+    return fail(CWB_ERR_ARG, "null argument");
+  void *base = nullptr;
+  int rc = static_scratch(&base);
+  if (rc)
+    return rc;
+  cwb_plan p;  // on the stack: no stream, event or device memory of its own
+  if ((rc = static_geometry(*grid, p)))
+    return rc;
+  unsigned char *bytes = static_cast<unsigned char *>(base);
+  p.ctr = reinterpret_cast<int *>(bytes);      // step counter and blocks done
+  p.err = reinterpret_cast<int *>(bytes + 8);  // error flag
+  p.fixed = bytes + 16;
+  p.fixed_cap = CWB_STATIC_SCRATCH_BYTES - 16;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  return grid->precision == 4 ? march_static<float>(p, ops, nops, t0, steps, s)
+                              : march_static<double>(p, ops, nops, t0, steps, s);
+}

@@ -159,6 +159,23 @@ int cwb_plan_destroy(cwb_plan *plan);
 int cwb_march(cwb_plan *plan, const cwb_op *ops, int32_t nops, int32_t t0,
               int32_t steps, int32_t graph, void *stream);
 
+/* Bytes of the static device scratch cwb_march_static uses (per GPU, until exit). */
+#define CWB_STATIC_SCRATCH_BYTES (256 * 1024)
+
+/* cwb_march for callers that cannot let a library allocate device memory, e.g. a host
+ * that owns the GPU through its own memory pool and forbids allocations behind its
+ * back. No counterpart in the reference. Runs the op list of cwb_march for `steps` steps
+ * directly on `stream`, without a plan: it allocates nothing, captures no graph, and
+ * keeps its step counter, error flag and folded-source lists (16 bytes per source plus
+ * 4 bytes per block of the step's grid) in one static device array of
+ * CWB_STATIC_SCRATCH_BYTES, whose device address it asks the runtime for on its first
+ * call on each device (make that first call before any stream capture). A march whose
+ * lists do not fit is refused with CWB_ERR_ARG. Every call shares the array: calls that
+ * overlap on the GPU (two streams, two host threads) race and must not be issued. The
+ * call returns after the march has finished on the GPU. */
+int cwb_march_static(const cwb_grid *grid, const cwb_op *ops, int32_t nops, int32_t t0,
+                     int32_t steps, void *stream);
+
 /* Elements per row of the pml memory of axis d (0 for an unlined axis); a forward
  * memory holds 3 such rows, an adjoint one 5. */
 int64_t cwb_pml_row(const cwb_plan *plan, int32_t d);
