@@ -13,12 +13,16 @@
 // node arithmetic is step.cuh's, i.e. cuwave fd_kernel + pml_kernel (scalar.cu:347-532).
 #pragma once
 
+#include <type_traits>
+
 #include "step.cuh"
 #include "tma.cuh"
 
 namespace cwb {
 
-constexpr int TMA_PREFETCH = 2;
+#ifndef TMA_MIN_BLOCKS
+#define TMA_MIN_BLOCKS 3  // resident blocks per SM the register budget is cut for
+#endif
 
 template <typename T>
 struct StepTmaParams {
@@ -37,7 +41,9 @@ struct TmaShape {
   static constexpr int HY = NDIM == 3 ? R : 0;
   static constexpr int WB = BX + 2 * H;
   static constexpr int HB = BY + 2 * HY;
-  static constexpr int STAGES = R + 1 + TMA_PREFETCH;
+  // planes in flight past the queue's lead: deeper where the ring still fits 3 blocks
+  static constexpr int PREFETCH = R <= 4 ? 3 : 2;
+  static constexpr int STAGES = R + 1 + PREFETCH;
   static constexpr int U1_BYTES = WB * HB * (int)sizeof(T);
   static constexpr int TILE_BYTES = BX * BY * (int)sizeof(T);
   static constexpr int align128(int b) { return (b + 127) / 128 * 128; }
@@ -58,7 +64,7 @@ __device__ __forceinline__ int level_index(const int *L, const int t) {
 }
 
 template <typename T, int NDIM, int R, bool UNIF, int BX, int BY, int RY>
-__global__ void __launch_bounds__(BX *(BY / RY))
+__global__ void __launch_bounds__(BX *(BY / RY), TMA_MIN_BLOCKS)
     step_tma_kernel(const __grid_constant__ StepTmaParams<T> P) {
   using S = TmaShape<T, NDIM, R, BX, BY>;
   constexpr int H = S::H, HY = S::HY, WB = S::WB, NS = S::STAGES, F = NDIM - 1;
@@ -163,42 +169,88 @@ __global__ void __launch_bounds__(BX *(BY / RY))
     slast = p.src_start[blk + 1];
     srow = p.sig_mul * t + p.sig_add;
   }
-  // wait for a staged plane, then give an edge tile's halo its mirrors; false if the
-  // wait ran out on any thread
+  // An edge tile's box past the walls takes the mirrored values (the copy zero-filled
+  // it). Only the out-of-range columns and rows are visited; a cell out of range on both
+  // axes is never read by a star stencil and is zeroed.
+  const int xlo_end = max(0, min(WB, H - x0));        // columns with x < 0
+  const int xhi_beg = max(0, min(WB, NF - (x0 - H)));  // columns with x > NF - 1
+  const int ylo_end = NDIM == 3 ? max(0, min(S::HB, HY - y0)) : 0;
+  const int yhi_beg = NDIM == 3 ? max(0, min(S::HB, NM - (y0 - HY))) : S::HB;
+  const auto fix_cell = [&](T *box, const int bx, const int by) {
+    const int xg = x0 - H + bx, yg = y0 - HY + by;
+    const bool xin = xg >= 0 && xg <= NF - 1;
+    const bool yin = NDIM == 2 || (yg >= 0 && yg <= NM - 1);
+    if (xin && yin)
+      return;
+    T v = (T)0;
+    if (xin != yin) {
+      int sx = 1, sy = 1;
+      const int mx = xin ? xg : mirror_node(xg, NF, dirF, sx);
+      const int my = (NDIM == 2 || yin) ? yg : mirror_node(yg, NM, dirM, sy);
+      const int lx = mx - (x0 - H), ly = my - (y0 - HY);
+      const bool mine = mx >= 0 && mx <= NF - 1 && my >= 0 && (NDIM == 2 || my <= NM - 1);
+      if (mine && lx >= 0 && lx < WB && ly >= 0 && ly < S::HB) {
+        const T m = box[ly * WB + lx];
+        v = sx * sy < 0 ? -m : m;
+      }
+    }
+    box[by * WB + bx] = v;
+  };
+  const auto fix = [&](const int plane) {
+    T *box = reinterpret_cast<T *>(stage(plane));
+    const int nthreads = BX * TY, tid = ty * BX + tx;
+    const int ncols = xlo_end + (WB - xhi_beg);
+    for (int c = tid; c < ncols * S::HB; c += nthreads) {
+      const int ci = c % ncols, by = c / ncols;
+      fix_cell(box, ci < xlo_end ? ci : xhi_beg + (ci - xlo_end), by);
+    }
+    const int nrows = ylo_end + (S::HB - yhi_beg);
+    for (int c = tid; c < nrows * WB; c += nthreads) {
+      const int ri = c / WB, bx = c % WB;
+      fix_cell(box, bx, ri < ylo_end ? ri : yhi_beg + (ri - ylo_end));
+    }
+  };
+  // wait for a staged plane: the leader polls the barrier, the block learns the outcome
+  // at the barrier after; then an edge tile's halo takes its mirrors. False if the
+  // bounded wait ran out.
   const auto arrive = [&](const int plane) -> bool {
     bool good = true;
-    if (plane <= last)
+    if (leader && plane <= last)
       good = mbar_wait(&full[plane % NS], (unsigned)((plane - c0) / NS) & 1u);
     if (!__syncthreads_and(good))
       return false;
     arrived = plane;
     if (plane <= last && edge) {
-      T *box = reinterpret_cast<T *>(stage(plane));
-      for (int cell = ty * BX + tx; cell < WB * S::HB; cell += BX * TY) {
-        const int bx = cell % WB, by = cell / WB;
-        const int xg = x0 - H + bx, yg = y0 - HY + by;
-        const bool xin = xg >= 0 && xg <= NF - 1;
-        const bool yin = NDIM == 2 || (yg >= 0 && yg <= NM - 1);
-        if (xin && yin)
-          continue;
-        T v = (T)0;
-        if (xin != yin) {
-          int sx = 1, sy = 1;
-          const int mx = xin ? xg : mirror_node(xg, NF, dirF, sx);
-          const int my = (NDIM == 2 || yin) ? yg : mirror_node(yg, NM, dirM, sy);
-          const int lx = mx - (x0 - H), ly = my - (y0 - HY);
-          const bool mine = mx >= 0 && mx <= NF - 1 && my >= 0 && (NDIM == 2 || my <= NM - 1);
-          if (mine && lx >= 0 && lx < WB && ly >= 0 && ly < S::HB) {
-            const T m = box[ly * WB + lx];
-            v = sx * sy < 0 ? -m : m;
-          }
-        }
-        box[by * WB + bx] = v;
-      }
+      fix(plane);
       __syncthreads();
     }
     return true;
   };
+
+  // what the tile's nodes can meet, fixed for the block: pml slabs of the in-plane axes,
+  // the mirror rows the folded refill writes from, Dirichlet wall nodes, sources
+  const int xa = max(x0, 1), xb = min(x0 + BX - 1, NF - 2);
+  const int ya = NDIM == 3 ? max(y0, 1) : 0, yb = NDIM == 3 ? min(y0 + BY - 1, NM - 2) : 0;
+  const auto meets = [](const int a, const int b, const int lo, const int hi) {
+    return a <= hi && lo <= b;
+  };
+  bool tile_general = (flags & K_DAMP) || sfirst < slast;
+  if (flags & K_PML) {
+    const int loF = g.lo[F], hiF = g.hi[F];
+    tile_general |= (loF && meets(xa, xb, 1, loF)) || (hiF && meets(xa, xb, NF - 1 - hiF, NF - 2));
+    if (NDIM == 3) {
+      const int loM = g.lo[1], hiM = g.hi[1];
+      tile_general |= (loM && meets(ya, yb, 1, loM)) || (hiM && meets(ya, yb, NM - 1 - hiM, NM - 2));
+    }
+  }
+  if (flags & K_REFILL) {
+    tile_general |= meets(xa, xb, 2, 2) || meets(xa, xb, NF - 3, NF - 3);
+    if (NDIM == 3)
+      tile_general |= meets(ya, yb, 2, 2) || meets(ya, yb, NM - 3, NM - 3);
+  }
+  tile_general |= ((dirF & 1) && meets(xa, xb, 1, 1)) || ((dirF & 2) && meets(xa, xb, NF - 2, NF - 2));
+  if (NDIM == 3)
+    tile_general |= ((dirM & 1) && meets(ya, yb, 1, 1)) || ((dirM & 2) && meets(ya, yb, NM - 2, NM - 2));
 
   bool ok = true;
   if (c0 < c1)
@@ -228,21 +280,24 @@ __global__ void __launch_bounds__(BX *(BY / RY))
       const int cell = (ty + k * TY + HY) * WB + tx + H;
       q[k][2 * R] = ahead <= N0 - 1 ? nxt[cell] : row_val(ahead, col[k]);
     }
+    // the plane's own slab, refill row or wall send it down the general path
+    bool general = tile_general;
+    if (flags & K_PML)
+      general |= (g.lo[0] && a0 <= g.lo[0]) || (g.hi[0] && a0 >= N0 - 1 - g.hi[0]);
+    if (flags & K_REFILL)
+      general |= a0 == 2 || a0 == N0 - 3;
+    general |= ((dir0 & 1) && a0 == 1) || ((dir0 & 2) && a0 == N0 - 2);
+    const T *tile0 = reinterpret_cast<const T *>(stage(a0) + S::U0_OFF);
+    const T *tilem = reinterpret_cast<const T *>(stage(a0) + S::MINV_OFF);
 
-#pragma unroll
-    for (int k = 0; k < RY; ++k) {
-      if (!inner[k])
-        continue;
+    const auto node = [&](const int k, auto full_path) {
+      constexpr bool GEN = decltype(full_path)::value;
       const int idx = a0 * s0 + col[k];
       const T uc = q[k][R];
       const T *trow = cur + (ty + k * TY + HY) * WB + tx + H;
       const auto tap0 = [&](const int j) { return q[k][R + j]; };
       const auto tapM = [&](const int j) { return trow[j * WB]; };
       const auto tapF = [&](const int j) { return trow[j]; };
-      const int A[3] = {a0, NDIM == 3 ? py[k] : px, px};
-      const int strides[3] = {s0, NDIM == 3 ? sM : 1, 1};
-      const T *tile0 = reinterpret_cast<const T *>(stage(a0) + S::U0_OFF);
-      const T *tilem = reinterpret_cast<const T *>(stage(a0) + S::MINV_OFF);
       const int tc = (ty + k * TY) * BX + tx;
 
       T Dp[NDIM], Dm[NDIM], gp[NDIM], gm[NDIM], dd[NDIM];
@@ -259,7 +314,8 @@ __global__ void __launch_bounds__(BX *(BY / RY))
           gp[d] = p.gconst;
           gm[d] = p.gconst;
         } else {
-          const T sp = p.stiff[idx + strides[d]], sm = p.stiff[idx - strides[d]];
+          const int st = d == 0 ? s0 : (d == F ? 1 : sM);
+          const T sp = p.stiff[idx + st], sm = p.stiff[idx - st];
           gp[d] = sc * sp / (sc + sp);
           gm[d] = sc * sm / (sc + sm);
         }
@@ -274,72 +330,97 @@ __global__ void __launch_bounds__(BX *(BY / RY))
       const T mi = (flags & K_DERIVE) ? (T)1 / sc : tilem[tc];
       const T old = tile0[tc];
       T v;
-      if (flags & K_DAMP) {
+      if (GEN && (flags & K_DAMP)) {
         const T beta = (T)0.5 * mi * p.damping[idx] * p.dt;
         v = ((T)2 * uc - old * ((T)1 - beta) + mi * lap) / ((T)1 + beta);
       } else {
         v = -old + (T)2 * uc + mi * lap;
       }
-      const bool held = held_wall(a0, N0, dir0) || (NDIM == 3 && held_wall(py[k], NM, dirM)) ||
-                        held_wall(px, NF, dirF);
-      if (held)
-        v = (T)0;
-      if (flags & K_PML) {
+      if constexpr (GEN) {
+        const int pyk = NDIM == 3 ? py[k] : 0;
+        const bool held = held_wall(a0, N0, dir0) || (NDIM == 3 && held_wall(pyk, NM, dirM)) ||
+                          held_wall(px, NF, dirF);
+        if (held)
+          v = (T)0;
+        if (flags & K_PML) {
 #pragma unroll
-        for (int d = 0; d < NDIM; ++d) {
-          const int lo = g.lo[d], hi = g.hi[d];
-          if (!(lo + hi))
-            continue;
-          const int a = A[d], N = g.n[d];
-          const int r = slab_row(a, N, lo, hi);
-          if (r < 0)
-            continue;
-          T Dpu, Dmu;
-          if (d == 0)
-            diffs_plain<T, R>(tap0, uc, p.w, Dpu, Dmu);
-          else if (d == F)
-            diffs_plain<T, R>(tapF, uc, p.w, Dpu, Dmu);
-          else
-            diffs_plain<T, R>(tapM, uc, p.w, Dpu, Dmu);
-          const T *prof = p.prof[d];
-          const T an = prof[a], bn = prof[N + a];
-          const T ah = prof[2 * N + a], bh = prof[3 * N + a];
-          const T ah1 = prof[2 * N + a - 1], bh1 = prof[3 * N + a - 1];
-          T *aux = p.aux[d];
-          const int sz = p.auxrow[d];
-          const int si = slab_index(g, d, r, A);
-          const T f = p.f[d];
-          const T pp = bh * aux[si] + ah * Dpu;
-          const T pm = bh1 * aux[sz + si] + ah1 * Dmu;
-          const T z = bn * aux[2 * sz + si] + an * f * (gp[d] * (Dpu + pp) - gm[d] * (Dmu + pm));
-          aux[si] = pp;
-          aux[sz + si] = pm;
-          aux[2 * sz + si] = z;
-          if (!held)
-            v += mi * (f * (gp[d] * pp - gm[d] * pm) + z);
+          for (int d = 0; d < NDIM; ++d) {
+            const int lo = g.lo[d], hi = g.hi[d];
+            if (!(lo + hi))
+              continue;
+            const int a = d == 0 ? a0 : (d == F ? px : pyk);
+            const int N = g.n[d];
+            const int r = slab_row(a, N, lo, hi);
+            if (r < 0)
+              continue;
+            T Dpu, Dmu;
+            if (d == 0)
+              diffs_plain<T, R>(tap0, uc, p.w, Dpu, Dmu);
+            else if (d == F)
+              diffs_plain<T, R>(tapF, uc, p.w, Dpu, Dmu);
+            else
+              diffs_plain<T, R>(tapM, uc, p.w, Dpu, Dmu);
+            const T *prof = p.prof[d];
+            const T an = prof[a], bn = prof[N + a];
+            const T ah = prof[2 * N + a], bh = prof[3 * N + a];
+            const T ah1 = prof[2 * N + a - 1], bh1 = prof[3 * N + a - 1];
+            T *aux = p.aux[d];
+            const int sz = p.auxrow[d];
+            const int rows = lo + hi, extF = g.ext[F];
+            // the memory's own layout: the padded grid with axis d replaced by its rows
+            int si;
+            if (NDIM == 3)
+              si = d == 0 ? (r * NM + pyk) * extF + px
+                          : (d == 1 ? (a0 * rows + r) * extF + px : (a0 * NM + pyk) * rows + r);
+            else
+              si = d == 0 ? r * extF + px : a0 * rows + r;
+            const T f = p.f[d];
+            const T pp = bh * aux[si] + ah * Dpu;
+            const T pm = bh1 * aux[sz + si] + ah1 * Dmu;
+            const T z = bn * aux[2 * sz + si] + an * f * (gp[d] * (Dpu + pp) - gm[d] * (Dmu + pm));
+            aux[si] = pp;
+            aux[sz + si] = pm;
+            aux[2 * sz + si] = z;
+            if (!held)
+              v += mi * (f * (gp[d] * pp - gm[d] * pm) + z);
+          }
         }
-      }
-      if (flags & K_SRC) {
-        const int lane = (ty + k * TY) * BX + tx;
-        for (int e = sfirst; e < slast; ++e) {
-          const int4 en = p.src_entry[e];
-          if (en.x == a0 && en.y == lane)
-            v += p.src_weight[en.z] * p.signal[srow * p.nsrc + en.z];
+        if (flags & K_SRC) {
+          const int lane = (ty + k * TY) * BX + tx;
+          for (int e = sfirst; e < slast; ++e) {
+            const int4 en = p.src_entry[e];
+            if (en.x == a0 && en.y == lane)
+              v += p.src_weight[en.z] * p.signal[srow * p.nsrc + en.z];
+          }
         }
-      }
-      if ((flags & K_REFILL) && held)
-        v = (T)0;
-      u2[idx] = v;
-      if (flags & K_REFILL) {
+        if ((flags & K_REFILL) && held)
+          v = (T)0;
+        u2[idx] = v;
+        if (flags & K_REFILL) {
 #pragma unroll
-        for (int d = 0; d < NDIM; ++d) {
-          const int a = A[d], N = g.n[d], st = strides[d];
-          if (((p.refill >> (2 * d)) & 1) && a == 2)
-            u2[idx - 2 * st] = ((g.dir >> (2 * d)) & 1) ? -v : v;
-          if (((p.refill >> (2 * d + 1)) & 1) && a == N - 3)
-            u2[idx + 2 * st] = ((g.dir >> (2 * d + 1)) & 1) ? -v : v;
+          for (int d = 0; d < NDIM; ++d) {
+            const int a = d == 0 ? a0 : (d == F ? px : pyk), N = g.n[d];
+            const int st = d == 0 ? s0 : (d == F ? 1 : sM);
+            if (((p.refill >> (2 * d)) & 1) && a == 2)
+              u2[idx - 2 * st] = ((g.dir >> (2 * d)) & 1) ? -v : v;
+            if (((p.refill >> (2 * d + 1)) & 1) && a == N - 3)
+              u2[idx + 2 * st] = ((g.dir >> (2 * d + 1)) & 1) ? -v : v;
+          }
         }
+      } else {
+        u2[idx] = v;
       }
+    };
+    if (general) {
+#pragma unroll
+      for (int k = 0; k < RY; ++k)
+        if (inner[k])
+          node(k, std::true_type{});
+    } else {
+#pragma unroll
+      for (int k = 0; k < RY; ++k)
+        if (inner[k])
+          node(k, std::false_type{});
     }
 #pragma unroll
     for (int k = 0; k < RY; ++k)

@@ -1,8 +1,8 @@
 // TMA tile loads and mbarriers for sm_100a, as inline PTX.
 //
-// Every wait on an mbarrier is bounded: after MAX_POLLS polls it gives up, raises the
-// launch's error flag and lets the kernel finish without the tile, so a lost copy
-// can never hang the GPU. The host reads the flag after the march.
+// Every wait on an mbarrier is bounded: after WAIT_CYCLES clock cycles (about a second)
+// it gives up, the kernel raises its error flag, drains what it issued and finishes, so
+// a lost copy can never hang the GPU. The host reads the flag after the march.
 #pragma once
 
 #include <cstdint>
@@ -10,7 +10,7 @@
 
 namespace cwb {
 
-constexpr unsigned MAX_POLLS = 1u << 26;  // ~ seconds of polling at most
+constexpr long long WAIT_CYCLES = 2000000000LL;  // ~1 s at 1.9 GHz
 
 __device__ __forceinline__ unsigned smem_addr(const void *p) {
   return static_cast<unsigned>(__cvta_generic_to_shared(p));
@@ -39,7 +39,8 @@ __device__ __forceinline__ void mbar_expect(uint64_t *bar, const unsigned bytes)
 // wait for phase `parity` of the barrier to complete; false if the bound ran out
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, const unsigned parity) {
   const unsigned addr = smem_addr(bar);
-  for (unsigned polls = 0; polls < MAX_POLLS; ++polls) {
+  const long long start = clock64();
+  for (;;) {
     unsigned done;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
@@ -50,8 +51,9 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, const unsigned parity) 
         : "memory");
     if (done)
       return true;
+    if (clock64() - start > WAIT_CYCLES)
+      return false;
   }
-  return false;
 }
 
 // a 4D tile (x fastest) of `map` at coordinates (x, y, z, w) into shared memory, its

@@ -137,16 +137,19 @@ def _adjoint_ops(sim, mat, P, eta, *, u_level=None, grads=None, load=None, probe
     return ops
 
 
-def sensitivity(sim: Simulation, source: Source, indicator, sensors, objective: Callable):
+def sensitivity(sim: Simulation, source: Source, indicator, sensors, objective: Callable,
+                *, _mat: dict | None = None, _probe: bool = False):
     """Cost and d(cost)/d(mass, stiff) with the forward history stored (cuwave sensitivity.py:384-497).
 
     The forward march writes every level into an (N + 2)-level history V, V[t + 2] = u^t;
     the adjoint march steps lambda with the gradients fused against V reversed.
+    (`_mat` replaces the materials built from `indicator`; `_probe` also returns
+    d(cost)/d(source.signal) in info["source"], from the same adjoint march.)
     """
     require_interior(sim, sensors, "sensor")
     require_interior(sim, source.position, "source")
     dev = device()
-    mat = sim.build_materials(indicator)
+    mat = sim.build_materials(indicator) if _mat is None else _mat
     shot = prepare_shot(sim, mat, source.position, source.signal)
     require_off_held_walls(sim, shot.position)
     plan = sim.plan()
@@ -171,10 +174,17 @@ def sensitivity(sim: Simulation, source: Source, indicator, sensors, objective: 
     eta = pml_memory(sim, 5, dev)
     # adjoint step m pairs lambda^n, n = N - 1 - m, with u^n = V[N + 1 - m]
     u_level = nat.level(V, mul=-1, add=N + 1)
+    probe = lam = None
+    if _probe:
+        lam = torch.zeros((N, shot.lin.numel()), dtype=sim.dtype, device=dev)
+        probe = (shot.lin, lam)
     ops = _adjoint_ops(sim, mat, P, eta, u_level=u_level, grads=grads,
-                       load=(sensor_lin, signal, weight))
+                       load=(sensor_lin, signal, weight), probe=probe)
     plan.march(ops, 0, N)
-    return cost, frozen(sim, sim.finalize_gradients(grads)), um, {}
+    info = {}
+    if _probe:
+        info["source"] = (lam.flip(0) * sim.adjoint_weights(shot.position)).contiguous()
+    return cost, frozen(sim, sim.finalize_gradients(grads)), um, info
 
 
 def source_sensitivity(sim: Simulation, source: Source, indicator, sensors, objective: Callable):
@@ -290,7 +300,8 @@ def _store_code(sim: Simulation, stored) -> int:
 
 def reconstruction_sensitivity(sim: Simulation, source: Source, indicator, sensors,
                                objective: Callable, strip_dtype: str | None = None,
-                               checkpoints: int | None = None):
+                               checkpoints: int | None = None, *, _mat: dict | None = None,
+                               _probe: bool = False):
     """Cost and gradients as `sensitivity`, marching the forward field backwards behind a
     recorded strip instead of storing it (cuwave sensitivity.py:500-750).
 
@@ -300,7 +311,9 @@ def reconstruction_sensitivity(sim: Simulation, source: Source, indicator, senso
     on the way back. With `checkpoints` the run is cut into segments replayed from
     snapshots on the treeverse schedule, so memory no longer grows with N.
 
-    Returns (cost, grads, traces, info) with info = {"strip", "drift", "segment", "sweeps"}.
+    Returns (cost, grads, traces, info) with info = {"strip", "drift", "segment", "sweeps"}
+    (and, with `_probe`, "source": d(cost)/d(source.signal) from the same adjoint march;
+    `_mat` replaces the materials built from `indicator`).
     """
     require_interior(sim, sensors, "sensor")
     require_interior(sim, source.position, "source")
@@ -314,10 +327,11 @@ def reconstruction_sensitivity(sim: Simulation, source: Source, indicator, senso
         )
     dev = device()
     N = sim.N
-    mat = sim.build_materials(indicator)
+    mat = sim.build_materials(indicator) if _mat is None else _mat
     shot = prepare_shot(sim, mat, source.position, source.signal)
     require_off_held_walls(sim, shot.position)
     plan = sim.plan()
+    lam = torch.zeros((N, shot.lin.numel()), dtype=sim.dtype, device=dev) if _probe else None
     itemsize = torch.empty(0, dtype=sim.dtype).element_size()
     stored_size = torch.empty(0, dtype=stored).element_size()
 
@@ -411,6 +425,8 @@ def reconstruction_sensitivity(sim: Simulation, source: Source, indicator, senso
         ops.append(nat.op(nat.OP_EXCITE, a=l0,
                           points=nat.points(sensor_lin, state["signal"], weight=sensor_weight,
                                             row_add=offset)))
+        if lam is not None:
+            ops.append(nat.op(nat.OP_RECORD, a=l0, points=nat.points(shot.lin, lam, row_add=offset)))
         # the triplet of step m + offset and the lambda just stepped
         o_ = offset
         ops.append(nat.op(nat.OP_GRADIENT, a=slot(0, mul=-1, add=N + 2 - o_),
@@ -469,4 +485,6 @@ def reconstruction_sensitivity(sim: Simulation, source: Source, indicator, senso
     seed = state["seed"]
     drift = float(torch.linalg.vector_norm(U[0] * valid)) / seed if seed > 0.0 else float("inf")
     info = {"strip": num_strip, "drift": drift, "segment": segment, "sweeps": state["steps"] / N}
+    if lam is not None:
+        info["source"] = (lam.flip(0) * sim.adjoint_weights(shot.position)).contiguous()
     return state["cost"], grads, um, info

@@ -358,15 +358,17 @@ def pml_memory(sim: Simulation, rows: int, dev: torch.device) -> list:
     return memory
 
 
-def simulate(sim: Simulation, source: Source, indicator, sensors=None, record_every=None):
+def simulate(sim: Simulation, source: Source, indicator, sensors=None, record_every=None,
+             *, _mat: dict | None = None):
     """Run `sim` forward under `source` and material `indicator` (cuwave wave.py:1071-1163).
 
     Returns the final field over the logical grid (ghosts kept, the padding dropped), a
     view of the march's own slot, followed by the (N, num_sensors) record when `sensors`
     is given and the stacked host snapshots of the field every `record_every` steps.
+    (`_mat` replaces the materials built from `indicator`.)
     """
     dev = device()
-    mat = sim.build_materials(indicator)
+    mat = sim.build_materials(indicator) if _mat is None else _mat
     shot = prepare_shot(sim, mat, source.position, source.signal)
     require_off_held_walls(sim, shot.position)
     if shot.signal.shape[0] < sim.N:
