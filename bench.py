@@ -76,7 +76,8 @@ def make_sim(w: dict):
 
     return AcousticWave(
         Nx=w["Nx"], dx=(1.0, 1.0, 1.0), N=w["steps"], dt=w["dt"], precision="float32",
-        space_order=8, stencil="optimized", pml=Pml(width=w["width"], wavespeed=w["c_max"]),
+        space_order=8, stencil="optimized",
+        pml=Pml(width=w["width"], wavespeed=w["c_max"]) if w["width"] else None,
         rho1=1.0, rho2=1.0, kappa1=1.0, kappa2=w["kappa2"],
     )
 
@@ -166,9 +167,9 @@ def reference_case(w: dict):
 
     Nx = w["Nx"]
     stiff, minv = o.acoustic_materials(Nx, w["indicator"], 1.0, 1.0, 1.0, w["kappa2"], np.float32)
-    widths = tuple((w["width"], w["width"]) for _ in range(3))
+    widths = tuple((w["width"], w["width"]) for _ in range(3)) if w["width"] else None
     profiles = o.pml_profiles(Nx, (1.0,) * 3, w["dt"], widths, w["width"], w["c_max"], 1e-6, 0.0,
-                              np.float32)
+                              np.float32) if w["width"] else None
     flat = lambda p: (p[0].astype(np.int64) * Nx[1] * ((Nx[2] + 31) // 32 * 32)  # noqa: E731
                       + p[1].astype(np.int64) * ((Nx[2] + 31) // 32 * 32) + p[2]).astype(np.int32)
     case = o.Case(Nx=Nx, R=4, coeffs=o.cell_coefficients(4, "optimized"),
@@ -183,7 +184,7 @@ def run_reference(args) -> int:
     rank, world, _ = dist_setup()
     if rank != 0:
         return 0
-    w = workload(args.size, args.nt)
+    w = workload(args.size, args.nt, args.pml)
     sample = args.ref_sample
     times = []
     from oracle import oracle as o
@@ -268,7 +269,7 @@ def run_ours(args) -> int:
 
         dist.init_process_group("nccl", timeout=timedelta(seconds=600),
                                 device_id=torch.device("cuda", local))
-    w = workload(args.size, args.nt)
+    w = workload(args.size, args.nt, args.pml)
     sim = make_sim(w)
     dev = torch.device("cuda", local)
     indicator = torch.as_tensor(w["indicator"], device=dev)
@@ -357,7 +358,7 @@ def run_ours(args) -> int:
         "config": config_line(w, args),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
-                     "kernel": "step_kernel<float,3,4,uniform> (fd + pml + sources + refill)",
+                     "kernel": step_kernel_name(),
                      "kernel_ms": kernel_ms, "algorithmic_bytes_per_launch": bytes_per_launch},
         "cpu_baseline": baseline,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
@@ -368,6 +369,12 @@ def run_ours(args) -> int:
     }
     print(json.dumps(line))
     return 0
+
+
+def step_kernel_name() -> str:
+    if os.environ.get("CWB_STEP3D", "1") != "0" and os.environ.get("CWB_NO_TMA", "0") == "0":
+        return "step3d_kernel<float,4,uniform> (blocked 3D step: fd + pml + sources + refill)"
+    return "step_tma_kernel<float,3,4,uniform> (row step: fd + pml + sources + refill)"
 
 
 def hbm_peak() -> tuple[float, str]:
@@ -396,6 +403,7 @@ def main(argv=None) -> int:
     parser.add_argument("--impl", choices=("ours", "reference"), default="ours")
     parser.add_argument("--size", type=int, default=512, help="grid nodes per axis (ghosts included)")
     parser.add_argument("--nt", type=int, default=4000, help="time steps of one job")
+    parser.add_argument("--pml", type=int, default=20, help="pml width in cells (0: none)")
     parser.add_argument("--kernel-steps", type=int, default=400)
     parser.add_argument("--cpu-sample", type=int, default=6, help="time steps the CPU baseline runs")
     parser.add_argument("--ref-sample", type=int, default=3, help="time steps per reference bench step")

@@ -13,6 +13,7 @@
 
 #include "cuwave_b200.h"
 #include "launch.cuh"
+#include "step3d.cuh"
 #include "step_tma.cuh"
 
 namespace {
@@ -49,6 +50,7 @@ struct cwb_plan {
   int *ctr = nullptr;
   int *err = nullptr;  // raised by a kernel whose bounded wait ran out
   bool tma = true;     // stage planes with tensor-map copies where the layout allows
+  bool blocked3 = true;  // 3D steps of a uniform stiffness on the register-blocked kernel
   cudaStream_t lane = nullptr;
   cudaEvent_t fork = nullptr, join = nullptr;
   int sms = 148;
@@ -73,7 +75,7 @@ int chunk_for(const cwb_plan *p, const int plane_blocks) {
     return p->chunk_override;
   const int rows = p->geo.n[0] - 2;
   if (p->geo.ndim == 3)
-    return std::min(rows, 128);
+    return std::min(rows, 32);  // the fastest of 32 .. 255 planes measured on 512^3
   const long long want = 8LL * p->sms;
   const long long chunk = (rows * (long long)plane_blocks + want - 1) / want;
   return (int)std::max<long long>(8, std::min<long long>(rows, chunk));
@@ -305,15 +307,14 @@ cudaError_t step_tma_nd(const cwb::StepTmaParams<T> &p, const int R, const bool 
 
 // The tensor maps of a TMA step: the level stacks of operands b (box with halo) and a,
 // and 1/m. False where the layout does not allow tensor-map copies.
-template <typename T>
+// `bx` x `by` tiles, the box of b wider by `H` on each side of the fast axis.
+template <typename T, class Params>
 bool tma_maps(const cwb_plan *p, const cwb_op &op, const bool derive, const T *minv,
-              cwb::StepTmaParams<T> &tp) {
+              Params &tp, const int bx, const int by, const int H) {
   const cwb::Geometry &g = p->geo;
   const int nd = g.ndim, F = nd - 1, R = p->grid.radius;
-  const int H = nd == 3 ? tma_halo_nd<T, 3>(R) : tma_halo_nd<T, 2>(R);
   const cuuint64_t ext = g.ext[F], nm = nd == 3 ? g.n[1] : 1, n0 = g.n[0];
   const cuuint64_t row = ext * sizeof(T), plane = row * nm;
-  const int bx = nd == 3 ? cwb::TMA_BX3 : cwb::TMA_BX2, by = nd == 3 ? cwb::TMA_BY3 : 1;
   const int hy = nd == 3 ? R : 0;
   for (const cwb_level *L : {&op.b, &op.a})
     if (L->count < 1 || (L->period > 0 && L->period > L->count))
@@ -395,6 +396,37 @@ cudaError_t step_tma_dispatch(const cwb::StepTmaParams<T> &p, const int ndim, co
 }
 
 template <typename T>
+int step3d_halo_r(const int R) {
+  switch (R) {
+  case 1: return cwb::step3d_halo<T, 1>();
+  case 2: return cwb::step3d_halo<T, 2>();
+  case 3: return cwb::step3d_halo<T, 3>();
+  case 4: return cwb::step3d_halo<T, 4>();
+  case 5: return cwb::step3d_halo<T, 5>();
+  case 6: return cwb::step3d_halo<T, 6>();
+  case 7: return cwb::step3d_halo<T, 7>();
+  case 8: return cwb::step3d_halo<T, 8>();
+  }
+  return -1;
+}
+
+template <typename T>
+cudaError_t step3d_r(const cwb::Step3Params<T> &p, const int R, const bool u, const dim3 grid,
+                     cudaStream_t s) {
+  switch (R) {
+  case 1: return cwb::step3d_unit<T, 1>(p, u, grid, s);
+  case 2: return cwb::step3d_unit<T, 2>(p, u, grid, s);
+  case 3: return cwb::step3d_unit<T, 3>(p, u, grid, s);
+  case 4: return cwb::step3d_unit<T, 4>(p, u, grid, s);
+  case 5: return cwb::step3d_unit<T, 5>(p, u, grid, s);
+  case 6: return cwb::step3d_unit<T, 6>(p, u, grid, s);
+  case 7: return cwb::step3d_unit<T, 7>(p, u, grid, s);
+  case 8: return cwb::step3d_unit<T, 8>(p, u, grid, s);
+  }
+  return cudaErrorInvalidValue;
+}
+
+template <typename T>
 cudaError_t adjoint_dispatch(const cwb::AdjointParams<T> &p, const int ndim, const int R,
                              const bool u, const int mode, const dim3 grid, cudaStream_t s) {
   return ndim == 3 ? adjoint_nd<T, 3>(p, R, u, mode, grid, s)
@@ -443,10 +475,29 @@ int translate(cwb_plan *p, const cwb_op &op, const size_t slot, cudaStream_t str
           return fail(CWB_ERR_ARG, "a lined axis needs its pml memory");
       }
     }
-    const bool tma = p->tma && tma_maps<T>(p, op, flags & cwb::K_DERIVE, sp.minv, tp);
+    // 3D, a uniform stiffness: the blocked kernel. It stores rows of four and keeps the
+    // taps it mirrors in its own run, so it wants an output level on 16-byte boundaries
+    // and axes of at least 3R nodes. Elsewhere the TMA row kernel, else the plain one.
+    const bool derive = flags & cwb::K_DERIVE;
+    cwb::Step3Params<T> s3;
+    std::memset(&s3, 0, sizeof s3);
+    const bool c_aligned = reinterpret_cast<uintptr_t>(op.c.base) % 16 == 0 &&
+                           (op.c.stride * (long long)sizeof(T)) % 16 == 0;
+    const bool roomy = ndim == 3 && g.n[0] >= 3 * R && g.n[1] >= 3 * R && g.n[2] >= 3 * R;
+    const int H3 = ndim == 3 ? step3d_halo_r<T>(R) : -1;
+    const bool blocked = p->tma && p->blocked3 && uniform && c_aligned && roomy && H3 >= 0 &&
+                         tma_maps<T>(p, op, derive, sp.minv, s3, cwb::S3_BX, cwb::S3_BY, H3);
+    const int Hrow = ndim == 3 ? tma_halo_nd<T, 3>(R) : tma_halo_nd<T, 2>(R);
+    const bool tma = !blocked && p->tma &&
+                     tma_maps<T>(p, op, derive, sp.minv, tp, ndim == 3 ? cwb::TMA_BX3 : cwb::TMA_BX2,
+                                 ndim == 3 ? cwb::TMA_BY3 : 1, Hrow);
     dim3 grid;
     int bx, by;
-    if (tma) {
+    if (blocked) {
+      bx = cwb::S3_BX;
+      by = cwb::S3_BY;
+      tma_grid(p, bx, by, grid, sp.chunk);
+    } else if (tma) {
       bx = ndim == 3 ? cwb::TMA_BX3 : cwb::TMA_BX2;
       by = ndim == 3 ? cwb::TMA_BY3 : 1;
       tma_grid(p, bx, by, grid, sp.chunk);
@@ -477,7 +528,16 @@ int translate(cwb_plan *p, const cwb_op &op, const size_t slot, cudaStream_t str
     sp.u2 = to_level(op.c, bytes);
     sp.ctr = p->ctr;
     tp.err = p->err;
-    if (tma) {
+    if (blocked) {
+      s3.s = sp;
+      s3.err = p->err;
+      out.push_back([s3, R, uniform, grid](cudaStream_t s, bool adv) {
+        cwb::Step3Params<T> q = s3;
+        if (adv)
+          q.s.flags |= cwb::K_ADV;
+        return step3d_r<T>(q, R, uniform, grid, s);
+      });
+    } else if (tma) {
       out.push_back([tp, ndim, R, uniform, grid](cudaStream_t s, bool adv) {
         cwb::StepTmaParams<T> q = tp;
         if (adv)
@@ -809,6 +869,8 @@ int cwb_plan_create(const cwb_grid *grid, cwb_plan **out) {
     p->chunk_override = std::atoi(env);
   if (const char *env = std::getenv("CWB_NO_TMA"))
     p->tma = std::atoi(env) == 0;
+  if (const char *env = std::getenv("CWB_STEP3D"))
+    p->blocked3 = std::atoi(env) != 0;
   if (cudaMalloc(&p->ctr, 2 * sizeof(int)) != cudaSuccess ||
       cudaMalloc(&p->err, sizeof(int)) != cudaSuccess ||
       cudaStreamCreateWithFlags(&p->lane, cudaStreamNonBlocking) != cudaSuccess ||
@@ -952,6 +1014,8 @@ int static_geometry(const cwb_grid &G, cwb_plan &p) {
     p.chunk_override = std::atoi(env);
   if (const char *env = std::getenv("CWB_NO_TMA"))
     p.tma = std::atoi(env) == 0;
+  if (const char *env = std::getenv("CWB_STEP3D"))
+    p.blocked3 = std::atoi(env) != 0;
   return CWB_OK;
 }
 

@@ -30,6 +30,15 @@ cudaError_t step_tma_unit(const StepTmaParams<T> &p, bool uniform, dim3 grid,
 template <typename T, int NDIM, int R>
 int step_tma_halo();  // the x halo of the staged box, a multiple of 16 bytes
 
+template <typename T>
+struct Step3Params;
+
+// the register-blocked 3D step of a uniform stiffness: 64 x 16 tiles, 256 threads
+template <typename T, int R>
+cudaError_t step3d_unit(const Step3Params<T> &p, bool uniform, dim3 grid, cudaStream_t stream);
+template <typename T, int R>
+int step3d_halo();  // the staged box's axis-2 halo, -1 where the kernel is not built
+
 template <typename T, int NDIM, int R>
 cudaError_t adjoint_unit(const AdjointParams<T> &p, bool uniform, int mode, dim3 grid,
                          cudaStream_t stream);

@@ -1,0 +1,611 @@
+// The 3D forward step of a uniform stiffness, register-blocked over TMA-staged planes.
+//
+// A block of 256 threads owns a 64 x 16 tile of the (axis-1, axis-2) plane and marches a
+// chunk of planes along axis 0. Each thread steps four consecutive axis-2 nodes of one
+// axis-1 row, so every tap it reads is a 16-byte row of four values.
+//
+//   * Axis 0 (the march) keeps, per node, the 2R values u(z-R+1) .. u(z+R) in a
+//     register queue fed one plane ahead from the staged planes, and carries g * D+ of
+//     the plane before as this plane's g * D- (the two are the same expression of the
+//     same values, so the reuse is bit-exact).
+//   * Axis 2 (fast) reads the row's 4 + 2H values once and forms D+ at the five faces
+//     x0 - 1 .. x0 + 3, each face's D+ serving as the next node's D-.
+//   * Axis 1 reads 2R rows of four from the staged box.
+//
+// One elected thread issues, per plane, a tensor-map copy of u^(t-1) over the tile and an
+// R-wide halo into a ring of R + 1 + PREFETCH boxes (the planes the axis-1/2 taps and the
+// queue's feed reach), and a copy of u^(t-2) and 1/m over the tile into a second ring.
+// Values past a wall take their mirrors (cuwave common.cuh:50-69): along axis 2 in the
+// row's registers, along axis 1 in the box rows past the wall (edge tiles only), along
+// axis 0 by reading the mirror plane from global memory at the chunk's ends.
+//
+// The node arithmetic is step.cuh's (cuwave fd_kernel + pml_kernel, scalar.cu:347-532) in
+// the same order; nodes on a pml slab, a Dirichlet wall, a folded refill row or a source
+// take the full per-node path after the plain update. Every wait on a copy is bounded
+// (tma.cuh): a lost copy raises the launch's error flag, the block drains what it issued
+// and leaves.
+#pragma once
+
+#include <type_traits>
+
+#include "step_tma.cuh"  // level_index, the pinned differences, the copies
+
+namespace cwb {
+
+constexpr int S3_BX = 64, S3_BY = 16, S3_THREADS = 256;
+
+template <typename T, int R>
+struct Step3Shape {
+  static constexpr int V = 16 / (int)sizeof(T);            // values per 16-byte row
+  static constexpr int H = (R + V - 1) / V * V;             // axis-2 halo, whole 16-byte rows
+  static constexpr int WB = S3_BX + 2 * H;                  // box width
+  static constexpr int HB = S3_BY + 2 * R;                  // box height
+  static constexpr int PREFETCH = 3;                        // planes issued past the feed
+  static constexpr int NS1 = R + 1 + PREFETCH;              // boxes of u^(t-1)
+  static constexpr int NS0 = PREFETCH + 1;                  // tiles of u^(t-2) and 1/m
+  static constexpr int BOX_BYTES = (WB * HB * (int)sizeof(T) + 127) / 128 * 128;
+  static constexpr int TILE_BYTES = S3_BX * S3_BY * (int)sizeof(T);
+  static constexpr int RING1 = NS1 * BOX_BYTES;
+  static constexpr int SMEM = RING1 + NS0 * 2 * TILE_BYTES + 128;
+  static constexpr int XR = 4 + 2 * H;                      // the row's run along axis 2
+  // the kernel is built for single precision up to radius 4 (its registers); the host
+  // sends other cases to the row kernel
+  static constexpr bool SUPPORTED = sizeof(T) == 4 && R <= 4;
+};
+
+template <typename T>
+struct Step3Params {
+  StepParams<T> s;
+  CUtensorMap map_u1;    // levels of b: (ext_F, n1, n0, levels), box (WB, HB, 1, 1)
+  CUtensorMap map_u0;    // levels of a: box (64, 16, 1, 1)
+  CUtensorMap map_minv;  // (ext_F, n1, n0), box (64, 16, 1)
+  int level_u1[3];
+  int level_u0[3];
+  int *err;
+};
+
+// four values from 16-byte aligned memory
+template <typename T>
+__device__ __forceinline__ void ld4(T *dst, const T *src) {
+  static_assert(sizeof(T) == 4, "16-byte rows of four");
+  const float4 v = *reinterpret_cast<const float4 *>(src);
+  dst[0] = v.x, dst[1] = v.y, dst[2] = v.z, dst[3] = v.w;
+}
+
+template <typename T>
+__device__ __forceinline__ void st4(T *dst, const T *v) {
+  static_assert(sizeof(T) == 4, "16-byte rows of four");
+  *reinterpret_cast<float4 *>(dst) = make_float4(v[0], v[1], v[2], v[3]);
+}
+
+// D+ of a node with the fused products of the pinned form (diffs_pinned's D+)
+template <typename T, int R, class Tap>
+__device__ __forceinline__ T dplus(const Tap &u, const T uc, const T *w) {
+  T d = u(1) - uc;
+  if (R > 1)
+    d = mul_rn(w[0], d);
+#pragma unroll
+  for (int k = 2; k <= R; ++k)
+    d = fma_rn(w[k - 1], u(k) - u(1 - k), d);
+  return d;
+}
+
+// The row's run past the axis-2 walls takes the mirrored values (cuwave common.cuh:50-54).
+// Low wall: node -1 - m sits at run index H - 1 - m, its mirror 3 + m at H + 3 + m. High
+// wall: with E the run index of node NF, node NF + m sits at E + m and its mirror
+// NF - 4 - m at E - 4 - m. E is a compile-time case of the run's place.
+template <typename T, int XR, int H>
+__device__ __forceinline__ void mirror_run_lo(T *xr, const T s) {
+#pragma unroll
+  for (int m = 0; m < H; ++m)
+    xr[H - 1 - m] = s * xr[H + 3 + m];
+}
+
+template <typename T, int XR, int E>
+__device__ __forceinline__ void mirror_run_hi(T *xr, const T s) {
+#pragma unroll
+  for (int m = 0; E + m < XR; ++m)
+    xr[E + m] = E - 4 - m >= 0 ? s * xr[E - 4 - m] : (T)0;
+}
+
+template <typename T, int R, bool UNIF>
+__global__ void __launch_bounds__(S3_THREADS, 2)
+    step3d_kernel(const __grid_constant__ Step3Params<T> P) {
+  using S = Step3Shape<T, R>;
+  static_assert(S::SUPPORTED, "the blocked 3D step is built for float up to radius 4");
+  static_assert(UNIF, "the blocked 3D step is built for a uniform stiffness");
+  constexpr int H = S::H, WB = S::WB, HB = S::HB, NS1 = S::NS1, NS0 = S::NS0, XR = S::XR;
+  constexpr int BX = S3_BX, BY = S3_BY;
+  extern __shared__ __align__(128) unsigned char s3_smem[];
+  __shared__ __align__(8) uint64_t full1[NS1];
+  __shared__ __align__(8) uint64_t full0[NS0];
+  unsigned char *ring1 = align_smem128(s3_smem);
+  unsigned char *ring0 = ring1 + S::RING1;
+
+  const StepParams<T> &p = P.s;
+  const Geometry &g = p.g;
+  const int t = step_index(p.ctr);
+  T *u2 = level<T>(p.u2, t);
+  const T *__restrict__ u1 = level<T>(p.u1, t);
+  const int lev1 = level_index(P.level_u1, t), lev0 = level_index(P.level_u0, t);
+
+  const int tid = threadIdx.x;
+  const int tq = tid & 15, ty = tid >> 4;  // the thread's quad along axis 2, its row
+  const int x0 = blockIdx.x * BX, y0 = blockIdx.y * BY;
+  const int xq = x0 + 4 * tq, py = y0 + ty;
+  const int N0 = g.n[0], NM = g.n[1], NF = g.n[2];
+  const int s0 = g.s[0], sM = g.s[1];
+  const int c0 = 1 + blockIdx.z * p.chunk;
+  const int c1 = min(N0 - 1, c0 + p.chunk);
+  const int dir0 = g.dir & 3, dirM = (g.dir >> 2) & 3, dirF = (g.dir >> 4) & 3;
+  const int flags = p.flags;
+  const bool leader = tid == 0;
+  const T gg = p.gconst;
+
+  // ring 1 holds the boxes of planes c0 .. lastbox, ring 0 the tiles of c0 .. c1 - 1
+  const int lastbox = min(c1 - 1 + R, N0 - 1);
+  const auto box = [&](const int plane) {
+    return reinterpret_cast<T *>(ring1 + ((unsigned)(plane - c0) % NS1) * S::BOX_BYTES);
+  };
+  const auto tile = [&](const int plane) {
+    return reinterpret_cast<T *>(ring0 + ((unsigned)(plane - c0) % NS0) * 2 * S::TILE_BYTES);
+  };
+  const auto parity1 = [&](const int plane) { return ((unsigned)(plane - c0) / NS1) & 1u; };
+  const auto parity0 = [&](const int plane) { return ((unsigned)(plane - c0) / NS0) & 1u; };
+  int issued1 = c0 - 1, issued0 = c0 - 1, arrived1 = c0 - 1, arrived0 = c0 - 1;
+  const auto issue1 = [&](const int plane) {
+    issued1 = plane;
+    uint64_t *bar = &full1[(unsigned)(plane - c0) % NS1];
+    mbar_expect(bar, WB * HB * (int)sizeof(T));
+    tma_load_4d(box(plane), &P.map_u1, bar, x0 - H, y0 - R, plane, lev1);
+  };
+  const auto issue0 = [&](const int plane) {
+    issued0 = plane;
+    uint64_t *bar = &full0[(unsigned)(plane - c0) % NS0];
+    const bool derive = flags & K_DERIVE;
+    mbar_expect(bar, S::TILE_BYTES * (derive ? 1 : 2));
+    T *dst = tile(plane);
+    tma_load_4d(dst, &P.map_u0, bar, x0, y0, plane, lev0);
+    if (!derive)
+      tma_load_3d(dst + BX * BY, &P.map_minv, bar, x0, y0, plane);
+  };
+
+  if (leader) {
+    for (int i = 0; i < NS1; ++i)
+      mbar_init(&full1[i], 1);
+    for (int i = 0; i < NS0; ++i)
+      mbar_init(&full0[i], 1);
+    fence_barrier_init();
+    prefetch_map(&P.map_u1);
+    prefetch_map(&P.map_u0);
+    if (!(flags & K_DERIVE))
+      prefetch_map(&P.map_minv);
+  }
+  __syncthreads();
+  if (leader && c0 < c1) {
+    for (int pl = c0; pl < c0 + NS1 - 1 && pl <= lastbox; ++pl)
+      issue1(pl);
+    for (int pl = c0; pl < c0 + NS0 - 1 && pl < c1; ++pl)
+      issue0(pl);
+  }
+
+  // box rows past an axis-1 wall take the mirrored rows; cells past both walls are read
+  // by no star stencil and are zeroed
+  const bool yedge = y0 - R < 0 || y0 + BY + R > NM;
+  const int ylo_end = max(0, min(HB, R - y0));
+  const int yhi_beg = max(0, min(HB, NM - (y0 - R)));
+  const auto yfix = [&](T *b) {
+    const int nrows = ylo_end + (HB - yhi_beg);
+    for (int c = tid; c < nrows * WB; c += S3_THREADS) {
+      const int ri = c / WB, bx = c % WB;
+      const int by = ri < ylo_end ? ri : yhi_beg + (ri - ylo_end);
+      const int xg = x0 - H + bx, yg = y0 - R + by;
+      T v = (T)0;
+      if (xg >= 0 && xg <= NF - 1) {
+        int sy;
+        const int my = mirror_node(yg, NM, dirM, sy);
+        const int ly = my - (y0 - R);
+        if (my >= 0 && my <= NM - 1 && ly >= 0 && ly < HB) {
+          const T m = b[ly * WB + bx];
+          v = sy < 0 ? -m : m;
+        }
+      }
+      b[by * WB + bx] = v;
+    }
+    // these generic-proxy writes precede the copy that later refills the stage
+    fence_proxy_async();
+  };
+
+  // the thread's nodes
+  const bool own = c0 < c1 && py >= 1 && py <= NM - 2 && xq + 3 >= 1 && xq <= NF - 2;
+  const bool full_quad = xq >= 1 && xq + 3 <= NF - 2;
+  const int e_hi = NF - (xq - H);  // run index of node NF
+  const bool fix_lo = xq - H < 0, fix_hi = e_hi <= XR - 1;
+  const T slo = (dirF & 1) ? (T)-1 : (T)1, shi = (dirF & 2) ? (T)-1 : (T)1;
+  const int crow = (ty + R) * WB + 4 * tq + H;  // the thread's first node in a box
+  const int ctile = ty * BX + 4 * tq;           // ... and in a tile
+  const long long gcol = (long long)py * sM + xq;
+  // u^(t-1) at plane b over the quad, through its mirror along axis 0, from global memory
+  const auto gquad = [&](const int b, T *dst) {
+    int sg;
+    const int m = mirror_node(b, N0, dir0, sg);
+    ld4(dst, u1 + (long long)m * s0 + gcol);
+    if (sg < 0) {
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+        dst[i] = -dst[i];
+    }
+  };
+
+  // the queue q[k] = u(z - R + 1 + k), k < 2R (what D+ at plane z reads), and g * D+
+  // of the plane before; D+ at plane c0 - 1 also reads u(c0 - R)
+  T q[2 * R][4];
+  T pz[4];
+  if (own) {
+    T first[4];
+    gquad(c0 - R, first);
+#pragma unroll
+    for (int k = 0; k < 2 * R - 1; ++k)
+      gquad(c0 - R + 1 + k, q[k]);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const auto tap = [&](const int j) { return j == -R + 1 ? first[i] : q[R - 2 + j][i]; };
+      pz[i] = mul_rn(dplus<T, R>(tap, tap(0), p.w), gg);
+    }
+  }
+
+  int sfirst = 0, slast = 0, srow = 0;
+  if (flags & K_SRC) {
+    const int blk = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+    sfirst = p.src_start[blk];
+    slast = p.src_start[blk + 1];
+    srow = p.sig_mul * t + p.sig_add;
+  }
+  // What the thread's nodes meet, fixed for the chunk: pml slabs, Dirichlet wall nodes
+  // and folded-refill rows of axes 1 and 2, and the block's sources. A quad that meets
+  // none of them (nor the axis-0 ones of its plane) takes the plain update alone.
+  const bool pml = flags & K_PML, damp = flags & K_DAMP;
+  const int fill = (flags & K_REFILL) ? p.refill : 0;
+  int inner = 0, xslab = 0, xheld = 0, xfill_lo = 0, xfill_hi = 0;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int px = xq + i;
+    if (px < 1 || px > NF - 2)
+      continue;
+    inner |= 1 << i;
+    if (pml && slab_row(px, NF, g.lo[2], g.hi[2]) >= 0)
+      xslab |= 1 << i;
+    if (held_wall(px, NF, dirF))
+      xheld |= 1 << i;
+    if (((fill >> 4) & 1) && px == 2)
+      xfill_lo |= 1 << i;
+    if (((fill >> 5) & 1) && px == NF - 3)
+      xfill_hi |= 1 << i;
+  }
+  const int yrow = pml ? slab_row(py, NM, g.lo[1], g.hi[1]) : -1;
+  const bool yheld = held_wall(py, NM, dirM);
+  const bool yfill_lo = ((fill >> 2) & 1) && py == 2, yfill_hi = ((fill >> 3) & 1) && py == NM - 3;
+  const bool has_src = sfirst < slast;
+  const bool thread_general = xslab || xheld || xfill_lo || xfill_hi || yrow >= 0 || yheld ||
+                              yfill_lo || yfill_hi || has_src;
+  const T mi_derived = (flags & K_DERIVE) ? (T)1 / p.sconst : (T)0;
+  // one pml memory update of a node and its share of the update (pml_kernel's order)
+  const auto pml_node = [&](T &v, const bool held, const T Dpu, const T Dmu, const T *prof,
+                            const int N, const int a, T &m0, T &m1, T &m2, const T f,
+                            const T mii) {
+    const T an = prof[a], bn = prof[N + a];
+    const T ah = prof[2 * N + a], bh = prof[3 * N + a];
+    const T ah1 = prof[2 * N + a - 1], bh1 = prof[3 * N + a - 1];
+    const T pp = bh * m0 + ah * Dpu;
+    const T pm = bh1 * m1 + ah1 * Dmu;
+    const T zz = bn * m2 + an * f * (gg * (Dpu + pp) - gg * (Dmu + pm));
+    m0 = pp;
+    m1 = pm;
+    m2 = zz;
+    if (!held)
+      v += mii * (f * (gg * pp - gg * pm) + zz);
+  };
+  // the memory rows of a quad contiguous along axis 2 (slabs of axes 0 and 1)
+  const auto pml_quad = [&](T *v, const int held, const T *Dpu, const T *Dmu, const int d,
+                            const int a, const long long si, const T *mi) {
+    T *aux = p.aux[d];
+    const long long sz = p.auxrow[d];
+    const T *prof = p.prof[d];
+    const int N = g.n[d];
+    const T f = p.f[d];
+    if (inner == 15) {
+      T m0[4], m1[4], m2[4];
+      ld4(m0, aux + si);
+      ld4(m1, aux + sz + si);
+      ld4(m2, aux + 2 * sz + si);
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+        pml_node(v[i], (held >> i) & 1, Dpu[i], Dmu[i], prof, N, a, m0[i], m1[i], m2[i], f, mi[i]);
+      st4(aux + si, m0);
+      st4(aux + sz + si, m1);
+      st4(aux + 2 * sz + si, m2);
+    } else {
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+        if ((inner >> i) & 1)
+          pml_node(v[i], (held >> i) & 1, Dpu[i], Dmu[i], prof, N, a, aux[si + i],
+                   aux[sz + si + i], aux[2 * sz + si + i], f, mi[i]);
+    }
+  };
+
+  // the boxes of planes c0 .. c0 + R - 1 before the first plane reads them
+  bool ok = true;
+  if (c0 < c1) {
+    bool good = true;
+    if (leader)
+      for (int pl = c0; pl < c0 + R && pl <= lastbox && good; ++pl) {
+        good = mbar_wait(&full1[(unsigned)(pl - c0) % NS1], parity1(pl));
+        if (good)
+          arrived1 = pl;
+      }
+    ok = __syncthreads_and(good);
+    if (ok && yedge) {
+      for (int pl = c0; pl < c0 + R && pl <= lastbox; ++pl)
+        yfix(box(pl));
+      __syncthreads();
+    }
+  }
+
+  for (int z = c0; z < c1 && ok; ++z) {
+    const int feed = z + R;  // the plane the queue takes in
+    bool good = true;
+    if (leader) {
+      if (feed <= lastbox)
+        good = mbar_wait(&full1[(unsigned)(feed - c0) % NS1], parity1(feed));
+      if (good)
+        good = mbar_wait(&full0[(unsigned)(z - c0) % NS0], parity0(z));
+    }
+    if (!__syncthreads_and(good)) {
+      ok = false;
+      break;
+    }
+    if (feed <= lastbox)
+      arrived1 = feed;
+    arrived0 = z;
+    // every thread is past plane z - 1: its stages take the planes PREFETCH ahead
+    if (leader) {
+      fence_proxy_async();
+      if (z + NS1 - 1 <= lastbox)
+        issue1(z + NS1 - 1);
+      if (z + NS0 - 1 < c1)
+        issue0(z + NS0 - 1);
+    }
+    // the feed's box is read along axis 1 from plane `feed` on, after barriers to come
+    if (yedge && feed <= lastbox)
+      yfix(box(feed));
+    if (!own)
+      continue;
+
+    const int zrow = pml ? slab_row(z, N0, g.lo[0], g.hi[0]) : -1;
+    const bool zheld = held_wall(z, N0, dir0);
+    const bool zfill_lo = (fill & 1) && z == 2, zfill_hi = ((fill >> 1) & 1) && z == N0 - 3;
+    const bool general = thread_general || zrow >= 0 || zheld || zfill_lo || zfill_hi;
+
+    const T *cb = box(z);
+    if (feed <= N0 - 1)
+      ld4(q[2 * R - 1], box(feed) + crow);
+    else
+      gquad(feed, q[2 * R - 1]);
+    // the row's run along axis 2, mirrored past the walls
+    const auto load_run = [&](T *xr) {
+#pragma unroll
+      for (int k = 0; k < XR / 4; ++k)
+        ld4(xr + 4 * k, cb + crow - H + 4 * k);
+      if (fix_lo)
+        mirror_run_lo<T, XR, H>(xr, slo);
+      if (fix_hi) {
+        switch (e_hi) {
+        case H + 2: mirror_run_hi<T, XR, H + 2>(xr, shi); break;
+        case H + 3: mirror_run_hi<T, XR, H + 3>(xr, shi); break;
+        case H + 4: mirror_run_hi<T, XR, H + 4>(xr, shi); break;
+        case H + 5: mirror_run_hi<T, XR, H + 5>(xr, shi); break;
+        case H + 6: mirror_run_hi<T, XR, H + 6>(xr, shi); break;
+        case H + 7: mirror_run_hi<T, XR, H + 7>(xr, shi); break;
+        default: break;
+        }
+      }
+    };
+    T xr[XR];
+    load_run(xr);
+    T uc[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+      uc[i] = xr[H + i];
+
+    // axis 2: D+ at faces x0 - 1 .. x0 + 3
+    T dx[5];
+#pragma unroll
+    for (int j = 0; j < 5; ++j) {
+      const auto tap = [&](const int k) { return xr[H - 1 + j + k]; };
+      dx[j] = dplus<T, R>(tap, xr[H - 1 + j], p.w);
+    }
+    // axis 1: D+ and D- from rows +k and -k
+    T dpy[4], dmy[4];
+    {
+      T rp[R + 1][4], rm[R + 1][4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+        rp[0][i] = rm[0][i] = uc[i];
+#pragma unroll
+      for (int k = 1; k <= R; ++k) {
+        ld4(rp[k], cb + crow + k * WB);
+        ld4(rm[k], cb + crow - k * WB);
+      }
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        T a = rp[1][i] - uc[i], b = uc[i] - rm[1][i];
+        if (R > 1) {
+          a = mul_rn(p.w[0], a);
+          b = mul_rn(p.w[0], b);
+        }
+#pragma unroll
+        for (int k = 2; k <= R; ++k) {
+          a = fma_rn(p.w[k - 1], rp[k][i] - rm[k - 1][i], a);
+          b = fma_rn(p.w[k - 1], rp[k - 1][i] - rm[k][i], b);
+        }
+        dpy[i] = a;
+        dmy[i] = b;
+      }
+    }
+    // axis 0 from the queue; the laplacian
+    T lap[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const auto tap = [&](const int j) { return q[R - 1 + j][i]; };
+      const T dpz = dplus<T, R>(tap, q[R - 1][i], p.w);
+      const T ddz = fma_rn(dpz, gg, -pz[i]);
+      pz[i] = mul_rn(dpz, gg);
+      const T ddy = fma_rn(dpy[i], gg, -mul_rn(dmy[i], gg));
+      const T ddx = fma_rn(dx[i + 1], gg, -mul_rn(dx[i], gg));
+      lap[i] = fma_rn(p.f[2], ddx, fma_rn(p.f[0], ddz, mul_rn(p.f[1], ddy)));
+    }
+    const T *tz = tile(z);
+    T old[4], mi[4];
+    ld4(old, tz + ctile);
+    if (flags & K_DERIVE) {
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+        mi[i] = mi_derived;
+    } else {
+      ld4(mi, tz + BX * BY + ctile);
+    }
+    const long long row = (long long)z * s0 + gcol;
+
+    T v[4];
+    if (!damp) {
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+        v[i] = -old[i] + (T)2 * uc[i] + mi[i] * lap[i];
+    } else {
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const T dmp = ((inner >> i) & 1) ? p.damping[row + i] : (T)0;
+        const T beta = (T)0.5 * mi[i] * dmp * p.dt;
+        v[i] = ((T)2 * uc[i] - old[i] * ((T)1 - beta) + mi[i] * lap[i]) / ((T)1 + beta);
+      }
+    }
+    if (general) {
+      // Dirichlet wall nodes hold zero; the pml memory of each lined axis the node sits
+      // in, axis by axis; the sources of this plane. The taps are read again here, so
+      // the plain update keeps no registers for them.
+      const int held = (zheld || yheld) ? inner : xheld;
+      T uc[4];
+      ld4(uc, cb + crow);
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+        if ((held >> i) & 1)
+          v[i] = (T)0;
+      if (zrow >= 0) {
+        T Dpu[4], Dmu[4], last[4];
+        gquad(z - R, last);  // the one plane the queue no longer holds
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          const auto tap = [&](const int j) { return j == -R ? last[i] : q[R - 1 + j][i]; };
+          diffs_plain<T, R>(tap, uc[i], p.w, Dpu[i], Dmu[i]);
+        }
+        pml_quad(v, held, Dpu, Dmu, 0, z, ((long long)zrow * NM + py) * g.ext[2] + xq, mi);
+      }
+      asm volatile("" ::: "memory");  // keeps the branches' loads apart (registers)
+      if (yrow >= 0) {
+        T Dpu[4], Dmu[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          const auto tap = [&](const int j) { return cb[crow + j * WB + i]; };
+          diffs_plain<T, R>(tap, uc[i], p.w, Dpu[i], Dmu[i]);
+        }
+        const int rows = g.lo[1] + g.hi[1];
+        pml_quad(v, held, Dpu, Dmu, 1, py, ((long long)z * rows + yrow) * g.ext[2] + xq, mi);
+      }
+      asm volatile("" ::: "memory");  // keeps the branches' loads apart (registers)
+      if (xslab) {
+        T xg[XR];
+        load_run(xg);
+        T *aux = p.aux[2];
+        const long long sz = p.auxrow[2];
+        const int rows = g.lo[2] + g.hi[2];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          if (!((xslab >> i) & 1))
+            continue;
+          const int px = xq + i;
+          const auto tap = [&](const int j) { return xg[H + i + j]; };
+          T Dpu, Dmu;
+          diffs_plain<T, R>(tap, uc[i], p.w, Dpu, Dmu);
+          const long long si = ((long long)z * NM + py) * rows + slab_row(px, NF, g.lo[2], g.hi[2]);
+          pml_node(v[i], (held >> i) & 1, Dpu, Dmu, p.prof[2], NF, px, aux[si], aux[sz + si],
+                   aux[2 * sz + si], p.f[2], mi[i]);
+        }
+      }
+      if (has_src) {
+        for (int e = sfirst; e < slast; ++e) {
+          const int4 en = p.src_entry[e];
+          if (en.x != z)
+            continue;
+#pragma unroll
+          for (int i = 0; i < 4; ++i)
+            if (en.y == ctile + i)
+              v[i] += p.src_weight[en.z] * p.signal[srow * p.nsrc + en.z];
+        }
+      }
+      if (fill) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+          if ((held >> i) & 1)
+            v[i] = (T)0;
+      }
+    }
+    if (inner == 15) {
+      st4(u2 + row, v);
+    } else {
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+        if ((inner >> i) & 1)
+          u2[row + i] = v[i];
+    }
+    if (general && fill) {
+      // the ghosts the folded refill writes from their mirror rows (sign past a
+      // Dirichlet face)
+      const auto put = [&](const long long at, const int i, const bool odd) {
+        u2[at] = odd ? -v[i] : v[i];
+      };
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        if (!((inner >> i) & 1))
+          continue;
+        if (zfill_lo)
+          put(row + i - 2LL * s0, i, dir0 & 1);
+        if (zfill_hi)
+          put(row + i + 2LL * s0, i, dir0 & 2);
+        if (yfill_lo)
+          put(row + i - 2LL * sM, i, dirM & 1);
+        if (yfill_hi)
+          put(row + i + 2LL * sM, i, dirM & 2);
+        if ((xfill_lo >> i) & 1)
+          put(row + i - 2, i, dirF & 1);
+        if ((xfill_hi >> i) & 1)
+          put(row + i + 2, i, dirF & 2);
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < 2 * R - 1; ++k)
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+        q[k][i] = q[k + 1][i];
+  }
+  if (!ok && leader) {
+    // a copy never arrived: flag it and drain what is in flight before leaving
+    atomicExch(P.err, 1);
+    for (int pl = arrived1 + 1; pl <= issued1; ++pl)
+      mbar_wait(&full1[(unsigned)(pl - c0) % NS1], parity1(pl));
+    for (int pl = arrived0 + 1; pl <= issued0; ++pl)
+      mbar_wait(&full0[(unsigned)(pl - c0) % NS0], parity0(pl));
+  }
+  finish_step(p.ctr, flags & K_ADV);
+}
+
+}  // namespace cwb

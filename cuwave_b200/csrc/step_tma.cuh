@@ -73,7 +73,7 @@ __global__ void __launch_bounds__(BX *(BY / RY), TMA_MIN_BLOCKS)
   extern __shared__ __align__(128) unsigned char tma_smem[];
   __shared__ __align__(8) uint64_t full[NS];
   unsigned char *ring =
-      reinterpret_cast<unsigned char *>((reinterpret_cast<uintptr_t>(tma_smem) + 127) & ~uintptr_t(127));
+      align_smem128(tma_smem);
 
   const StepParams<T> &p = P.s;
   const Geometry &g = p.g;
@@ -99,12 +99,12 @@ __global__ void __launch_bounds__(BX *(BY / RY), TMA_MIN_BLOCKS)
   // whether the box reaches past a wall or into the padding, so its halo needs mirrors
   const bool edge = x0 - H < 0 || x0 + BX + H > NF || (NDIM == 3 && (y0 - HY < 0 || y0 + BY + HY > NM));
 
-  const auto stage = [&](const int plane) { return ring + (plane % NS) * S::STAGE_BYTES; };
+  const auto stage = [&](const int plane) { return ring + ((unsigned)plane % NS) * S::STAGE_BYTES; };
   int issued = c0 - 1, arrived = c0 - 1;  // the last plane issued (leader) and waited for
   const auto issue = [&](const int plane) {
     issued = plane;
     unsigned char *st = stage(plane);
-    uint64_t *bar = &full[plane % NS];
+    uint64_t *bar = &full[(unsigned)plane % NS];
     const bool node_tiles = plane < c1;  // u^(t-2) and 1/m only for planes stepped here
     unsigned bytes = S::U1_BYTES;
     if (node_tiles)
@@ -216,7 +216,7 @@ __global__ void __launch_bounds__(BX *(BY / RY), TMA_MIN_BLOCKS)
   const auto arrive = [&](const int plane) -> bool {
     bool good = true;
     if (leader && plane <= last)
-      good = mbar_wait(&full[plane % NS], (unsigned)((plane - c0) / NS) & 1u);
+      good = mbar_wait(&full[(unsigned)plane % NS], ((unsigned)(plane - c0) / NS) & 1u);
     if (!__syncthreads_and(good))
       return false;
     arrived = plane;
@@ -434,7 +434,7 @@ __global__ void __launch_bounds__(BX *(BY / RY), TMA_MIN_BLOCKS)
     if (leader) {
       atomicExch(P.err, 1);
       for (int pl = arrived + 1; pl <= issued; ++pl)
-        mbar_wait(&full[pl % NS], (unsigned)((pl - c0) / NS) & 1u);
+        mbar_wait(&full[(unsigned)pl % NS], ((unsigned)(pl - c0) / NS) & 1u);
     }
   }
   finish_step(p.ctr, flags & K_ADV);

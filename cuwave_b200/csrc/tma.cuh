@@ -16,6 +16,13 @@ __device__ __forceinline__ unsigned smem_addr(const void *p) {
   return static_cast<unsigned>(__cvta_generic_to_shared(p));
 }
 
+// `base` advanced to the next 128-byte boundary by pointer arithmetic on the shared array
+// itself, so the compiler keeps every access through it in the shared window (a round
+// trip through an integer would leave it a generic pointer, with 64-bit address math)
+__device__ __forceinline__ unsigned char *align_smem128(unsigned char *base) {
+  return base + ((128u - (smem_addr(base) & 127u)) & 127u);
+}
+
 __device__ __forceinline__ void mbar_init(uint64_t *bar, const unsigned count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count)
                : "memory");

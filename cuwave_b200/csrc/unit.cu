@@ -4,6 +4,7 @@
 #include "launch.cuh"
 #include "step.cuh"
 #include "step_tma.cuh"
+#include "step3d.cuh"
 
 #if !defined(CWB_REAL) || !defined(CWB_NDIM) || !defined(CWB_RADIUS)
 #error "unit.cu is compiled with CWB_REAL, CWB_NDIM and CWB_RADIUS"
@@ -75,6 +76,35 @@ int step_tma_halo() {
   return TmaShape<T, NDIM, R, 32, 1>::H;
 }
 
+#if CWB_NDIM == 3
+template <typename T, int R, bool U>
+cudaError_t step3d_one(const Step3Params<T> &p, const dim3 grid, cudaStream_t s) {
+  if constexpr (!Step3Shape<T, R>::SUPPORTED || !U) {
+    return cudaErrorInvalidValue;
+  } else {
+    const size_t smem = Step3Shape<T, R>::SMEM;
+    const auto k = step3d_kernel<T, R, U>;
+    cudaError_t e = allow_smem(k, smem);
+    if (e != cudaSuccess)
+      return e;
+    k<<<grid, S3_THREADS, smem, s>>>(p);
+    return cudaGetLastError();
+  }
+}
+
+template <typename T, int R>
+cudaError_t step3d_unit(const Step3Params<T> &p, const bool uniform, const dim3 grid,
+                        cudaStream_t stream) {
+  return uniform ? step3d_one<T, R, true>(p, grid, stream) : step3d_one<T, R, false>(p, grid, stream);
+}
+
+template <typename T, int R>
+int step3d_halo() {
+  return Step3Shape<T, R>::SUPPORTED && Step3Shape<T, R>::SMEM <= 227 * 1024 ? Step3Shape<T, R>::H
+                                                                            : -1;
+}
+#endif
+
 template <typename T, int NDIM, int R>
 cudaError_t step_unit(const StepParams<T> &p, const bool uniform, const dim3 grid,
                       cudaStream_t stream) {
@@ -100,6 +130,11 @@ template cudaError_t step_unit<CWB_REAL, CWB_NDIM, CWB_RADIUS>(const StepParams<
 template cudaError_t step_tma_unit<CWB_REAL, CWB_NDIM, CWB_RADIUS>(
     const StepTmaParams<CWB_REAL> &, bool, dim3, cudaStream_t);
 template int step_tma_halo<CWB_REAL, CWB_NDIM, CWB_RADIUS>();
+#if CWB_NDIM == 3
+template cudaError_t step3d_unit<CWB_REAL, CWB_RADIUS>(const Step3Params<CWB_REAL> &, bool, dim3,
+                                                       cudaStream_t);
+template int step3d_halo<CWB_REAL, CWB_RADIUS>();
+#endif
 template cudaError_t adjoint_unit<CWB_REAL, CWB_NDIM, CWB_RADIUS>(
     const AdjointParams<CWB_REAL> &, bool, int, dim3, cudaStream_t);
 

@@ -3,7 +3,9 @@
 The adjoint is the exact transpose of the discrete forward step, so the gradient and
 the finite difference agree to the difference's own truncation (h^2) and round-off,
 as the reference's gradient tests check theirs (cuwave sensitivity_test.py:267-692,
-1196-1320: float64, h = 1e-7 relative, tolerances 2e-6 and 1e-8).
+1196-1320: float64 central differences). The cells checked are drawn among those whose
+gradient is at least 5% of the largest: elsewhere a difference quotient resolves only the
+loss's own round-off.
 """
 
 import numpy as np
@@ -18,7 +20,7 @@ def _problem(mode="history", checkpoints=None, pml=6, ndim=2):
     from cuwave_b200.autograd import Problem
     from cuwave_b200.signals import ricker
 
-    Nx = (34, 38) if ndim == 2 else (22, 20, 24)
+    Nx = (34, 38) if ndim == 2 else (36, 34, 38)
     N = 90 if ndim == 2 else 50
     dt = 0.5 * stable_dt((1.0,) * ndim, 1.3, 8)
     sim = AcousticWave(Nx=Nx, dx=(1.0,) * ndim, N=N, dt=dt, precision="float64", space_order=8,
@@ -57,11 +59,17 @@ def test_speed_gradient_matches_finite_differences(mode, checkpoints):
     loss = _loss(c, sig, problem, observed)
     loss.backward()
     grad = c.grad.cpu().numpy()
-    rng = np.random.default_rng(7)
+    # 16 random cells among those the misfit is sensitive to (a central difference at a
+    # cell of near-zero gradient measures only the loss's round-off, eps * loss / h)
     lo = problem.sim.pml.width + 2
-    cells = [tuple(rng.integers(lo, n - lo) for n in sim.Nx) for _ in range(8)]
+    inner = np.zeros(grad.shape, bool)
+    inner[tuple(slice(lo, n - lo) for n in sim.Nx)] = True
+    scale = np.abs(grad[inner]).max()
+    candidates = np.argwhere(inner & (np.abs(grad) >= 0.05 * scale))
+    rng = np.random.default_rng(7)
+    cells = [tuple(candidates[i]) for i in rng.choice(len(candidates), 16, replace=False)]
     for cell in cells:
-        h = 1e-6 * c0[cell]
+        h = 1e-5 * c0[cell]
         cp = c0.copy()
         cp[cell] += h
         cm = c0.copy()
@@ -69,7 +77,7 @@ def test_speed_gradient_matches_finite_differences(mode, checkpoints):
         lp = float(_loss(torch.tensor(cp, device=dev), sig, problem, observed))
         lm = float(_loss(torch.tensor(cm, device=dev), sig, problem, observed))
         fd = (lp - lm) / (2 * h)
-        assert grad[cell] == pytest.approx(fd, rel=2e-5, abs=1e-12 * abs(float(loss))), cell
+        assert abs(grad[cell] - fd) <= 1e-5 * abs(fd) + 1e-7 * scale, (cell, grad[cell], fd)
 
 
 def test_signal_gradient_matches_finite_differences():
@@ -81,15 +89,17 @@ def test_signal_gradient_matches_finite_differences():
     loss = _loss(c, sig, problem, observed)
     loss.backward()
     grad = sig.grad.cpu().numpy()
+    scale = np.abs(grad).max()
+    h = 1e-5 * np.abs(signal).max()
     for t in (5, 17, 33, 60):
-        h = 1e-6
         sp = signal.copy()
         sp[t, 0] += h
         sm = signal.copy()
         sm[t, 0] -= h
         lp = float(_loss(c, torch.tensor(sp, device=dev), problem, observed))
         lm = float(_loss(c, torch.tensor(sm, device=dev), problem, observed))
-        assert grad[t, 0] == pytest.approx((lp - lm) / (2 * h), rel=1e-6, abs=1e-14)
+        fd = (lp - lm) / (2 * h)
+        assert abs(grad[t, 0] - fd) <= 1e-6 * abs(fd) + 1e-8 * scale, (t, grad[t, 0], fd)
 
 
 @pytest.mark.parametrize("ndim", [2, 3])

@@ -59,10 +59,11 @@ def test_sensitivity_matches_reference(name):
 
 
 def _random_case(ndim, R, *, dirichlet=0, pml=0, uniform=False, damping=False, seed=1,
-                 dtype=np.float32, nsrc=3, nsens=5):
+                 dtype=np.float32, nsrc=3, nsens=5, Nx=None):
     """A seeded case with a heterogeneous stiffness, for the oracle and the product."""
     rng = np.random.default_rng(seed)
-    Nx = (27, 29) if ndim == 2 else (19, 21, 23)
+    if Nx is None:
+        Nx = (27, 29) if ndim == 2 else (19, 21, 23)
     Nx = tuple(n + 2 * pml for n in Nx)
     shape = o.padded(Nx)
     stiff = np.zeros(shape, dtype)
@@ -164,6 +165,22 @@ def test_uniform_stiffness_path_matches_oracle():
     field, _ = _product(case, meta)
     ref_field, _ = case.forward(meta["N"])
     np.testing.assert_array_equal(field, ref_field)
+
+
+@pytest.mark.parametrize("R,dirichlet,pml,damping", [
+    (1, 0b000000, 0, False), (2, 0b100110, 0, False), (3, 0b011001, 3, False),
+    (4, 0b100110, 4, False), (4, 0b000000, 0, True), (4, 0b111111, 0, False), (2, 0b010101, 6, False),
+])
+def test_blocked_uniform_step_matches_oracle(R, dirichlet, pml, damping):
+    """Several 64 x 16 tiles and 32-plane chunks, an axis-2 extent with padding, Dirichlet
+    and Neumann faces, pml slabs, damping and folded sources on the blocked 3D kernel of a
+    uniform stiffness."""
+    case, meta = _random_case(3, R, dirichlet=dirichlet, pml=pml, uniform=True, damping=damping,
+                              seed=11 + R, nsrc=6, nsens=9, Nx=(45, 37, 139))
+    field, traces = _product(case, meta)
+    ref_field, ref_traces = case.forward(meta["N"])
+    np.testing.assert_array_equal(field, ref_field)
+    np.testing.assert_array_equal(traces, ref_traces)
 
 
 @pytest.mark.parametrize("name", cases.GRADIENT)
