@@ -13,6 +13,7 @@
 
 #include "cuwave_b200.h"
 #include "launch.cuh"
+#include "pml.cuh"
 #include "step3d.cuh"
 #include "step_tma.cuh"
 
@@ -441,6 +442,95 @@ void fill_weights(const cwb_plan *p, T *w, T *f) {
     f[d] = d < p->geo.ndim ? (T)p->grid.factors[d] : (T)0;
 }
 
+template <typename T>
+cudaError_t pml_step_r(const cwb::PmlStepParams<T> &p, const int ndim, const int R,
+                       const bool u, const dim3 grid, cudaStream_t s) {
+  switch (ndim * 16 + R) {
+#define CWB_PML_CASE(D, RR) \
+  case D * 16 + RR: return cwb::pml_step_unit<T, D, RR>(p, u, grid, s);
+    CWB_PML_CASE(2, 1) CWB_PML_CASE(2, 2) CWB_PML_CASE(2, 3) CWB_PML_CASE(2, 4)
+    CWB_PML_CASE(2, 5) CWB_PML_CASE(2, 6) CWB_PML_CASE(2, 7) CWB_PML_CASE(2, 8)
+    CWB_PML_CASE(3, 1) CWB_PML_CASE(3, 2) CWB_PML_CASE(3, 3) CWB_PML_CASE(3, 4)
+    CWB_PML_CASE(3, 5) CWB_PML_CASE(3, 6) CWB_PML_CASE(3, 7) CWB_PML_CASE(3, 8)
+#undef CWB_PML_CASE
+  }
+  return cudaErrorInvalidValue;
+}
+
+// The pml launch of axes 1 and 2 after the blocked step (which advanced axis 0's memory in
+// its march): their slab union cut into disjoint boxes (axis-1 slabs over every interior
+// plane; axis-2 slabs over the axis-1 interior), so each slab node is visited once. The
+// launch's threads count quads of four fast-axis nodes.
+template <typename T>
+void pml_launch(const cwb_plan *p, const cwb::StepParams<T> &sp, const bool uniform,
+                std::vector<Launch> &out) {
+  const Geometry &g = p->geo;
+  const int nd = g.ndim, R = p->grid.radius;
+  cwb::PmlStepParams<T> pp;
+  std::memset(&pp, 0, sizeof pp);
+  pp.g = g;
+  for (int k = 0; k < cwb::MAXR; ++k)
+    pp.w[k] = sp.w[k];
+  for (int d = 0; d < 3; ++d) {
+    pp.f[d] = sp.f[d];
+    pp.prof[d] = sp.prof[d];
+    pp.aux[d] = sp.aux[d];
+    pp.auxrow[d] = sp.auxrow[d];
+  }
+  pp.gconst = sp.gconst;
+  pp.sconst = sp.sconst;
+  pp.flags = sp.flags & cwb::K_DERIVE;
+  pp.u1 = sp.u1;
+  pp.u2 = sp.u2;
+  pp.stiff = sp.stiff;
+  pp.minv = sp.minv;
+  pp.ctr = sp.ctr;
+  // interior range of each axis, narrowed past the slabs of the axes before it (axis 0,
+  // whose memory the blocked step advances in its march, stays whole)
+  int first[3], count[3];
+  for (int d = 0; d < nd; ++d) {
+    first[d] = 1;
+    count[d] = g.n[d] - 2;
+  }
+  long long total = 0;
+  for (int d = 1; d < nd; ++d) {
+    for (int side = 0; side < 2; ++side) {
+      const int w = side ? g.hi[d] : g.lo[d];
+      if (w <= 0)
+        continue;
+      for (int e = 0; e < nd; ++e) {
+        pp.org[pp.nbox][e] = first[e];
+        pp.ext[pp.nbox][e] = count[e];
+      }
+      pp.org[pp.nbox][d] = side ? g.n[d] - 1 - g.hi[d] : 1;
+      pp.ext[pp.nbox][d] = w;
+      bool empty = false;
+      for (int e = 0; e < nd; ++e)
+        empty |= pp.ext[pp.nbox][e] <= 0;
+      if (empty)
+        continue;
+      // a thread per quad of four fast-axis nodes (16-byte aligned) of one row
+      const int F = nd - 1, x0 = pp.org[pp.nbox][F], x1 = x0 + pp.ext[pp.nbox][F] - 1;
+      long long threads = (x1 >> 2) - (x0 >> 2) + 1;
+      for (int e = 0; e < F; ++e)
+        threads *= pp.ext[pp.nbox][e];
+      total += threads;
+      pp.end[pp.nbox++] = total;
+    }
+    first[d] = 1 + g.lo[d];
+    count[d] = g.n[d] - 2 - g.lo[d] - g.hi[d];
+  }
+  if (total == 0)
+    return;
+  const dim3 grid((unsigned)((total + cwb::PML_THREADS - 1) / cwb::PML_THREADS));
+  out.push_back([pp, nd, R, uniform, grid](cudaStream_t s, bool adv) {
+    cwb::PmlStepParams<T> q = pp;
+    if (adv)
+      q.flags |= cwb::K_ADV;
+    return pml_step_r<T>(q, nd, R, uniform, grid, s);
+  });
+}
+
 // the launches of one op, each taking (stream, advance)
 template <typename T>
 int translate(cwb_plan *p, const cwb_op &op, const size_t slot, cudaStream_t stream,
@@ -491,13 +581,50 @@ int translate(cwb_plan *p, const cwb_op &op, const size_t slot, cudaStream_t str
     const bool tma = !blocked && p->tma &&
                      tma_maps<T>(p, op, derive, sp.minv, tp, ndim == 3 ? cwb::TMA_BX3 : cwb::TMA_BX2,
                                  ndim == 3 ? cwb::TMA_BY3 : 1, Hrow);
+    if (blocked) {
+      // the plain update, then the pml memory, the sources and the refill, each a
+      // launch of its own in the order of cuwave's step
+      dim3 grid;
+      tma_grid(p, cwb::S3_BX, cwb::S3_BY, grid, sp.chunk);
+      sp.flags = flags;
+      sp.u0 = to_level(op.a, bytes);
+      sp.u1 = to_level(op.b, bytes);
+      sp.u2 = to_level(op.c, bytes);
+      sp.ctr = p->ctr;
+      s3.s = sp;
+      s3.err = p->err;
+      out.push_back([s3, R, uniform, grid](cudaStream_t s, bool adv) {
+        cwb::Step3Params<T> q = s3;
+        if (adv)
+          q.s.flags |= cwb::K_ADV;
+        return step3d_r<T>(q, R, uniform, grid, s);
+      });
+      if (op.flags & CWB_PML)
+        pml_launch<T>(p, sp, uniform, out);
+      if ((op.flags & CWB_FOLD_SOURCES) && op.points.num > 0) {
+        if (!op.points.weight || !op.points.record)
+          return fail(CWB_ERR_ARG, "folded sources need weights and a signal");
+        cwb_op ex;
+        std::memset(&ex, 0, sizeof ex);
+        ex.kind = CWB_OP_EXCITE;
+        ex.a = op.c;
+        ex.points = op.points;
+        if ((rc = translate<T>(p, ex, slot, stream, out)))
+          return rc;
+      }
+      if (op.flags & CWB_FOLD_REFILL) {
+        cwb_op rf;
+        std::memset(&rf, 0, sizeof rf);
+        rf.kind = CWB_OP_REFILL;
+        rf.a = op.c;
+        if ((rc = translate<T>(p, rf, slot, stream, out)))
+          return rc;
+      }
+      return CWB_OK;
+    }
     dim3 grid;
     int bx, by;
-    if (blocked) {
-      bx = cwb::S3_BX;
-      by = cwb::S3_BY;
-      tma_grid(p, bx, by, grid, sp.chunk);
-    } else if (tma) {
+    if (tma) {
       bx = ndim == 3 ? cwb::TMA_BX3 : cwb::TMA_BX2;
       by = ndim == 3 ? cwb::TMA_BY3 : 1;
       tma_grid(p, bx, by, grid, sp.chunk);
@@ -528,16 +655,7 @@ int translate(cwb_plan *p, const cwb_op &op, const size_t slot, cudaStream_t str
     sp.u2 = to_level(op.c, bytes);
     sp.ctr = p->ctr;
     tp.err = p->err;
-    if (blocked) {
-      s3.s = sp;
-      s3.err = p->err;
-      out.push_back([s3, R, uniform, grid](cudaStream_t s, bool adv) {
-        cwb::Step3Params<T> q = s3;
-        if (adv)
-          q.s.flags |= cwb::K_ADV;
-        return step3d_r<T>(q, R, uniform, grid, s);
-      });
-    } else if (tma) {
+    if (tma) {
       out.push_back([tp, ndim, R, uniform, grid](cudaStream_t s, bool adv) {
         cwb::StepTmaParams<T> q = tp;
         if (adv)

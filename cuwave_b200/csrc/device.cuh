@@ -29,15 +29,18 @@ struct DLevel {
   int mul, add, period;
 };
 
+// level index mul * t + add (mod period): 32-bit integer arithmetic, a 64-bit modulo
+// being a long emulated sequence on the GPU (step counts and level counts are far below
+// 2^31)
 template <typename T>
 __device__ __forceinline__ T *level(const DLevel &L, const int t) {
-  long long k = (long long)L.mul * t + L.add;
+  int k = L.mul * t + L.add;
   if (L.period > 0) {
     k %= L.period;
     if (k < 0)
       k += L.period;
   }
-  return reinterpret_cast<T *>(L.base + k * L.stride);
+  return reinterpret_cast<T *>(L.base + (long long)k * L.stride);
 }
 
 __device__ __forceinline__ int step_index(const int *ctr) {
@@ -90,6 +93,55 @@ __device__ __forceinline__ int node_image(const int b, const int N, const int od
 // whether node a is the wall node of a Dirichlet face of `odd` (cuwave common.cuh:43-46)
 __device__ __forceinline__ bool held_wall(const int a, const int N, const int odd) {
   return ((odd & 1) && a == 1) || ((odd & 2) && a == N - 2);
+}
+
+// A run of nodes along the fast axis past its walls takes the mirrored values (cuwave common.cuh:50-54).
+// Low wall: node -1 - m sits at run index H - 1 - m, its mirror 3 + m at H + 3 + m. High
+// wall: with E the run index of node NF, node NF + m sits at E + m and its mirror
+// NF - 4 - m at E - 4 - m. E is a compile-time case of the run's place.
+template <typename T, int XR, int H>
+__device__ __forceinline__ void mirror_run_lo(T *xr, const T s) {
+#pragma unroll
+  for (int m = 0; m < H; ++m)
+    xr[H - 1 - m] = s * xr[H + 3 + m];
+}
+
+template <typename T, int XR, int E>
+__device__ __forceinline__ void mirror_run_hi(T *xr, const T s) {
+#pragma unroll
+  for (int m = 0; E + m < XR; ++m)
+    xr[E + m] = E - 4 - m >= 0 ? s * xr[E - 4 - m] : (T)0;
+}
+
+// mirror_run_hi for the run's place e = E0, E0 + 1, .. < XR, chosen at run time
+template <typename T, int XR, int E>
+__device__ __forceinline__ void mirror_run_hi_at(T *xr, const T s, const int e) {
+  if (e == E)
+    mirror_run_hi<T, XR, E>(xr, s);
+  else if constexpr (E + 1 < XR)
+    mirror_run_hi_at<T, XR, E + 1>(xr, s, e);
+}
+
+// four consecutive values from 16-byte aligned memory, and back
+template <typename T>
+__device__ __forceinline__ void load4(T *dst, const T *src) {
+  if constexpr (sizeof(T) == 4) {
+    const float4 v = *reinterpret_cast<const float4 *>(src);
+    dst[0] = v.x, dst[1] = v.y, dst[2] = v.z, dst[3] = v.w;
+  } else {
+    const double2 a = reinterpret_cast<const double2 *>(src)[0];
+    const double2 b = reinterpret_cast<const double2 *>(src)[1];
+    dst[0] = a.x, dst[1] = a.y, dst[2] = b.x, dst[3] = b.y;
+  }
+}
+template <typename T>
+__device__ __forceinline__ void store4(T *dst, const T *v) {
+  if constexpr (sizeof(T) == 4) {
+    *reinterpret_cast<float4 *>(dst) = make_float4(v[0], v[1], v[2], v[3]);
+  } else {
+    reinterpret_cast<double2 *>(dst)[0] = make_double2(v[0], v[1]);
+    reinterpret_cast<double2 *>(dst)[1] = make_double2(v[2], v[3]);
+  }
 }
 
 template <typename T>

@@ -39,6 +39,13 @@ cudaError_t step3d_unit(const Step3Params<T> &p, bool uniform, dim3 grid, cudaSt
 template <typename T, int R>
 int step3d_halo();  // the staged box's axis-2 halo, -1 where the kernel is not built
 
+template <typename T>
+struct PmlStepParams;
+
+// the pml memory update of a step over the slab nodes (after the blocked step)
+template <typename T, int NDIM, int R>
+cudaError_t pml_step_unit(const PmlStepParams<T> &p, bool uniform, dim3 grid, cudaStream_t stream);
+
 template <typename T, int NDIM, int R>
 cudaError_t adjoint_unit(const AdjointParams<T> &p, bool uniform, int mode, dim3 grid,
                          cudaStream_t stream);

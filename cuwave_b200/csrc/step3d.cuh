@@ -19,9 +19,12 @@
 // row's registers, along axis 1 in the box rows past the wall (edge tiles only), along
 // axis 0 by reading the mirror plane from global memory at the chunk's ends.
 //
-// The node arithmetic is step.cuh's (cuwave fd_kernel + pml_kernel, scalar.cu:347-532) in
-// the same order; nodes on a pml slab, a Dirichlet wall, a folded refill row or a source
-// take the full per-node path after the plain update. Every wait on a copy is bounded
+// The node arithmetic is step.cuh's (cuwave fd_kernel, scalar.cu:347-427) in the same
+// order, Dirichlet wall nodes held at zero. An axis-0 pml slab row is a whole plane of
+// the march, so its memory terms (pml_kernel's axis 0) are applied here, uniformly over
+// the plane; those of axes 1 and 2 (pml.cuh), the sources and the ghost refill follow as
+// launches of their own, in the order of cuwave's step, so no quad branches apart from
+// the others of its plane. Every wait on a copy is bounded
 // (tma.cuh): a lost copy raises the launch's error flag, the block drains what it issued
 // and leaves.
 #pragma once
@@ -88,24 +91,6 @@ __device__ __forceinline__ T dplus(const Tap &u, const T uc, const T *w) {
   for (int k = 2; k <= R; ++k)
     d = fma_rn(w[k - 1], u(k) - u(1 - k), d);
   return d;
-}
-
-// The row's run past the axis-2 walls takes the mirrored values (cuwave common.cuh:50-54).
-// Low wall: node -1 - m sits at run index H - 1 - m, its mirror 3 + m at H + 3 + m. High
-// wall: with E the run index of node NF, node NF + m sits at E + m and its mirror
-// NF - 4 - m at E - 4 - m. E is a compile-time case of the run's place.
-template <typename T, int XR, int H>
-__device__ __forceinline__ void mirror_run_lo(T *xr, const T s) {
-#pragma unroll
-  for (int m = 0; m < H; ++m)
-    xr[H - 1 - m] = s * xr[H + 3 + m];
-}
-
-template <typename T, int XR, int E>
-__device__ __forceinline__ void mirror_run_hi(T *xr, const T s) {
-#pragma unroll
-  for (int m = 0; E + m < XR; ++m)
-    xr[E + m] = E - 4 - m >= 0 ? s * xr[E - 4 - m] : (T)0;
 }
 
 template <typename T, int R, bool UNIF>
@@ -254,84 +239,22 @@ __global__ void __launch_bounds__(S3_THREADS, 2)
     }
   }
 
-  int sfirst = 0, slast = 0, srow = 0;
-  if (flags & K_SRC) {
-    const int blk = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
-    sfirst = p.src_start[blk];
-    slast = p.src_start[blk + 1];
-    srow = p.sig_mul * t + p.sig_add;
-  }
-  // What the thread's nodes meet, fixed for the chunk: pml slabs, Dirichlet wall nodes
-  // and folded-refill rows of axes 1 and 2, and the block's sources. A quad that meets
-  // none of them (nor the axis-0 ones of its plane) takes the plain update alone.
-  const bool pml = flags & K_PML, damp = flags & K_DAMP;
-  const int fill = (flags & K_REFILL) ? p.refill : 0;
-  int inner = 0, xslab = 0, xheld = 0, xfill_lo = 0, xfill_hi = 0;
+  // What the thread's nodes meet: Dirichlet wall nodes, which hold zero. The pml memory
+  // of axes 1 and 2, the sources and the ghost refill run as launches of their own after
+  // this one, in the order of cuwave's step (fd, pml, excitation, refill).
+  const bool damp = flags & K_DAMP;
+  int inner = 0, xheld = 0;
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
     const int px = xq + i;
     if (px < 1 || px > NF - 2)
       continue;
     inner |= 1 << i;
-    if (pml && slab_row(px, NF, g.lo[2], g.hi[2]) >= 0)
-      xslab |= 1 << i;
     if (held_wall(px, NF, dirF))
       xheld |= 1 << i;
-    if (((fill >> 4) & 1) && px == 2)
-      xfill_lo |= 1 << i;
-    if (((fill >> 5) & 1) && px == NF - 3)
-      xfill_hi |= 1 << i;
   }
-  const int yrow = pml ? slab_row(py, NM, g.lo[1], g.hi[1]) : -1;
   const bool yheld = held_wall(py, NM, dirM);
-  const bool yfill_lo = ((fill >> 2) & 1) && py == 2, yfill_hi = ((fill >> 3) & 1) && py == NM - 3;
-  const bool has_src = sfirst < slast;
-  const bool thread_general = xslab || xheld || xfill_lo || xfill_hi || yrow >= 0 || yheld ||
-                              yfill_lo || yfill_hi || has_src;
   const T mi_derived = (flags & K_DERIVE) ? (T)1 / p.sconst : (T)0;
-  // one pml memory update of a node and its share of the update (pml_kernel's order)
-  const auto pml_node = [&](T &v, const bool held, const T Dpu, const T Dmu, const T *prof,
-                            const int N, const int a, T &m0, T &m1, T &m2, const T f,
-                            const T mii) {
-    const T an = prof[a], bn = prof[N + a];
-    const T ah = prof[2 * N + a], bh = prof[3 * N + a];
-    const T ah1 = prof[2 * N + a - 1], bh1 = prof[3 * N + a - 1];
-    const T pp = bh * m0 + ah * Dpu;
-    const T pm = bh1 * m1 + ah1 * Dmu;
-    const T zz = bn * m2 + an * f * (gg * (Dpu + pp) - gg * (Dmu + pm));
-    m0 = pp;
-    m1 = pm;
-    m2 = zz;
-    if (!held)
-      v += mii * (f * (gg * pp - gg * pm) + zz);
-  };
-  // the memory rows of a quad contiguous along axis 2 (slabs of axes 0 and 1)
-  const auto pml_quad = [&](T *v, const int held, const T *Dpu, const T *Dmu, const int d,
-                            const int a, const long long si, const T *mi) {
-    T *aux = p.aux[d];
-    const long long sz = p.auxrow[d];
-    const T *prof = p.prof[d];
-    const int N = g.n[d];
-    const T f = p.f[d];
-    if (inner == 15) {
-      T m0[4], m1[4], m2[4];
-      ld4(m0, aux + si);
-      ld4(m1, aux + sz + si);
-      ld4(m2, aux + 2 * sz + si);
-#pragma unroll
-      for (int i = 0; i < 4; ++i)
-        pml_node(v[i], (held >> i) & 1, Dpu[i], Dmu[i], prof, N, a, m0[i], m1[i], m2[i], f, mi[i]);
-      st4(aux + si, m0);
-      st4(aux + sz + si, m1);
-      st4(aux + 2 * sz + si, m2);
-    } else {
-#pragma unroll
-      for (int i = 0; i < 4; ++i)
-        if ((inner >> i) & 1)
-          pml_node(v[i], (held >> i) & 1, Dpu[i], Dmu[i], prof, N, a, aux[si + i],
-                   aux[sz + si + i], aux[2 * sz + si + i], f, mi[i]);
-    }
-  };
 
   // the boxes of planes c0 .. c0 + R - 1 before the first plane reads them
   bool ok = true;
@@ -381,10 +304,8 @@ __global__ void __launch_bounds__(S3_THREADS, 2)
     if (!own)
       continue;
 
-    const int zrow = pml ? slab_row(z, N0, g.lo[0], g.hi[0]) : -1;
-    const bool zheld = held_wall(z, N0, dir0);
-    const bool zfill_lo = (fill & 1) && z == 2, zfill_hi = ((fill >> 1) & 1) && z == N0 - 3;
-    const bool general = thread_general || zrow >= 0 || zheld || zfill_lo || zfill_hi;
+    const int held = (yheld || held_wall(z, N0, dir0)) ? inner : xheld;
+    const int zrow = (flags & K_PML) ? slab_row(z, N0, g.lo[0], g.hi[0]) : -1;
 
     const T *cb = box(z);
     if (feed <= N0 - 1)
@@ -489,74 +410,62 @@ __global__ void __launch_bounds__(S3_THREADS, 2)
         v[i] = ((T)2 * uc[i] - old[i] * ((T)1 - beta) + mi[i] * lap[i]) / ((T)1 + beta);
       }
     }
-    if (general) {
-      // Dirichlet wall nodes hold zero; the pml memory of each lined axis the node sits
-      // in, axis by axis; the sources of this plane. The taps are read again here, so
-      // the plain update keeps no registers for them.
-      const int held = (zheld || yheld) ? inner : xheld;
-      T uc[4];
-      ld4(uc, cb + crow);
+    // Dirichlet wall nodes hold zero
 #pragma unroll
-      for (int i = 0; i < 4; ++i)
-        if ((held >> i) & 1)
-          v[i] = (T)0;
-      if (zrow >= 0) {
-        T Dpu[4], Dmu[4], last[4];
-        gquad(z - R, last);  // the one plane the queue no longer holds
+    for (int i = 0; i < 4; ++i)
+      if ((held >> i) & 1)
+        v[i] = (T)0;
+    if (zrow >= 0) {
+      // an axis-0 slab row: the plane's pml memory (pml_kernel's axis 0), its taps from
+      // the queue and the one plane the queue no longer holds
+      T last[4], Dpu[4], Dmu[4];
+      gquad(z - R, last);
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const auto tap = [&](const int j) { return j == -R ? last[i] : q[R - 1 + j][i]; };
+        diffs_plain<T, R>(tap, uc[i], p.w, Dpu[i], Dmu[i]);
+      }
+      const T *prof = p.prof[0];
+      const T an = prof[z], bn = prof[N0 + z];
+      const T ah = prof[2 * N0 + z], bh = prof[3 * N0 + z];
+      const T ah1 = prof[2 * N0 + z - 1], bh1 = prof[3 * N0 + z - 1];
+      const T f = p.f[0];
+      T *aux = p.aux[0];
+      const long long sz = p.auxrow[0];
+      T *m = aux + ((long long)zrow * NM + py) * g.ext[2] + xq;
+      T m0[4], m1[4], m2[4];
+      if (inner == 15) {
+        ld4(m0, m), ld4(m1, m + sz), ld4(m2, m + 2 * sz);
+      } else {
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
-          const auto tap = [&](const int j) { return j == -R ? last[i] : q[R - 1 + j][i]; };
-          diffs_plain<T, R>(tap, uc[i], p.w, Dpu[i], Dmu[i]);
+          const bool on = (inner >> i) & 1;
+          m0[i] = on ? m[i] : (T)0;
+          m1[i] = on ? m[sz + i] : (T)0;
+          m2[i] = on ? m[2 * sz + i] : (T)0;
         }
-        pml_quad(v, held, Dpu, Dmu, 0, z, ((long long)zrow * NM + py) * g.ext[2] + xq, mi);
       }
-      asm volatile("" ::: "memory");  // keeps the branches' loads apart (registers)
-      if (yrow >= 0) {
-        T Dpu[4], Dmu[4];
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          const auto tap = [&](const int j) { return cb[crow + j * WB + i]; };
-          diffs_plain<T, R>(tap, uc[i], p.w, Dpu[i], Dmu[i]);
-        }
-        const int rows = g.lo[1] + g.hi[1];
-        pml_quad(v, held, Dpu, Dmu, 1, py, ((long long)z * rows + yrow) * g.ext[2] + xq, mi);
+      for (int i = 0; i < 4; ++i) {
+        const T pp = bh * m0[i] + ah * Dpu[i];
+        const T pm = bh1 * m1[i] + ah1 * Dmu[i];
+        const T zz = bn * m2[i] + an * f * (gg * (Dpu[i] + pp) - gg * (Dmu[i] + pm));
+        m0[i] = pp;
+        m1[i] = pm;
+        m2[i] = zz;
+        if (!((held >> i) & 1))
+          v[i] += mi[i] * (f * (gg * pp - gg * pm) + zz);
       }
-      asm volatile("" ::: "memory");  // keeps the branches' loads apart (registers)
-      if (xslab) {
-        T xg[XR];
-        load_run(xg);
-        T *aux = p.aux[2];
-        const long long sz = p.auxrow[2];
-        const int rows = g.lo[2] + g.hi[2];
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          if (!((xslab >> i) & 1))
-            continue;
-          const int px = xq + i;
-          const auto tap = [&](const int j) { return xg[H + i + j]; };
-          T Dpu, Dmu;
-          diffs_plain<T, R>(tap, uc[i], p.w, Dpu, Dmu);
-          const long long si = ((long long)z * NM + py) * rows + slab_row(px, NF, g.lo[2], g.hi[2]);
-          pml_node(v[i], (held >> i) & 1, Dpu, Dmu, p.prof[2], NF, px, aux[si], aux[sz + si],
-                   aux[2 * sz + si], p.f[2], mi[i]);
-        }
-      }
-      if (has_src) {
-        for (int e = sfirst; e < slast; ++e) {
-          const int4 en = p.src_entry[e];
-          if (en.x != z)
-            continue;
-#pragma unroll
-          for (int i = 0; i < 4; ++i)
-            if (en.y == ctile + i)
-              v[i] += p.src_weight[en.z] * p.signal[srow * p.nsrc + en.z];
-        }
-      }
-      if (fill) {
+      if (inner == 15) {
+        st4(m, m0), st4(m + sz, m1), st4(m + 2 * sz, m2);
+      } else {
 #pragma unroll
         for (int i = 0; i < 4; ++i)
-          if ((held >> i) & 1)
-            v[i] = (T)0;
+          if ((inner >> i) & 1) {
+            m[i] = m0[i];
+            m[sz + i] = m1[i];
+            m[2 * sz + i] = m2[i];
+          }
       }
     }
     if (inner == 15) {
@@ -566,30 +475,6 @@ __global__ void __launch_bounds__(S3_THREADS, 2)
       for (int i = 0; i < 4; ++i)
         if ((inner >> i) & 1)
           u2[row + i] = v[i];
-    }
-    if (general && fill) {
-      // the ghosts the folded refill writes from their mirror rows (sign past a
-      // Dirichlet face)
-      const auto put = [&](const long long at, const int i, const bool odd) {
-        u2[at] = odd ? -v[i] : v[i];
-      };
-#pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        if (!((inner >> i) & 1))
-          continue;
-        if (zfill_lo)
-          put(row + i - 2LL * s0, i, dir0 & 1);
-        if (zfill_hi)
-          put(row + i + 2LL * s0, i, dir0 & 2);
-        if (yfill_lo)
-          put(row + i - 2LL * sM, i, dirM & 1);
-        if (yfill_hi)
-          put(row + i + 2LL * sM, i, dirM & 2);
-        if ((xfill_lo >> i) & 1)
-          put(row + i - 2, i, dirF & 1);
-        if ((xfill_hi >> i) & 1)
-          put(row + i + 2, i, dirF & 2);
-      }
     }
 #pragma unroll
     for (int k = 0; k < 2 * R - 1; ++k)

@@ -54,13 +54,13 @@ struct TmaShape {
 };
 
 __device__ __forceinline__ int level_index(const int *L, const int t) {
-  long long k = (long long)L[0] * t + L[1];
+  int k = L[0] * t + L[1];
   if (L[2] > 0) {
     k %= L[2];
     if (k < 0)
       k += L[2];
   }
-  return (int)k;
+  return k;
 }
 
 template <typename T, int NDIM, int R, bool UNIF, int BX, int BY, int RY>

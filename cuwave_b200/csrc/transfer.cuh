@@ -148,11 +148,11 @@ __global__ void pml_aux_kernel(const PmlAuxParams<T> p) {
   if (active) {
     // decompose the slab index over the grid with axis d replaced by its rows
     int A[3] = {0, 0, 0};
-    long long rest = k;
+    int rest = (int)k;  // below memrow, an int
     int r = 0;
     for (int e = g.ndim - 1; e >= 0; --e) {
       const int extent = e == d ? lo + hi : g.ext[e];
-      const int c = (int)(rest % extent);
+      const int c = rest % extent;
       rest /= extent;
       if (e == d)
         r = c;

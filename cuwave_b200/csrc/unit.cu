@@ -4,6 +4,7 @@
 #include "launch.cuh"
 #include "step.cuh"
 #include "step_tma.cuh"
+#include "pml.cuh"
 #include "step3d.cuh"
 
 #if !defined(CWB_REAL) || !defined(CWB_NDIM) || !defined(CWB_RADIUS)
@@ -106,6 +107,16 @@ int step3d_halo() {
 #endif
 
 template <typename T, int NDIM, int R>
+cudaError_t pml_step_unit(const PmlStepParams<T> &p, const bool uniform, const dim3 grid,
+                          cudaStream_t s) {
+  if (uniform)
+    pml_step_kernel<T, NDIM, R, true><<<grid, PML_THREADS, 0, s>>>(p);
+  else
+    pml_step_kernel<T, NDIM, R, false><<<grid, PML_THREADS, 0, s>>>(p);
+  return cudaGetLastError();
+}
+
+template <typename T, int NDIM, int R>
 cudaError_t step_unit(const StepParams<T> &p, const bool uniform, const dim3 grid,
                       cudaStream_t stream) {
   return uniform ? step_one<T, NDIM, R, true>(p, grid, stream)
@@ -135,6 +146,8 @@ template cudaError_t step3d_unit<CWB_REAL, CWB_RADIUS>(const Step3Params<CWB_REA
                                                        cudaStream_t);
 template int step3d_halo<CWB_REAL, CWB_RADIUS>();
 #endif
+template cudaError_t pml_step_unit<CWB_REAL, CWB_NDIM, CWB_RADIUS>(
+    const PmlStepParams<CWB_REAL> &, bool, dim3, cudaStream_t);
 template cudaError_t adjoint_unit<CWB_REAL, CWB_NDIM, CWB_RADIUS>(
     const AdjointParams<CWB_REAL> &, bool, int, dim3, cudaStream_t);
 
