@@ -228,8 +228,9 @@ def config_line(w: dict, args) -> dict:
 
 # ------------------------------------------------------------------- our arm
 def step_kernel_ms(sim, mat_inputs, steps: int) -> float:
-    """Average duration of the dominant kernel (the fused step: fd + pml + sources +
-    refill) over `steps` back-to-back launches on the stream it runs on, by CUDA events."""
+    """Average duration of one march step (its launches: the blocked step with the axis-0
+    pml, the pml of axes 1-2, the sources, the refill) over `steps` back-to-back steps on
+    the stream they run on, by CUDA events."""
     import torch
 
     from cuwave_b200 import _native as nat
@@ -373,7 +374,8 @@ def run_ours(args) -> int:
 
 def step_kernel_name() -> str:
     if os.environ.get("CWB_STEP3D", "1") != "0" and os.environ.get("CWB_NO_TMA", "0") == "0":
-        return "step3d_kernel<float,4,uniform> (blocked 3D step: fd + pml + sources + refill)"
+        return ("one march step: step3d_kernel<float,4,uniform> (fd + axis-0 pml) + "
+                "pml_step_kernel (axes 1-2) + excite_kernel + refill_kernel")
     return "step_tma_kernel<float,3,4,uniform> (row step: fd + pml + sources + refill)"
 
 
@@ -385,14 +387,23 @@ def hbm_peak() -> tuple[float, str]:
 
 
 def profile_traffic(w: dict):
-    """DRAM bytes per launch of the step kernel from the committed ncu summary, scaled to
-    this workload's units, or None when no capture was summarised."""
+    """DRAM bytes of one march step (all its launches) from the committed ncu summary
+    (profiles/traffic.json, captured on a smaller grid): each kernel's bytes per unit
+    (interior node, slab node of axes 1-2, face node) scaled to this workload, or None
+    when no capture was summarised."""
     path = ROOT / "profiles" / "traffic.json"
     if not path.exists():
         return None
-    data = json.loads(path.read_text())
-    per_update = data.get("dram_bytes_per_interior_update")
-    return None if per_update is None else per_update * interior_updates(w)
+    data = json.loads(path.read_text())["kernels"]
+    n, wd = w["Nx"][0] - 2, w["width"]
+    units = {"interior nodes": n**3, "slab nodes of axes 1 and 2": n * 2 * wd * n + n * (n - 2 * wd) * 2 * wd,
+             "face nodes": 6 * n * n, "sources": w["source"].shape[1]}
+    total = 0.0
+    for entry in data.values():
+        if entry["unit"] not in units:
+            return None
+        total += entry["bytes_per_unit"] * units[entry["unit"]]
+    return total
 
 
 def main(argv=None) -> int:
