@@ -44,7 +44,7 @@ struct PmlStepParams {
 };
 
 template <typename T, int NDIM, int R, bool UNIF>
-__global__ void __launch_bounds__(PML_THREADS, 3) pml_step_kernel(const __grid_constant__ PmlStepParams<T> p) {
+__global__ void __launch_bounds__(PML_THREADS, 4) pml_step_kernel(const __grid_constant__ PmlStepParams<T> p) {
   constexpr int F = NDIM - 1;
   constexpr int H = (R + 3) / 4 * 4;  // the run's halo, whole quads
   constexpr int XR = 4 + 2 * H;
