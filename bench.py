@@ -257,6 +257,89 @@ def step_kernel_ms(sim, mat_inputs, steps: int) -> float:
     return a.elapsed_time(b) / steps
 
 
+def blob_speed(n: int, seed: int = 0) -> np.ndarray:
+    """Config 0's speed: 1 plus 8 seeded Gaussian blobs (A in [-0.3, 0.3], sigma in
+    [10, 40] cells at 512, scaled with the grid)."""
+    rng = np.random.default_rng(seed)
+    y, x = np.meshgrid(np.arange(n), np.arange(n), indexing="ij")
+    c = np.ones((n, n))
+    for _ in range(8):
+        a, s = rng.uniform(-0.3, 0.3), rng.uniform(10, 40) * n / 512
+        cy, cx = rng.uniform(1, n - 1, 2)
+        c += a * np.exp(-((y - cy) ** 2 + (x - cx) ** 2) / (2 * s * s))
+    return c
+
+
+def march_ms(plan, ops, t0: int, steps: int) -> float:
+    """CUDA-event time of `steps` march steps of `ops` on the stream they run on."""
+    import torch
+
+    plan.march(ops, t0, 3)
+    stream = torch.cuda.current_stream()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    a.record(stream)
+    plan.march(ops, t0, steps)
+    b.record(stream)
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) / steps
+
+
+def two_d_kernels(peak: float, steps: int = 200) -> dict:
+    """The 2D kernels at the shapes of configs 0 and 2 (512^2 Neumann; 2048^2 with a
+    20-cell PML): the forward step and the fused adjoint step (adjoint + gradients + pml
+    transpose + adjoint load), each as Gpt-updates/s and its algorithmic HBM bytes over its
+    CUDA-event time."""
+    import torch
+
+    from cuwave_b200 import AcousticWave, Pml, _native as nat
+    from cuwave_b200.sensitivity import _adjoint_ops
+    from cuwave_b200.stencils import stable_dt
+    from cuwave_b200.wave import flatten_indices, forward_ops, pml_memory, prepare_shot
+
+    dev = torch.device("cuda")
+    out = {}
+    for name, n, width in (("forward_2d_512", 512, 0), ("sensitivity_2d_2048", 2048, 20)):
+        c = blob_speed(n)
+        kappa2 = 0.25
+        dt = 0.5 * stable_dt((1.0, 1.0), float(c.max()), 8, "optimized")
+        N = steps + 8
+        sim = AcousticWave(Nx=(n, n), dx=(1.0, 1.0), N=N, dt=dt, precision="float32", space_order=8,
+                           pml=Pml(width=width, wavespeed=float(c.max())) if width else None,
+                           rho1=1.0, rho2=1.0, kappa1=1.0, kappa2=kappa2)
+        ind = torch.zeros(sim.Nx_padded, dtype=torch.float32, device=dev)
+        ind[:n, :n] = torch.as_tensor((1.0 / c**2 - 1.0) / (1.0 / kappa2 - 1.0), device=dev)
+        mat = sim.build_materials(ind)
+        signal = torch.zeros((N, 1), dtype=torch.float32, device=dev)
+        shot = prepare_shot(sim, mat, torch.tensor([[n // 2], [n // 2]], device=dev), signal)
+        interior = (n - 2) ** 2
+        slab = 2 * 2 * width * (n - 2) if width else 0
+        U = torch.zeros((2, *sim.Nx_padded), dtype=torch.float32, device=dev)
+        ops = forward_ops(sim, mat, nat.level(U, add=0, period=2), nat.level(U, add=1, period=2),
+                          nat.level(U, add=0, period=2), shot, pml_memory(sim, 3, dev))
+        plan = sim.plan()
+        ms = march_ms(plan, ops, 0, steps)
+        fwd_bytes = 16 * interior + 24 * slab
+        entry = {"forward_gpts": interior / (ms / 1e3) / 1e9, "forward_ms_per_step": ms,
+                 "forward_roofline_frac": fwd_bytes / (ms / 1e3) / 1e9 / peak}
+        if width:
+            V = torch.zeros((N + 2, *sim.Nx_padded), dtype=torch.float32, device=dev)
+            P = torch.zeros((2, *sim.Nx_padded), dtype=torch.float32, device=dev)
+            sensors = torch.stack([torch.full((256,), 50), torch.linspace(30, n - 31, 256).round().long()]).int().to(dev)
+            lin = flatten_indices(sim, sensors)
+            adj_signal = torch.zeros((N, 256), dtype=torch.float32, device=dev)
+            grads = sim.gradient_fields(mat)
+            aops = _adjoint_ops(sim, mat, P, pml_memory(sim, 5, dev), u_level=nat.level(V, mul=-1, add=N + 1),
+                                grads=grads, load=(lin, adj_signal, sim.excitation_weights(mat, lin)))
+            ams = march_ms(plan, aops, 0, steps)
+            adj_bytes = 32 * interior + 44 * slab
+            entry.update({"adjoint_gpts": interior / (ams / 1e3) / 1e9, "adjoint_ms_per_step": ams,
+                          "adjoint_roofline_frac": adj_bytes / (ams / 1e3) / 1e9 / peak})
+            del V, P
+        out[name] = entry
+    return out
+
+
 def run_ours(args) -> int:
     import torch
     import torch.distributed as dist
@@ -345,6 +428,7 @@ def run_ours(args) -> int:
     achieved = bytes_per_launch / (kernel_ms / 1e3) / 1e9
     peak, peak_kind = hbm_peak()
     traffic = profile_traffic(w)
+    kernels_2d = two_d_kernels(peak) if args.size == 512 and not args.no_2d and world == 1 else None
 
     if world > 1:
         dist.barrier()
@@ -367,6 +451,7 @@ def run_ours(args) -> int:
         "gpu_launches": launches,
         "clocks": clock,
         "kernel_updates_per_s": interior_updates(w) / (kernel_ms / 1e3) / 1e9,
+        "kernels_2d": kernels_2d,
     }
     print(json.dumps(line))
     return 0
@@ -419,6 +504,7 @@ def main(argv=None) -> int:
     parser.add_argument("--cpu-sample", type=int, default=6, help="time steps the CPU baseline runs")
     parser.add_argument("--ref-sample", type=int, default=3, help="time steps per reference bench step")
     parser.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
+    parser.add_argument("--no-2d", action="store_true", help="skip the 2D kernel measurements")
     args = parser.parse_args(argv)
     if args.impl == "reference":
         return run_reference(args)

@@ -14,6 +14,7 @@
 #include "cuwave_b200.h"
 #include "launch.cuh"
 #include "pml.cuh"
+#include "step2d.cuh"
 #include "step3d.cuh"
 #include "step_tma.cuh"
 
@@ -51,7 +52,7 @@ struct cwb_plan {
   int *ctr = nullptr;
   int *err = nullptr;  // raised by a kernel whose bounded wait ran out
   bool tma = true;     // stage planes with tensor-map copies where the layout allows
-  bool blocked3 = true;  // 3D steps of a uniform stiffness on the register-blocked kernel
+  bool blocked3 = true;  // uniform-stiffness steps on the register-blocked kernels (CWB_STEP3D=0: off)
   cudaStream_t lane = nullptr;
   cudaEvent_t fork = nullptr, join = nullptr;
   int sms = 148;
@@ -412,6 +413,37 @@ int step3d_halo_r(const int R) {
 }
 
 template <typename T>
+bool step2d_built_r(const int R) {
+  switch (R) {
+  case 1: return cwb::step2d_built<T, 1>();
+  case 2: return cwb::step2d_built<T, 2>();
+  case 3: return cwb::step2d_built<T, 3>();
+  case 4: return cwb::step2d_built<T, 4>();
+  case 5: return cwb::step2d_built<T, 5>();
+  case 6: return cwb::step2d_built<T, 6>();
+  case 7: return cwb::step2d_built<T, 7>();
+  case 8: return cwb::step2d_built<T, 8>();
+  }
+  return false;
+}
+
+template <typename T>
+cudaError_t step2d_r(const cwb::StepParams<T> &p, const int R, const bool u, const dim3 grid,
+                     cudaStream_t s) {
+  switch (R) {
+  case 1: return cwb::step2d_unit<T, 1>(p, u, grid, s);
+  case 2: return cwb::step2d_unit<T, 2>(p, u, grid, s);
+  case 3: return cwb::step2d_unit<T, 3>(p, u, grid, s);
+  case 4: return cwb::step2d_unit<T, 4>(p, u, grid, s);
+  case 5: return cwb::step2d_unit<T, 5>(p, u, grid, s);
+  case 6: return cwb::step2d_unit<T, 6>(p, u, grid, s);
+  case 7: return cwb::step2d_unit<T, 7>(p, u, grid, s);
+  case 8: return cwb::step2d_unit<T, 8>(p, u, grid, s);
+  }
+  return cudaErrorInvalidValue;
+}
+
+template <typename T>
 cudaError_t step3d_r(const cwb::Step3Params<T> &p, const int R, const bool u, const dim3 grid,
                      cudaStream_t s) {
   switch (R) {
@@ -581,26 +613,57 @@ int translate(cwb_plan *p, const cwb_op &op, const size_t slot, cudaStream_t str
     const bool tma = !blocked && p->tma &&
                      tma_maps<T>(p, op, derive, sp.minv, tp, ndim == 3 ? cwb::TMA_BX3 : cwb::TMA_BX2,
                                  ndim == 3 ? cwb::TMA_BY3 : 1, Hrow);
-    if (blocked) {
-      // the plain update, then the pml memory, the sources and the refill, each a
-      // launch of its own in the order of cuwave's step
-      dim3 grid;
-      tma_grid(p, cwb::S3_BX, cwb::S3_BY, grid, sp.chunk);
+    // 2D, a uniform stiffness, float, radius <= 4: the quad step, which reads u^(t-1),
+    // u^(t-2) and 1/m as 16-byte rows (levels and 1/m on 16-byte boundaries)
+    const auto aligned16 = [](const void *ptr, const long long stride_elems) {
+      return reinterpret_cast<uintptr_t>(ptr) % 16 == 0 && (stride_elems * (long long)sizeof(T)) % 16 == 0;
+    };
+    const bool quad2 = ndim == 2 && p->blocked3 && uniform && step2d_built_r<T>(R) &&
+                       aligned16(op.a.base, op.a.stride) && aligned16(op.b.base, op.b.stride) &&
+                       aligned16(op.c.base, op.c.stride) && (derive || aligned16(sp.minv, 0)) &&
+                       g.n[0] >= 3 * R && g.n[1] >= 3 * R;
+    if (quad2) {
+      // enough quads x row chunks to give every SM a few blocks of 128 threads
+      const long long rows = g.n[0] - 2, quads = (g.n[1] - 2) / 4 + 1;
+      const long long want = (long long)p->sms * 1024;
+      const int chunk = (int)std::max<long long>(1, std::min<long long>(rows, rows * quads / want));
+      sp.chunk = p->chunk_override > 0 ? p->chunk_override : chunk;
+      const long long threads = quads * ((rows + sp.chunk - 1) / sp.chunk);
+      const dim3 grid((unsigned)((threads + cwb::S2_THREADS - 1) / cwb::S2_THREADS));
       sp.flags = flags;
       sp.u0 = to_level(op.a, bytes);
       sp.u1 = to_level(op.b, bytes);
       sp.u2 = to_level(op.c, bytes);
       sp.ctr = p->ctr;
-      s3.s = sp;
-      s3.err = p->err;
-      out.push_back([s3, R, uniform, grid](cudaStream_t s, bool adv) {
-        cwb::Step3Params<T> q = s3;
+      out.push_back([sp, R, uniform, grid](cudaStream_t s, bool adv) {
+        cwb::StepParams<T> q = sp;
         if (adv)
-          q.s.flags |= cwb::K_ADV;
-        return step3d_r<T>(q, R, uniform, grid, s);
+          q.flags |= cwb::K_ADV;
+        return step2d_r<T>(q, R, uniform, grid, s);
       });
-      if (op.flags & CWB_PML)
-        pml_launch<T>(p, sp, uniform, out);
+    }
+    if (blocked || quad2) {
+      // after the update (and its pml memory), the sources and the refill, each a
+      // launch of its own in the order of cuwave's step
+      if (blocked) {
+        dim3 grid;
+        tma_grid(p, cwb::S3_BX, cwb::S3_BY, grid, sp.chunk);
+        sp.flags = flags;
+        sp.u0 = to_level(op.a, bytes);
+        sp.u1 = to_level(op.b, bytes);
+        sp.u2 = to_level(op.c, bytes);
+        sp.ctr = p->ctr;
+        s3.s = sp;
+        s3.err = p->err;
+        out.push_back([s3, R, uniform, grid](cudaStream_t s, bool adv) {
+          cwb::Step3Params<T> q = s3;
+          if (adv)
+            q.s.flags |= cwb::K_ADV;
+          return step3d_r<T>(q, R, uniform, grid, s);
+        });
+        if (op.flags & CWB_PML)
+          pml_launch<T>(p, sp, uniform, out);
+      }
       if ((op.flags & CWB_FOLD_SOURCES) && op.points.num > 0) {
         if (!op.points.weight || !op.points.record)
           return fail(CWB_ERR_ARG, "folded sources need weights and a signal");

@@ -39,6 +39,12 @@ cudaError_t step3d_unit(const Step3Params<T> &p, bool uniform, dim3 grid, cudaSt
 template <typename T, int R>
 int step3d_halo();  // the staged box's axis-2 halo, -1 where the kernel is not built
 
+// the 2D quad step of a uniform stiffness (float, radius <= 4), 128 threads a block
+template <typename T, int R>
+cudaError_t step2d_unit(const StepParams<T> &p, bool uniform, dim3 grid, cudaStream_t stream);
+template <typename T, int R>
+bool step2d_built();
+
 template <typename T>
 struct PmlStepParams;
 

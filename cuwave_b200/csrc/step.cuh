@@ -39,6 +39,18 @@ __device__ __forceinline__ void diffs_pinned(const Tap &u, const T uc, const T *
   }
 }
 
+// D+ of a node with the fused products of the pinned form (diffs_pinned's D+)
+template <typename T, int R, class Tap>
+__device__ __forceinline__ T dplus(const Tap &u, const T uc, const T *w) {
+  T d = u(1) - uc;
+  if (R > 1)
+    d = mul_rn(w[0], d);
+#pragma unroll
+  for (int k = 2; k <= R; ++k)
+    d = fma_rn(w[k - 1], u(k) - u(1 - k), d);
+  return d;
+}
+
 // D+ and D- with products and sums rounded apart, as cell_differences forms them
 template <typename T, int R, class Tap>
 __device__ __forceinline__ void diffs_plain(const Tap &u, const T uc, const T *w, T &Dp,

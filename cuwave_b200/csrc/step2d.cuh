@@ -1,0 +1,251 @@
+// The 2D forward step of a uniform stiffness: quads of four fast-axis nodes marching rows.
+//
+// A thread owns four consecutive axis-1 nodes (a quad, 16-byte aligned) and marches a
+// chunk of axis-0 rows. It keeps, per node, the 2R values u(z-R+1) .. u(z+R) of its
+// column in a register queue fed one row per step and carries g * D+ of the row before as
+// this row's g * D- (the same expression of the same values, so the reuse is bit-exact).
+// The axis-1 taps are the quad's run of 4 + 2H values: the queue's centre row and two
+// 16-byte loads beside it, which neighbouring threads share through L1. There is no
+// shared memory and no barrier: every load is a coalesced 16-byte row and warps run
+// independently.
+//
+// The node arithmetic is step.cuh's (cuwave fd_kernel, scalar.cu:347-427) in the same
+// order, Dirichlet wall nodes held at zero. An axis-0 pml slab row is a whole row of the
+// march, so its memory terms apply uniformly over the row; the axis-1 slab columns apply
+// theirs quad by quad after it (cuwave pml_kernel, scalar.cu:500-532, axes in order).
+// The sources and the ghost refill follow as launches of their own, in the order of
+// cuwave's step. Values past a wall take their mirrors (cuwave common.cuh:50-54): along
+// axis 1 in the run's registers, along axis 0 by reading the mirror row.
+#pragma once
+
+#include "step.cuh"
+
+namespace cwb {
+
+constexpr int S2_THREADS = 128;
+
+template <typename T, int R>
+struct Step2Shape {
+  static constexpr int H = (R + 3) / 4 * 4;  // the run's halo, whole quads
+  static constexpr int XR = 4 + 2 * H;
+  // float up to radius 4 (its registers); the host sends other cases to the row kernel
+  static constexpr bool SUPPORTED = sizeof(T) == 4 && R <= 4;
+};
+
+template <typename T, int R, bool UNIF>
+__global__ void __launch_bounds__(S2_THREADS, 4) step2d_kernel(const StepParams<T> p) {
+  using S = Step2Shape<T, R>;
+  static_assert(S::SUPPORTED && UNIF, "the 2D quad step is built for float, radius <= 4, a uniform stiffness");
+  constexpr int H = S::H, XR = S::XR;
+  const Geometry &g = p.g;
+  const int t = step_index(p.ctr);
+  const int N0 = g.n[0], NF = g.n[1], ext = g.ext[1];
+  const int nq = (NF - 2) / 4 + 1;  // quads covering nodes 0 .. NF - 2
+  const long long k = (long long)blockIdx.x * S2_THREADS + threadIdx.x;
+  const int quad = (int)(k % nq);
+  const int cz = (int)(k / nq);
+  const int c0 = 1 + cz * p.chunk;
+  const int c1 = min(N0 - 1, c0 + p.chunk);
+  const int xq = 4 * quad;
+  if (c0 < c1 && xq <= NF - 2) {
+    const T *__restrict__ u0 = level<T>(p.u0, t);
+    const T *__restrict__ u1 = level<T>(p.u1, t);
+    T *u2 = level<T>(p.u2, t);
+    const T *__restrict__ minv = p.minv;
+    const int dir0 = g.dir & 3, dirF = (g.dir >> 2) & 3;
+    const int s0 = g.s[0];
+    const int flags = p.flags;
+    const T gg = p.gconst;
+    // the quad's interior nodes, its Dirichlet wall nodes, its axis-1 slab nodes
+    int inner = 0, xheld = 0, xslab = 0;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int x = xq + i;
+      if (x < 1 || x > NF - 2)
+        continue;
+      inner |= 1 << i;
+      if (held_wall(x, NF, dirF))
+        xheld |= 1 << i;
+      if ((flags & K_PML) && slab_row(x, NF, g.lo[1], g.hi[1]) >= 0)
+        xslab |= 1 << i;
+    }
+    const bool fix_lo = xq - H < 0;
+    const int e_hi = NF - (xq - H);
+    const bool fix_hi = e_hi <= XR - 1;
+    const T slo = (dirF & 1) ? (T)-1 : (T)1, shi = (dirF & 2) ? (T)-1 : (T)1;
+    const T mi_derived = (flags & K_DERIVE) ? (T)1 / p.sconst : (T)0;
+    // u^(t-1) over the quad at row b, through its mirror past the axis-0 walls
+    const auto row4 = [&](const int b, T *dst) {
+      int sg = 1;
+      const int m = (b >= 0 && b <= N0 - 1) ? b : mirror_node(b, N0, dir0, sg);
+      load4(dst, u1 + (long long)m * s0 + xq);
+      if (sg < 0) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+          dst[i] = -dst[i];
+      }
+    };
+    // the queue q[k] = u(z - R + 1 + k) and g * D+ of the row before (which reads u(c0 - R))
+    T q[2 * R][4], pz[4];
+    {
+      T first[4];
+      row4(c0 - R, first);
+#pragma unroll
+      for (int j = 0; j < 2 * R - 1; ++j)
+        row4(c0 - R + 1 + j, q[j]);
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const auto tap = [&](const int j) { return j == -R + 1 ? first[i] : q[R - 2 + j][i]; };
+        pz[i] = mul_rn(dplus<T, R>(tap, tap(0), p.w), gg);
+      }
+    }
+    for (int z = c0; z < c1; ++z) {
+      row4(z + R, q[2 * R - 1]);
+      const long long row = (long long)z * s0 + xq;
+      // the run along axis 1: left quad, the queue's centre, right quad; mirrored
+      T xr[XR];
+#pragma unroll
+      for (int c = 0; c < XR / 4; ++c) {
+        const int x = xq - H + 4 * c;
+        if (c == H / 4) {
+#pragma unroll
+          for (int i = 0; i < 4; ++i)
+            xr[4 * c + i] = q[R - 1][i];
+        } else if (x >= 0 && x + 3 <= ext - 1) {
+          load4(xr + 4 * c, u1 + row - H + 4 * c);
+        } else {
+#pragma unroll
+          for (int i = 0; i < 4; ++i)
+            xr[4 * c + i] = (T)0;
+        }
+      }
+      if (fix_lo)
+        mirror_run_lo<T, XR, H>(xr, slo);
+      if (fix_hi)
+        mirror_run_hi_at<T, XR, H + 2>(xr, shi, e_hi);
+      T old[4], mi[4];
+      load4(old, u0 + row);
+      if (flags & K_DERIVE) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+          mi[i] = mi_derived;
+      } else {
+        load4(mi, minv + row);
+      }
+      // axis 1: D+ at faces x0 - 1 .. x0 + 3; axis 0 from the queue; the laplacian
+      T dx[5];
+#pragma unroll
+      for (int j = 0; j < 5; ++j) {
+        const auto tap = [&](const int kk) { return xr[H - 1 + j + kk]; };
+        dx[j] = dplus<T, R>(tap, xr[H - 1 + j], p.w);
+      }
+      T v[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const auto tap = [&](const int j) { return q[R - 1 + j][i]; };
+        const T dpz = dplus<T, R>(tap, q[R - 1][i], p.w);
+        const T ddz = fma_rn(dpz, gg, -pz[i]);
+        pz[i] = mul_rn(dpz, gg);
+        const T ddx = fma_rn(dx[i + 1], gg, -mul_rn(dx[i], gg));
+        const T lap = R == 1 ? fma_rn(p.f[0], ddz, mul_rn(p.f[1], ddx))
+                             : fma_rn(p.f[1], ddx, mul_rn(p.f[0], ddz));
+        const T uc = q[R - 1][i];
+        if (flags & K_DAMP) {
+          const T dmp = ((inner >> i) & 1) ? p.damping[row + i] : (T)0;
+          const T beta = (T)0.5 * mi[i] * dmp * p.dt;
+          v[i] = ((T)2 * uc - old[i] * ((T)1 - beta) + mi[i] * lap) / ((T)1 + beta);
+        } else {
+          v[i] = -old[i] + (T)2 * uc + mi[i] * lap;
+        }
+      }
+      const int held = held_wall(z, N0, dir0) ? inner : xheld;
+      if (held) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+          if ((held >> i) & 1)
+            v[i] = (T)0;
+      }
+      if (flags & K_PML) {
+        // one node's memory step and share of the update along axis d (pml_kernel's order)
+        const auto node = [&](const int i, const int d, const int a, const int N, const T Dpu,
+                              const T Dmu, T &m0, T &m1, T &m2) {
+          const T *prof = p.prof[d];
+          const T an = prof[a], bn = prof[N + a];
+          const T ah = prof[2 * N + a], bh = prof[3 * N + a];
+          const T ah1 = prof[2 * N + a - 1], bh1 = prof[3 * N + a - 1];
+          const T f = p.f[d];
+          const T pp = bh * m0 + ah * Dpu;
+          const T pm = bh1 * m1 + ah1 * Dmu;
+          const T zz = bn * m2 + an * f * (gg * (Dpu + pp) - gg * (Dmu + pm));
+          m0 = pp;
+          m1 = pm;
+          m2 = zz;
+          if (!((held >> i) & 1))
+            v[i] += mi[i] * (f * (gg * pp - gg * pm) + zz);
+        };
+        const int zrow = slab_row(z, N0, g.lo[0], g.hi[0]);
+        if (zrow >= 0) {
+          // an axis-0 slab row: its memory row is contiguous over the quad
+          T last[4];
+          row4(z - R, last);
+          T *aux = p.aux[0];
+          const long long sz = p.auxrow[0], si = (long long)zrow * ext + xq;
+          T m0[4], m1[4], m2[4];
+          load4(m0, aux + si);
+          load4(m1, aux + sz + si);
+          load4(m2, aux + 2 * sz + si);
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            if (!((inner >> i) & 1))
+              continue;
+            const auto tap = [&](const int j) { return j == -R ? last[i] : q[R - 1 + j][i]; };
+            T Dpu, Dmu;
+            diffs_plain<T, R>(tap, q[R - 1][i], p.w, Dpu, Dmu);
+            node(i, 0, z, N0, Dpu, Dmu, m0[i], m1[i], m2[i]);
+          }
+          // the quad's nodes outside the interior keep their memory
+#pragma unroll
+          for (int i = 0; i < 4; ++i)
+            if ((inner >> i) & 1) {
+              aux[si + i] = m0[i];
+              aux[sz + si + i] = m1[i];
+              aux[2 * sz + si + i] = m2[i];
+            }
+        }
+        if (xslab) {
+          T *aux = p.aux[1];
+          const long long sz = p.auxrow[1];
+          const int lo = g.lo[1], hi = g.hi[1];
+          const long long base = (long long)z * (lo + hi);
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            if (!((xslab >> i) & 1))
+              continue;
+            const int x = xq + i;
+            const auto tap = [&](const int j) { return xr[H + i + j]; };
+            T Dpu, Dmu;
+            diffs_plain<T, R>(tap, xr[H + i], p.w, Dpu, Dmu);
+            const long long si = base + slab_row(x, NF, lo, hi);
+            node(i, 1, x, NF, Dpu, Dmu, aux[si], aux[sz + si], aux[2 * sz + si]);
+          }
+        }
+      }
+      if (inner == 15) {
+        store4(u2 + row, v);
+      } else {
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+          if ((inner >> i) & 1)
+            u2[row + i] = v[i];
+      }
+#pragma unroll
+      for (int j = 0; j < 2 * R - 1; ++j)
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+          q[j][i] = q[j + 1][i];
+    }
+  }
+  finish_step(p.ctr, p.flags & K_ADV);
+}
+
+}  // namespace cwb

@@ -81,18 +81,6 @@ __device__ __forceinline__ void st4(T *dst, const T *v) {
   *reinterpret_cast<float4 *>(dst) = make_float4(v[0], v[1], v[2], v[3]);
 }
 
-// D+ of a node with the fused products of the pinned form (diffs_pinned's D+)
-template <typename T, int R, class Tap>
-__device__ __forceinline__ T dplus(const Tap &u, const T uc, const T *w) {
-  T d = u(1) - uc;
-  if (R > 1)
-    d = mul_rn(w[0], d);
-#pragma unroll
-  for (int k = 2; k <= R; ++k)
-    d = fma_rn(w[k - 1], u(k) - u(1 - k), d);
-  return d;
-}
-
 template <typename T, int R, bool UNIF>
 __global__ void __launch_bounds__(S3_THREADS, 2)
     step3d_kernel(const __grid_constant__ Step3Params<T> P) {

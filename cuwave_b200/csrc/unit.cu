@@ -5,6 +5,7 @@
 #include "step.cuh"
 #include "step_tma.cuh"
 #include "pml.cuh"
+#include "step2d.cuh"
 #include "step3d.cuh"
 
 #if !defined(CWB_REAL) || !defined(CWB_NDIM) || !defined(CWB_RADIUS)
@@ -106,6 +107,26 @@ int step3d_halo() {
 }
 #endif
 
+#if CWB_NDIM == 2
+template <typename T, int R>
+cudaError_t step2d_unit(const StepParams<T> &p, const bool uniform, const dim3 grid,
+                        cudaStream_t s) {
+  if constexpr (!Step2Shape<T, R>::SUPPORTED) {
+    return cudaErrorInvalidValue;
+  } else {
+    if (!uniform)
+      return cudaErrorInvalidValue;
+    step2d_kernel<T, R, true><<<grid, S2_THREADS, 0, s>>>(p);
+    return cudaGetLastError();
+  }
+}
+
+template <typename T, int R>
+bool step2d_built() {
+  return Step2Shape<T, R>::SUPPORTED;
+}
+#endif
+
 template <typename T, int NDIM, int R>
 cudaError_t pml_step_unit(const PmlStepParams<T> &p, const bool uniform, const dim3 grid,
                           cudaStream_t s) {
@@ -141,6 +162,11 @@ template cudaError_t step_unit<CWB_REAL, CWB_NDIM, CWB_RADIUS>(const StepParams<
 template cudaError_t step_tma_unit<CWB_REAL, CWB_NDIM, CWB_RADIUS>(
     const StepTmaParams<CWB_REAL> &, bool, dim3, cudaStream_t);
 template int step_tma_halo<CWB_REAL, CWB_NDIM, CWB_RADIUS>();
+#if CWB_NDIM == 2
+template cudaError_t step2d_unit<CWB_REAL, CWB_RADIUS>(const StepParams<CWB_REAL> &, bool, dim3,
+                                                       cudaStream_t);
+template bool step2d_built<CWB_REAL, CWB_RADIUS>();
+#endif
 #if CWB_NDIM == 3
 template cudaError_t step3d_unit<CWB_REAL, CWB_RADIUS>(const Step3Params<CWB_REAL> &, bool, dim3,
                                                        cudaStream_t);

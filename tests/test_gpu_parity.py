@@ -183,6 +183,22 @@ def test_blocked_uniform_step_matches_oracle(R, dirichlet, pml, damping):
     np.testing.assert_array_equal(traces, ref_traces)
 
 
+@pytest.mark.parametrize("R,dirichlet,pml,damping", [
+    (1, 0b0000, 0, False), (2, 0b0110, 0, False), (3, 0b1001, 3, False),
+    (4, 0b0110, 4, False), (4, 0b0000, 0, True), (4, 0b1111, 0, False), (2, 0b0101, 6, False),
+])
+def test_quad_2d_uniform_step_matches_oracle(R, dirichlet, pml, damping):
+    """The 2D quad step of a uniform stiffness on a grid of many row chunks and quads, an
+    axis-1 extent with padding, Dirichlet and Neumann faces, pml slabs, damping and
+    sources."""
+    case, meta = _random_case(2, R, dirichlet=dirichlet, pml=pml, uniform=True, damping=damping,
+                              seed=31 + R, nsrc=6, nsens=9, Nx=(187, 139))
+    field, traces = _product(case, meta)
+    ref_field, ref_traces = case.forward(meta["N"])
+    np.testing.assert_array_equal(field, ref_field)
+    np.testing.assert_array_equal(traces, ref_traces)
+
+
 @pytest.mark.parametrize("name", cases.GRADIENT)
 def test_reconstruction_matches_reference(name):
     """The strip-replay adjoint with two checkpoints against the reference's own run."""

@@ -81,14 +81,14 @@ def test_static_march_matches_plan_march(name):
 
 def test_static_march_refuses_lists_past_its_array():
     """A march whose source lists cannot fit the static array is refused, not truncated.
-    (A 2D march: its step folds the sources through per-block lists, which the 3D step of
-    a uniform stiffness does not build.)"""
+    (A radius-8 march: its step folds the sources through per-block lists, which the
+    register-blocked steps of radius 4 and below do not build.)"""
     from cuwave_b200 import _native as nat
     from cuwave_b200.wave import prepare_shot
 
     lib = nat.library()
     lib.cwb_march_static.restype = ctypes.c_int
-    fx = cases.load("fwd2d_r4")
+    fx = cases.load("fwd2d_r8")
     sim, design = cases.product_sim(fx)
     mat = sim.build_materials(design.copy())
     # 20000 sources on interior nodes: 320 kB of list entries, past the 256 kB array
