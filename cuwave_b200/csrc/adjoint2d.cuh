@@ -1,0 +1,401 @@
+// The 2D transposed step of a uniform stiffness, with or without the gradient densities:
+// quads of four fast-axis nodes marching rows, like step2d.cuh.
+//
+// MODE_STEP       lambda^n = 2 lambda^(n+1) - lambda^(n+2) + dt^2/m (W^-1 A^T W lambda^(n+1)),
+//                 the pml transpose gathered in (cuwave adjoint_kernel + pml_adjoint_kernel,
+//                 scalar_sensitivity.cu:388-441, 545-597);
+// MODE_STEP_GRAD  the same, accumulating g_mass and g_stiff against u^n
+//                 (adjoint_gradient_kernel, scalar_sensitivity.cu:444-515).
+//
+// A thread owns a quad and marches a chunk of rows, keeping lambda^(n+1) over rows
+// z-R .. z+R and u^n over rows z-R+1 .. z+R in register queues (the axis-0 taps) and
+// reading the quad's axis-1 runs of 4 + 2H values as 16-byte rows. The taps read through
+// the node image (a stored ghost is never read; lambda and u odd across a Dirichlet face)
+// and read zero on a held wall node, as cuwave's `reflected` does
+// (scalar_sensitivity.cu:177-184). Along axis 1 the quad shares its runs' first
+// differences and the plain D+ of u between neighbouring nodes: the same subtractions and
+// products of the same values the per-node form performs, so the sums are bit-identical;
+// a node on a held wall keeps the per-node form (its own value is not its taps' zero).
+// The arithmetic order is transposed_divergence_taps and stiffness_gradient_taps
+// (scalar_sensitivity.cu:119-154).
+#pragma once
+
+#include "adjoint.cuh"
+#include "step.cuh"
+
+namespace cwb {
+
+constexpr int A2_THREADS = 128;
+
+template <typename T, int R>
+struct Adj2Shape {
+  static constexpr int H = (R + 3) / 4 * 4;
+  static constexpr int XR = 4 + 2 * H;
+  static constexpr bool SUPPORTED = sizeof(T) == 4 && R <= 4;
+};
+
+// xr[c] = 0 at the run index c = e (a held wall node), e known at run time
+template <typename T, int XR>
+__device__ __forceinline__ void zero_at(T *xr, const int e) {
+#pragma unroll
+  for (int c = 0; c < XR; ++c)
+    if (c == e)
+      xr[c] = (T)0;
+}
+
+// A run of nodes xq - H .. xq + 3 + H along the fast axis read through the node image
+// (node b < 1 reads 2 - b, b > N - 2 reads 2(N - 2) - b, odd across a Dirichlet face),
+// zero on a held wall node
+template <typename T, int XR, int H>
+__device__ __forceinline__ void image_run(T *xr, const T *row, const int xq, const int N,
+                                          const int ext, const int odd) {
+#pragma unroll
+  for (int c = 0; c < XR / 4; ++c) {
+    const int x = xq - H + 4 * c;
+    if (x >= 0 && x + 3 <= ext - 1) {
+      load4(xr + 4 * c, row - H + 4 * c);
+    } else {
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+        xr[4 * c + i] = (T)0;
+    }
+  }
+  if (xq - H < 1 || xq + 3 + H > N - 2) {
+    // rebuild the positions past the walls from the stored interior ones
+    T raw[XR];
+#pragma unroll
+    for (int c = 0; c < XR; ++c)
+      raw[c] = xr[c];
+#pragma unroll
+    for (int c = 0; c < XR; ++c) {
+      const int b = xq - H + c;
+      if (b < 1 || b > N - 2) {
+        int sg;
+        const int m = node_image(b, N, odd, sg);
+        const int cm = m - (xq - H);
+        T v = (T)0;
+#pragma unroll
+        for (int s = 0; s < XR; ++s)
+          if (s == cm)
+            v = raw[s];
+        xr[c] = sg < 0 ? -v : v;
+      }
+    }
+  }
+  if (odd & 1)
+    zero_at<T, XR>(xr, 1 - (xq - H));
+  if (odd & 2)
+    zero_at<T, XR>(xr, N - 2 - (xq - H));
+}
+
+template <typename T, int R, int MODE>
+__global__ void __launch_bounds__(A2_THREADS, 4) adjoint2d_kernel(const AdjointParams<T> p) {
+  using S = Adj2Shape<T, R>;
+  static_assert(S::SUPPORTED && MODE != MODE_GRAD, "the 2D quad adjoint: float, radius <= 4");
+  constexpr bool GR = MODE == MODE_STEP_GRAD;
+  constexpr int H = S::H, XR = S::XR;
+  const Geometry &g = p.g;
+  const int t = step_index(p.ctr);
+  const int N0 = g.n[0], NF = g.n[1], ext = g.ext[1];
+  const int nq = (NF - 2) / 4 + 1;
+  const long long k = (long long)blockIdx.x * A2_THREADS + threadIdx.x;
+  const int quad = (int)(k % nq), cz = (int)(k / nq);
+  const int c0 = 1 + cz * p.chunk, c1 = min(N0 - 1, c0 + p.chunk);
+  const int xq = 4 * quad;
+  if (c0 < c1 && xq <= NF - 2) {
+    T *l0 = level<T>(p.l0, t);
+    const T *__restrict__ l1 = level<T>(p.l1, t);
+    const T *__restrict__ u1 = GR ? level<T>(p.u1, t) : nullptr;
+    const int dir0 = g.dir & 3, dirF = (g.dir >> 2) & 3;
+    const int s0 = g.s[0];
+    const int flags = p.flags;
+    const T gg = p.gconst, dg = p.dgconst;
+    int inner = 0, xheld = 0;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int x = xq + i;
+      if (x < 1 || x > NF - 2)
+        continue;
+      inner |= 1 << i;
+      if (held_wall(x, NF, dirF))
+        xheld |= 1 << i;
+    }
+    const T mi_derived = (flags & K_DERIVE) ? (T)1 / p.sconst : (T)0;
+    // whether a node of the quad is within R of an axis-1 pml slab (fixed for the thread)
+    const auto reach = [&](const int a, const int N, const int lo_d, const int hi_d) {
+      return (lo_d && a >= 1 && a <= lo_d + R) || (hi_d && a <= N - 2 && a >= N - 1 - (hi_d + R));
+    };
+    bool xreach = false;
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+      xreach |= ((inner >> i) & 1) && reach(xq + i, NF, g.lo[1], g.hi[1]);
+    // a field over the quad at row b through the node image along axis 0
+    const auto row4 = [&](const T *f, const int b, T *dst) {
+      int sg = 1;
+      const int m = (b >= 1 && b <= N0 - 2) ? b : node_image(b, N0, dir0, sg);
+      load4(dst, f + (long long)m * s0 + xq);
+      if (sg < 0) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+          dst[i] = -dst[i];
+      }
+    };
+    const auto held_row = [&](const int b) {
+      return ((dir0 & 1) && b == 1) || ((dir0 & 2) && b == N0 - 2);
+    };
+    // the queues hold taps: a held wall row reads zero there (its own centre is read
+    // again from memory when the march reaches it)
+    const auto tap4 = [&](const T *f, const int b, T *dst) {
+      row4(f, b, dst);
+      if (held_row(b)) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+          dst[i] = (T)0;
+      }
+    };
+    // queues: lambda rows z-R .. z+R, u rows z-R+1 .. z+R; the plain D+ of u at the row
+    // before (this row's D-), which reads u row c0 - R once
+    T ql[2 * R + 1][4], qu[2 * R][4], dmz[4];
+#pragma unroll
+    for (int j = 0; j < 2 * R; ++j)
+      tap4(l1, c0 - R + j, ql[j]);
+    if constexpr (GR) {
+      T first[4];
+      tap4(u1, c0 - R, first);
+#pragma unroll
+      for (int j = 0; j < 2 * R - 1; ++j)
+        tap4(u1, c0 - R + 1 + j, qu[j]);
+      const auto utap = [&](const int j, const int i) -> T {
+        return j == -R + 1 ? first[i] : qu[R - 2 + j][i];
+      };
+      // (u on a held wall row is zero, so its tap is its centre)
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const T uc = utap(0, i);
+        T d = p.w[0] * (utap(1, i) - uc);
+#pragma unroll
+        for (int kk = 2; kk <= R; ++kk)
+          d += p.w[kk - 1] * (utap(kk, i) - utap(1 - kk, i));
+        dmz[i] = d;
+      }
+    }
+    for (int z = c0; z < c1; ++z) {
+      tap4(l1, z + R, ql[2 * R]);
+      if constexpr (GR)
+        tap4(u1, z + R, qu[2 * R - 1]);
+      const long long row = (long long)z * s0 + xq;
+      const bool zheld = held_row(z);
+      const bool zreach = reach(z, N0, g.lo[0], g.hi[0]);
+      const auto ltap = [&](const int j, const int i) -> T { return ql[R + j][i]; };
+      const auto utap = [&](const int j, const int i) -> T { return qu[R - 1 + j][i]; };
+      // the row's own lambda and u: the queue's centre, or memory on a held wall row
+      T lcz[4], ucz[4];
+      if (!zheld) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          lcz[i] = ql[R][i];
+          ucz[i] = GR ? qu[R - 1][i] : (T)0;
+        }
+      } else {
+        row4(l1, z, lcz);
+        if constexpr (GR)
+          row4(u1, z, ucz);
+      }
+      // the axis-1 runs through the node image, zero on a held wall node
+      T lr[XR], ur[XR];
+      image_run<T, XR, H>(lr, l1 + row, xq, NF, ext, dirF);
+      if constexpr (GR)
+        image_run<T, XR, H>(ur, u1 + row, xq, NF, ext, dirF);
+      // shared along axis 1: g times the first differences of lambda, the plain D+ of u
+      T ge[XR];
+#pragma unroll
+      for (int c = H - R + 1; c <= H + 3 + R; ++c)
+        ge[c] = gg * (lr[c] - lr[c - 1]);
+      T dpx[5];
+      if constexpr (GR) {
+#pragma unroll
+        for (int j = 0; j < 5; ++j) {
+          const int c = H - 1 + j;
+          T d = p.w[0] * (ur[c + 1] - ur[c]);
+#pragma unroll
+          for (int kk = 2; kk <= R; ++kk)
+            d += p.w[kk - 1] * (ur[c + kk] - ur[c + 1 - kk]);
+          dpx[j] = d;
+        }
+      }
+      T ln[4], gm[4], gs4[4];
+      T lov[4], miv[4], uc[4], lc[4];
+      load4(lov, l0 + row);
+      if (flags & K_DERIVE) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+          miv[i] = mi_derived;
+      } else {
+        load4(miv, p.minv + row);
+      }
+      if constexpr (GR) {
+        load4(gm, p.g_mass + row);
+        load4(gs4, p.g_stiff + row);
+      }
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        lc[i] = lcz[i];
+        uc[i] = GR ? ucz[i] : (T)0;
+        const bool held = zheld || ((xheld >> i) & 1);
+        const T lw = held ? (T)0 : lc[i];
+        // axis 0: the per-node form
+        T div0 = (T)0;
+        {
+          T lh = lc[i], ll = lc[i];
+#pragma unroll
+          for (int j = 1; j <= R; ++j) {
+            const T lh1 = ltap(j, i), ll1 = ltap(-j, i);
+            div0 += p.w[j - 1] * (gg * (lh1 - lh) - gg * (ll - ll1));
+            lh = lh1;
+            ll = ll1;
+          }
+        }
+        // axis 1: shared differences, or the per-node form on a held wall node
+        const int c = H + i;
+        T div1 = (T)0;
+        if (!((xheld >> i) & 1)) {
+#pragma unroll
+          for (int j = 1; j <= R; ++j)
+            div1 += p.w[j - 1] * (ge[c + j] - ge[c - j + 1]);
+        } else {
+          T lh = lc[i], ll = lc[i];
+#pragma unroll
+          for (int j = 1; j <= R; ++j) {
+            const T lh1 = lr[c + j], ll1 = lr[c - j];
+            div1 += p.w[j - 1] * (gg * (lh1 - lh) - gg * (ll - ll1));
+            lh = lh1;
+            ll = ll1;
+          }
+        }
+        T div_l = (T)0;
+        div_l += p.f[0] * div0;
+        div_l += p.f[1] * div1;
+        T gsum = (T)0;
+        if constexpr (GR) {
+          // the stiffness densities (stiffness_gradient_taps), axis 0 then axis 1
+          T dpz = p.w[0] * (utap(1, i) - uc[i]);
+#pragma unroll
+          for (int kk = 2; kk <= R; ++kk)
+            dpz += p.w[kk - 1] * (utap(kk, i) - utap(1 - kk, i));
+          const T sd0 = p.f[0] * (dg * dpz * (ltap(1, i) - lw) + dg * dmz[i] * (lw - ltap(-1, i)));
+          dmz[i] = dpz;
+          const T sd1 = p.f[1] * (dg * dpx[i + 1] * (lr[c + 1] - lw) + dg * dpx[i] * (lw - lr[c - 1]));
+          gsum += sd0;
+          gsum += sd1;
+        }
+        const T lo = lov[i], mi = miv[i];
+        T v;
+        if (flags & K_DAMP) {
+          const T dmp = ((inner >> i) & 1) ? p.damping[row + i] : (T)0;
+          const T beta = (T)0.5 * mi * dmp * p.dt;
+          v = ((T)2 * lc[i] - lo * ((T)1 - beta) + mi * div_l) / ((T)1 + beta);
+        } else {
+          v = -lo + (T)2 * lc[i] + mi * div_l;
+        }
+        if (held)
+          v = (T)0;
+        ln[i] = v;
+        if constexpr (GR) {
+          gm[i] = gm[i] - p.mf * uc[i] * (v - (T)2 * lc[i] + lo);
+          gs4[i] = gs4[i] - p.mf * gsum;
+        }
+      }
+      if ((flags & K_PML) && (zreach || xreach)) {
+        // the pml transpose gathered from the memories' c+ and c- rows (pml_adjoint_kernel
+        // and pml_tap, scalar_sensitivity.cu:545-597, 237-251), node by node where a
+        // node is within R of a lined axis' slab
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          if (!((inner >> i) & 1))
+            continue;
+          const int A[2] = {z, xq + i};
+          T wcell = (T)1;
+#pragma unroll
+          for (int e = 0; e < 2; ++e)
+            if (A[e] == 1 || A[e] == g.n[e] - 2)
+              wcell *= (T)0.5;
+#pragma unroll 1
+          for (int d = 0; d < 2; ++d) {
+            const int lo_d = g.lo[d], hi_d = g.hi[d];
+            if (!(lo_d + hi_d))
+              continue;
+            const int a = A[d], N = g.n[d];
+            const bool reached = (lo_d && a >= 1 && a <= lo_d + R) ||
+                                 (hi_d && a <= N - 2 && a >= N - 1 - (hi_d + R));
+            if (!reached)
+              continue;
+            const T *mem = p.mem[d];
+            const long long sz = p.memrow[d];
+            const int rows = lo_d + hi_d;
+            const auto tap = [&](const int ai, const int q) -> T {
+              const int r = slab_row(ai, N, lo_d, hi_d);
+              const long long si = d == 0 ? (long long)r * ext + A[1] : (long long)A[0] * rows + r;
+              return mem[3 * sz + si] * plus_tap<T, R>(p.w, q) + mem[4 * sz + si] * minus_tap<T, R>(p.w, q);
+            };
+            T sum = (T)0;
+#pragma unroll 1
+            for (int m = -R; m <= R; ++m)
+              if (slab_row(a + m, N, lo_d, hi_d) >= 0)
+                sum += tap(a + m, -m);
+#pragma unroll 1
+            for (int high = 0; high < 2; ++high) {
+              // the reads past the wall that land on a, folded back, odd on a Dirichlet face
+              const int ghost = high ? 2 * (N - 2) - a : 2 - a;
+              if (high ? ghost < N - 1 : ghost > 0)
+                continue;
+              T fold = (T)0;
+#pragma unroll 1
+              for (int kk = 1; kk <= R; ++kk) {
+                const int ai = high ? N - 1 - kk : kk;
+                if (slab_row(ai, N, lo_d, hi_d) >= 0 && ghost - ai >= -R && ghost - ai <= R)
+                  fold += tap(ai, ghost - ai);
+              }
+              sum += ((g.dir >> (2 * d + high)) & 1) ? -fold : fold;
+            }
+            const T delta = miv[i] * sum / wcell;
+            ln[i] += delta;
+            if constexpr (GR)
+              gm[i] -= p.mf * uc[i] * delta;
+          }
+        }
+      }
+      if (inner == 15) {
+        store4(l0 + row, ln);
+        if constexpr (GR) {
+          store4(p.g_mass + row, gm);
+          store4(p.g_stiff + row, gs4);
+        }
+      } else {
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+          if ((inner >> i) & 1) {
+            l0[row + i] = ln[i];
+            if constexpr (GR) {
+              p.g_mass[row + i] = gm[i];
+              p.g_stiff[row + i] = gs4[i];
+            }
+          }
+      }
+#pragma unroll
+      for (int j = 0; j < 2 * R; ++j)
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+          ql[j][i] = ql[j + 1][i];
+      if constexpr (GR) {
+#pragma unroll
+        for (int j = 0; j < 2 * R - 1; ++j)
+#pragma unroll
+          for (int i = 0; i < 4; ++i)
+            qu[j][i] = qu[j + 1][i];
+      }
+    }
+  }
+  finish_step(p.ctr, p.flags & K_ADV);
+}
+
+}  // namespace cwb

@@ -14,6 +14,7 @@
 #include "cuwave_b200.h"
 #include "launch.cuh"
 #include "pml.cuh"
+#include "adjoint2d.cuh"
 #include "step2d.cuh"
 #include "step3d.cuh"
 #include "step_tma.cuh"
@@ -444,6 +445,22 @@ cudaError_t step2d_r(const cwb::StepParams<T> &p, const int R, const bool u, con
 }
 
 template <typename T>
+cudaError_t adjoint2d_r(const cwb::AdjointParams<T> &p, const int R, const int mode,
+                        const dim3 grid, cudaStream_t s) {
+  switch (R) {
+  case 1: return cwb::adjoint2d_unit<T, 1>(p, mode, grid, s);
+  case 2: return cwb::adjoint2d_unit<T, 2>(p, mode, grid, s);
+  case 3: return cwb::adjoint2d_unit<T, 3>(p, mode, grid, s);
+  case 4: return cwb::adjoint2d_unit<T, 4>(p, mode, grid, s);
+  case 5: return cwb::adjoint2d_unit<T, 5>(p, mode, grid, s);
+  case 6: return cwb::adjoint2d_unit<T, 6>(p, mode, grid, s);
+  case 7: return cwb::adjoint2d_unit<T, 7>(p, mode, grid, s);
+  case 8: return cwb::adjoint2d_unit<T, 8>(p, mode, grid, s);
+  }
+  return cudaErrorInvalidValue;
+}
+
+template <typename T>
 cudaError_t step3d_r(const cwb::Step3Params<T> &p, const int R, const bool u, const dim3 grid,
                      cudaStream_t s) {
   switch (R) {
@@ -795,6 +812,33 @@ int translate(cwb_plan *p, const cwb_op &op, const size_t slot, cudaStream_t str
     ap.g_stiff = static_cast<T *>(op.g_stiff);
     ap.flags = flags;
     ap.ctr = p->ctr;
+    // 2D, a uniform stiffness, float, radius <= 4: the quad adjoint (16-byte rows of the
+    // levels, 1/m and the accumulators)
+    const auto aligned16 = [](const void *ptr, const long long stride_elems) {
+      return reinterpret_cast<uintptr_t>(ptr) % 16 == 0 &&
+             (stride_elems * (long long)sizeof(T)) % 16 == 0;
+    };
+    if (ndim == 2 && mode != cwb::MODE_GRAD && p->blocked3 && uniform && step2d_built_r<T>(R) &&
+        aligned16(op.a.base, op.a.stride) && aligned16(op.b.base, op.b.stride) &&
+        (mode != cwb::MODE_STEP_GRAD ||
+         (aligned16(op.c.base, op.c.stride) && aligned16(op.g_mass, 0) && aligned16(op.g_stiff, 0))) &&
+        ((flags & cwb::K_DERIVE) || aligned16(ap.minv, 0)) && g.n[0] >= 3 * R && g.n[1] >= 3 * R) {
+      // short chunks: the adjoint's rows are long dependent chains, so many threads of
+      // two rows each keep more of them in flight than long marches (measured on 2048^2)
+      const long long rows = g.n[0] - 2, quads = (g.n[1] - 2) / 4 + 1;
+      const long long want = (long long)p->sms * 4096;
+      const int chunk = (int)std::max<long long>(1, std::min<long long>(rows, rows * quads / want));
+      ap.chunk = p->chunk_override > 0 ? p->chunk_override : std::max(2, chunk);
+      const long long threads = quads * ((rows + ap.chunk - 1) / ap.chunk);
+      const dim3 grid((unsigned)((threads + cwb::A2_THREADS - 1) / cwb::A2_THREADS));
+      out.push_back([ap, R, mode, grid](cudaStream_t s, bool adv) {
+        cwb::AdjointParams<T> q = ap;
+        if (adv)
+          q.flags |= cwb::K_ADV;
+        return adjoint2d_r<T>(q, R, mode, grid, s);
+      });
+      return CWB_OK;
+    }
     dim3 grid;
     stencil_grid(p, grid, ap.chunk);
     out.push_back([ap, ndim, R, uniform, mode, grid](cudaStream_t s, bool adv) {

@@ -45,6 +45,11 @@ cudaError_t step2d_unit(const StepParams<T> &p, bool uniform, dim3 grid, cudaStr
 template <typename T, int R>
 bool step2d_built();
 
+// the 2D quad adjoint of a uniform stiffness (float, radius <= 4), MODE_STEP or
+// MODE_STEP_GRAD, 128 threads a block
+template <typename T, int R>
+cudaError_t adjoint2d_unit(const AdjointParams<T> &p, int mode, dim3 grid, cudaStream_t stream);
+
 template <typename T>
 struct PmlStepParams;
 

@@ -5,6 +5,7 @@
 #include "step.cuh"
 #include "step_tma.cuh"
 #include "pml.cuh"
+#include "adjoint2d.cuh"
 #include "step2d.cuh"
 #include "step3d.cuh"
 
@@ -125,6 +126,22 @@ template <typename T, int R>
 bool step2d_built() {
   return Step2Shape<T, R>::SUPPORTED;
 }
+
+template <typename T, int R>
+cudaError_t adjoint2d_unit(const AdjointParams<T> &p, const int mode, const dim3 grid,
+                           cudaStream_t s) {
+  if constexpr (!Adj2Shape<T, R>::SUPPORTED) {
+    return cudaErrorInvalidValue;
+  } else {
+    if (mode == MODE_STEP_GRAD)
+      adjoint2d_kernel<T, R, MODE_STEP_GRAD><<<grid, A2_THREADS, 0, s>>>(p);
+    else if (mode == MODE_STEP)
+      adjoint2d_kernel<T, R, MODE_STEP><<<grid, A2_THREADS, 0, s>>>(p);
+    else
+      return cudaErrorInvalidValue;
+    return cudaGetLastError();
+  }
+}
 #endif
 
 template <typename T, int NDIM, int R>
@@ -166,6 +183,8 @@ template int step_tma_halo<CWB_REAL, CWB_NDIM, CWB_RADIUS>();
 template cudaError_t step2d_unit<CWB_REAL, CWB_RADIUS>(const StepParams<CWB_REAL> &, bool, dim3,
                                                        cudaStream_t);
 template bool step2d_built<CWB_REAL, CWB_RADIUS>();
+template cudaError_t adjoint2d_unit<CWB_REAL, CWB_RADIUS>(const AdjointParams<CWB_REAL> &, int,
+                                                          dim3, cudaStream_t);
 #endif
 #if CWB_NDIM == 3
 template cudaError_t step3d_unit<CWB_REAL, CWB_RADIUS>(const Step3Params<CWB_REAL> &, bool, dim3,
