@@ -66,6 +66,26 @@ __device__ __forceinline__ void finish_step(int *ctr, const bool advance) {
   }
 }
 
+// a += v as one IEEE addition, atomically: a compare-and-swap loop, since the hardware's
+// float atomic add flushes subnormal results to zero and the reference's host adds do not
+__device__ __forceinline__ void atomic_add_exact(float *a, const float v) {
+  unsigned *w = reinterpret_cast<unsigned *>(a);
+  unsigned old = *reinterpret_cast<volatile unsigned *>(w), seen;
+  do {
+    seen = old;
+    old = atomicCAS(w, seen, __float_as_uint(__uint_as_float(seen) + v));
+  } while (old != seen);
+}
+__device__ __forceinline__ void atomic_add_exact(double *a, const double v) {
+  unsigned long long *w = reinterpret_cast<unsigned long long *>(a);
+  unsigned long long old = *reinterpret_cast<volatile unsigned long long *>(w), seen;
+  do {
+    seen = old;
+    old = atomicCAS(w, seen,
+                    (unsigned long long)__double_as_longlong(__longlong_as_double((long long)seen) + v));
+  } while (old != seen);
+}
+
 // products and fused products the compiler keeps as written
 __device__ __forceinline__ float mul_rn(const float a, const float b) { return __fmul_rn(a, b); }
 __device__ __forceinline__ double mul_rn(const double a, const double b) { return __dmul_rn(a, b); }

@@ -45,7 +45,7 @@ __global__ void excite_kernel(const TransferParams<T> p) {
   if (j < p.num) {
     T *a = level<T>(p.a, t);
     const long long row = (long long)p.row_mul * t + p.row_add;
-    atomicAdd(&a[p.lin[j]], p.weight[j] * record_read(p, row * p.num + j));
+    atomic_add_exact(&a[p.lin[j]], p.weight[j] * record_read(p, row * p.num + j));
   }
   finish_step(p.ctr, p.flags & K_ADV);
 }
@@ -61,10 +61,10 @@ __global__ void load_kernel(const TransferParams<T> p, T *g_mass) {
     const long long row = (long long)p.row_mul * t + p.row_add;
     const int n = p.lin[j];
     const T load = p.weight[j] * record_read(p, row * p.num + j);
-    atomicAdd(&a[n], load);
+    atomic_add_exact(&a[n], load);
     if (p.flags & K_MASS) {
       const T *u1 = level<T>(p.c, t);
-      atomicAdd(&g_mass[n], -p.scale * u1[n] * load);
+      atomic_add_exact(&g_mass[n], -p.scale * u1[n] * load);
     }
   }
   finish_step(p.ctr, p.flags & K_ADV);
