@@ -103,7 +103,7 @@ __global__ void __launch_bounds__(S3_THREADS, 2)
   const int lev1 = level_index(P.level_u1, t), lev0 = level_index(P.level_u0, t);
 
   const int tid = threadIdx.x;
-  const int tq = tid & 15, ty = tid >> 4;  // the thread's quad along axis 2, its row
+  const int tq = tid % (BX / 4), ty = tid / (BX / 4);  // the thread's quad along axis 2, its row
   const int x0 = blockIdx.x * BX, y0 = blockIdx.y * BY;
   const int xq = x0 + 4 * tq, py = y0 + ty;
   const int N0 = g.n[0], NM = g.n[1], NF = g.n[2];
