@@ -62,10 +62,11 @@ def flat(fx, position) -> np.ndarray:
     return lin.astype(np.int32)
 
 
-def oracle_case(fx):
+def oracle_case(fx, dtype=None):
+    """The oracle Case of a fixture, in its own precision or in `dtype`."""
     from oracle import oracle as o
 
-    dt_ = dtype_of(fx)
+    dt_ = dtype_of(fx) if dtype is None else dtype
     Nx = tuple(int(n) for n in fx["Nx"])
     ndim = len(Nx)
     order, dt = int(fx["order"]), float(fx["dt"])
