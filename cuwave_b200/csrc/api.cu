@@ -580,6 +580,34 @@ void pml_launch(const cwb_plan *p, const cwb::StepParams<T> &sp, const bool unif
   });
 }
 
+// The step op's common parameters: geometry, stencil row, factors, materials, pml memory.
+template <typename T>
+int step_setup(const cwb_plan *p, const cwb_op &op, cwb::StepParams<T> &sp, int &flags,
+               bool &uniform) {
+  int rc;
+  if ((rc = check_level(op.a, "a")) || (rc = check_level(op.b, "b")) ||
+      (rc = check_level(op.c, "c")))
+    return rc;
+  sp.g = p->geo;
+  fill_weights(p, sp.w, sp.f);
+  sp.dt = (T)p->grid.dt;
+  T dgconst;
+  flags = 0;
+  if ((rc = fill_material<T>(p, op.mat, &sp.stiff, &sp.minv, &sp.damping, sp.prof, sp.sconst,
+                             sp.gconst, dgconst, flags, uniform, op.flags & CWB_PML)))
+    return rc;
+  if (op.flags & CWB_PML) {
+    flags |= cwb::K_PML;
+    for (int d = 0; d < p->geo.ndim; ++d) {
+      sp.aux[d] = static_cast<T *>(op.memory[d]);
+      sp.auxrow[d] = (int)p->pml_row[d];
+      if (lined(p, d) && !sp.aux[d])
+        return fail(CWB_ERR_ARG, "a lined axis needs its pml memory");
+    }
+  }
+  return CWB_OK;
+}
+
 // the launches of one op, each taking (stream, advance)
 template <typename T>
 int translate(cwb_plan *p, const cwb_op &op, const size_t slot, cudaStream_t stream,
@@ -590,30 +618,13 @@ int translate(cwb_plan *p, const cwb_op &op, const size_t slot, cudaStream_t str
   int rc;
   switch (op.kind) {
   case CWB_OP_STEP: {
-    if ((rc = check_level(op.a, "a")) || (rc = check_level(op.b, "b")) ||
-        (rc = check_level(op.c, "c")))
-      return rc;
     cwb::StepTmaParams<T> tp;
     std::memset(&tp, 0, sizeof tp);
     cwb::StepParams<T> &sp = tp.s;
-    sp.g = g;
-    fill_weights(p, sp.w, sp.f);
-    sp.dt = (T)p->grid.dt;
     bool uniform;
     int flags = 0;
-    T dgconst;
-    if ((rc = fill_material<T>(p, op.mat, &sp.stiff, &sp.minv, &sp.damping, sp.prof, sp.sconst,
-                               sp.gconst, dgconst, flags, uniform, op.flags & CWB_PML)))
+    if ((rc = step_setup<T>(p, op, sp, flags, uniform)))
       return rc;
-    if (op.flags & CWB_PML) {
-      flags |= cwb::K_PML;
-      for (int d = 0; d < ndim; ++d) {
-        sp.aux[d] = static_cast<T *>(op.memory[d]);
-        sp.auxrow[d] = (int)p->pml_row[d];
-        if (lined(p, d) && !sp.aux[d])
-          return fail(CWB_ERR_ARG, "a lined axis needs its pml memory");
-      }
-    }
     // 3D, a uniform stiffness: the blocked kernel. It stores rows of four and keeps the
     // taps it mirrors in its own run, so it wants an output level on 16-byte boundaries
     // and axes of at least 3R nodes. Elsewhere the TMA row kernel, else the plain one.
@@ -968,8 +979,121 @@ int enqueue_step(const std::vector<Launch> &launches, cudaStream_t s) {
 }
 
 template <typename T>
+cudaError_t march2d_r(const cwb::March2Params<T> &mp, const int R, const int sms, cudaStream_t s) {
+  switch (R) {
+  case 1: return cwb::march2d_unit<T, 1>(mp, sms, s);
+  case 2: return cwb::march2d_unit<T, 2>(mp, sms, s);
+  case 3: return cwb::march2d_unit<T, 3>(mp, sms, s);
+  case 4: return cwb::march2d_unit<T, 4>(mp, sms, s);
+  case 5: return cwb::march2d_unit<T, 5>(mp, sms, s);
+  case 6: return cwb::march2d_unit<T, 6>(mp, sms, s);
+  case 7: return cwb::march2d_unit<T, 7>(mp, sms, s);
+  case 8: return cwb::march2d_unit<T, 8>(mp, sms, s);
+  }
+  return cudaErrorInvalidValue;
+}
+
+// A 2D op list [step, records] of a uniform stiffness (float, radius <= 4) runs as one
+// cooperative launch of all its steps, sources and refill folded into the step and a
+// grid-wide barrier before the records (march2d_kernel). Returns false where the list is
+// another shape, leaving it to the per-step march.
+template <typename T>
+bool march2d_path(cwb_plan *p, const cwb_op *ops, const int nops, const int t0, const int steps,
+                  cudaStream_t user, int &rc) {
+  const Geometry &g = p->geo;
+  const int R = p->grid.radius;
+  if (!p->blocked3 || g.ndim != 2 || steps < 16 || nops < 1 || nops > 1 + cwb::MARCH2_RECORDS ||
+      ops[0].kind != CWB_OP_STEP || !step2d_built_r<T>(R) || g.n[0] < 3 * R || g.n[1] < 3 * R)
+    return false;
+  for (int i = 1; i < nops; ++i)
+    if (ops[i].kind != CWB_OP_RECORD || ops[i].points.num <= 0 || !ops[i].points.lin ||
+        !ops[i].points.record || ops[i].points.store < 0 || ops[i].points.store > 2 ||
+        (ops[i].points.store == 2 && sizeof(T) == 4) || check_level(ops[i].a, "a"))
+      return false;
+  const cwb_op &op = ops[0];
+  const cwb_points &src = op.points;
+  if ((op.flags & CWB_FOLD_SOURCES) && src.num > 0 &&
+      (src.num > 32 || !src.lin || !src.weight || !src.record))
+    return false;
+  cwb::March2Params<T> mp;
+  std::memset(&mp, 0, sizeof mp);
+  cwb::StepParams<T> &sp = mp.s;
+  int flags = 0;
+  bool uniform = false;
+  if (step_setup<T>(p, op, sp, flags, uniform) || !uniform)
+    return false;
+  const auto aligned16 = [](const void *ptr, const long long stride_elems) {
+    return reinterpret_cast<uintptr_t>(ptr) % 16 == 0 && (stride_elems * (long long)sizeof(T)) % 16 == 0;
+  };
+  if (!aligned16(op.a.base, op.a.stride) || !aligned16(op.b.base, op.b.stride) ||
+      !aligned16(op.c.base, op.c.stride) || (!(flags & cwb::K_DERIVE) && !aligned16(sp.minv, 0)))
+    return false;
+  const int bytes = sizeof(T);
+  const long long rows = g.n[0] - 2, quads = (g.n[1] - 2) / 4 + 1;
+  // a grid whose rows the co-resident threads cover about once: larger ones keep more
+  // rows in flight launched step by step (measured: 512^2 10.8 us a step here against
+  // 16 us launched; 2048^2 69 us against 52 us)
+  if (rows * quads > (long long)p->sms * 1024)
+    return false;
+  const long long want = (long long)p->sms * 1024;
+  sp.chunk = (int)std::max<long long>(1, std::min<long long>(rows, rows * quads / want));
+  if (p->chunk_override > 0)
+    sp.chunk = p->chunk_override;
+  sp.flags = flags;
+  sp.u0 = to_level(op.a, bytes);
+  sp.u1 = to_level(op.b, bytes);
+  sp.u2 = to_level(op.c, bytes);
+  sp.ctr = p->ctr;
+  mp.units = quads * ((rows + sp.chunk - 1) / sp.chunk);
+  if ((op.flags & CWB_FOLD_SOURCES) && src.num > 0) {
+    mp.fold.lin = src.lin;
+    mp.fold.weight = static_cast<const T *>(src.weight);
+    mp.fold.signal = static_cast<const T *>(src.record);
+    mp.fold.nsrc = src.num;
+    mp.fold.sig_mul = src.row_mul;
+    mp.fold.sig_add = src.row_add;
+  }
+  if (op.flags & CWB_FOLD_REFILL)
+    mp.fold.refill = p->grid.neumann | p->grid.dirichlet;
+  mp.nrec = nops - 1;
+  for (int i = 1; i < nops; ++i) {
+    cwb::TransferParams<T> &tp = mp.rec[i - 1];
+    tp.g = g;
+    tp.a = to_level(ops[i].a, bytes);
+    tp.lin = ops[i].points.lin;
+    tp.record = ops[i].points.record;
+    tp.num = ops[i].points.num;
+    tp.row_mul = ops[i].points.row_mul;
+    tp.row_add = ops[i].points.row_add;
+    tp.store = ops[i].points.store;
+    tp.ctr = p->ctr;
+  }
+  mp.t0 = t0;
+  mp.steps = steps;
+  rc = CWB_OK;
+  const auto run = [&]() -> int {
+    CWB_CUDA(cudaEventRecord(p->fork, user));
+    CWB_CUDA(cudaStreamWaitEvent(p->lane, p->fork, 0));
+    cudaStream_t s = p->lane;
+    CWB_CUDA(cwb::launch_set_counter(p->ctr, t0, s));
+    CWB_CUDA(march2d_r<T>(mp, R, p->sms, s));
+    g_launches += 2;
+    CWB_CUDA(cudaEventRecord(p->join, s));
+    CWB_CUDA(cudaStreamWaitEvent(user, p->join, 0));
+    return CWB_OK;
+  };
+  rc = run();
+  return true;
+}
+
+template <typename T>
 int march(cwb_plan *p, const cwb_op *ops, const int nops, const int t0, const int steps,
           const int graph, cudaStream_t user) {
+  {
+    int rc = CWB_OK;
+    if (march2d_path<T>(p, ops, nops, t0, steps, user, rc))
+      return rc;
+  }
   std::vector<Launch> launches;
   for (int i = 0; i < nops; ++i) {
     const int rc = translate<T>(p, ops[i], (size_t)i, user, launches);

@@ -51,6 +51,12 @@ template <typename T, int R>
 cudaError_t adjoint2d_unit(const AdjointParams<T> &p, int mode, dim3 grid, cudaStream_t stream);
 
 template <typename T>
+struct March2Params;
+// the multi-step 2D march, one cooperative launch of as many blocks as fit on `sms` SMs
+template <typename T, int R>
+cudaError_t march2d_unit(const March2Params<T> &p, int sms, cudaStream_t stream);
+
+template <typename T>
 struct PmlStepParams;
 
 // the pml memory update of a step over the slab nodes (after the blocked step)

@@ -18,7 +18,10 @@
 // axis 1 in the run's registers, along axis 0 by reading the mirror row.
 #pragma once
 
+#include <cooperative_groups.h>
+
 #include "step.cuh"
+#include "transfer.cuh"
 
 namespace cwb {
 
@@ -32,16 +35,27 @@ struct Step2Shape {
   static constexpr bool SUPPORTED = sizeof(T) == 4 && R <= 4;
 };
 
-template <typename T, int R, bool UNIF>
-__global__ void __launch_bounds__(S2_THREADS, 4) step2d_kernel(const StepParams<T> p) {
+// The sources and the ghost refill a multi-step march folds into the step: the sources
+// added node by node after the pml (cuwave excitation_kernel, common.cuh:456-464), the
+// ghosts written from their mirror rows (cuwave scalar.cu:535-555). None in a plain step.
+template <typename T>
+struct Fold2 {
+  const int *lin;       // flat source nodes
+  const T *weight;      // their weights
+  const T *signal;      // (rows, nsrc)
+  int nsrc, sig_mul, sig_add;
+  int refill;           // faces whose ghosts are written
+};
+
+// unit k (a quad and a chunk of rows) of the step at t
+template <typename T, int R>
+__device__ __forceinline__ void step2d_rows(const StepParams<T> &p, const int t, const long long k,
+                                            const Fold2<T> &fold) {
   using S = Step2Shape<T, R>;
-  static_assert(S::SUPPORTED && UNIF, "the 2D quad step is built for float, radius <= 4, a uniform stiffness");
   constexpr int H = S::H, XR = S::XR;
   const Geometry &g = p.g;
-  const int t = step_index(p.ctr);
   const int N0 = g.n[0], NF = g.n[1], ext = g.ext[1];
   const int nq = (NF - 2) / 4 + 1;  // quads covering nodes 0 .. NF - 2
-  const long long k = (long long)blockIdx.x * S2_THREADS + threadIdx.x;
   const int quad = (int)(k % nq);
   const int cz = (int)(k / nq);
   const int c0 = 1 + cz * p.chunk;
@@ -230,6 +244,20 @@ __global__ void __launch_bounds__(S2_THREADS, 4) step2d_kernel(const StepParams<
           }
         }
       }
+      if (fold.nsrc) {
+        // the sources of this quad, in the list's order
+        const long long srow = (long long)fold.sig_mul * t + fold.sig_add;
+        for (int e = 0; e < fold.nsrc; ++e) {
+          const long long n = fold.lin[e] - row;
+          if (n >= 0 && n < 4) {
+            const T add = fold.weight[e] * fold.signal[srow * fold.nsrc + e];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+              if (n == i)
+                v[i] += add;
+          }
+        }
+      }
       if (inner == 15) {
         store4(u2 + row, v);
       } else {
@@ -238,6 +266,23 @@ __global__ void __launch_bounds__(S2_THREADS, 4) step2d_kernel(const StepParams<
           if ((inner >> i) & 1)
             u2[row + i] = v[i];
       }
+      if (fold.refill) {
+        const int fr = fold.refill;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          if (!((inner >> i) & 1))
+            continue;
+          const int x = xq + i;
+          if ((fr & 1) && z == 2)
+            u2[row + i - 2LL * s0] = (dir0 & 1) ? -v[i] : v[i];
+          if ((fr & 2) && z == N0 - 3)
+            u2[row + i + 2LL * s0] = (dir0 & 2) ? -v[i] : v[i];
+          if ((fr & 4) && x == 2)
+            u2[row + i - 2] = (dirF & 1) ? -v[i] : v[i];
+          if ((fr & 8) && x == NF - 3)
+            u2[row + i + 2] = (dirF & 2) ? -v[i] : v[i];
+        }
+      }
 #pragma unroll
       for (int j = 0; j < 2 * R - 1; ++j)
 #pragma unroll
@@ -245,7 +290,59 @@ __global__ void __launch_bounds__(S2_THREADS, 4) step2d_kernel(const StepParams<
           q[j][i] = q[j + 1][i];
     }
   }
+}
+
+template <typename T, int R, bool UNIF>
+__global__ void __launch_bounds__(S2_THREADS, 4) step2d_kernel(const StepParams<T> p) {
+  static_assert(Step2Shape<T, R>::SUPPORTED && UNIF,
+                "the 2D quad step is built for float, radius <= 4, a uniform stiffness");
+  const Fold2<T> none{};
+  step2d_rows<T, R>(p, step_index(p.ctr), (long long)blockIdx.x * S2_THREADS + threadIdx.x, none);
   finish_step(p.ctr, p.flags & K_ADV);
+}
+
+// The multi-step march of an L2-resident 2D grid: one cooperative launch runs `steps`
+// steps of [step (sources and refill folded), records] with a grid-wide barrier between a
+// step and its records, where the plain march launches four kernels a step. It stands in
+// for cuwave's blocked_kernel (several steps per launch, excitation, refill and record
+// folded in; scalar.cu:571-791) on a grid whose fields stay in L2 between steps.
+constexpr int MARCH2_RECORDS = 4;
+
+template <typename T>
+struct March2Params {
+  StepParams<T> s;
+  Fold2<T> fold;
+  TransferParams<T> rec[MARCH2_RECORDS];  // store, level and rows of each record
+  int nrec;
+  int t0, steps;
+  long long units;  // quads x row chunks
+};
+
+template <typename T, int R>
+__global__ void __launch_bounds__(S2_THREADS, 4) march2d_kernel(const __grid_constant__ March2Params<T> mp) {
+  static_assert(Step2Shape<T, R>::SUPPORTED, "the 2D quad step is built for float, radius <= 4");
+  namespace cg = cooperative_groups;
+  cg::grid_group grid = cg::this_grid();
+  const long long gtid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long gsize = (long long)gridDim.x * blockDim.x;
+  for (int s = 0; s < mp.steps; ++s) {
+    const int t = mp.t0 + s;
+    for (long long k = gtid; k < mp.units; k += gsize)
+      step2d_rows<T, R>(mp.s, t, k, mp.fold);
+    grid.sync();  // the step's nodes and ghosts are all written
+    for (int r = 0; r < mp.nrec; ++r) {
+      const TransferParams<T> &rp = mp.rec[r];
+      const T *a = level<T>(rp.a, t);
+      const long long row = (long long)rp.row_mul * t + rp.row_add;
+      for (long long j = gtid; j < rp.num; j += gsize)
+        record_write(rp, row * rp.num + j, a[rp.lin[j]]);
+    }
+    // the next step writes the level two back and reads this one: no barrier needed
+  }
+  if (gtid == 0) {
+    mp.s.ctr[1] = 0;
+    mp.s.ctr[0] = mp.t0 + mp.steps;
+  }
 }
 
 }  // namespace cwb

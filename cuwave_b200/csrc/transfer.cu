@@ -30,6 +30,11 @@ cudaError_t launch_pml_aux(const PmlAuxParams<T> &p, cudaStream_t stream) {
   return cudaGetLastError();
 }
 
+__global__ void set_counter_kernel(int *ctr, const int t0) {
+  ctr[0] = t0;
+  ctr[1] = 0;
+}
+
 cudaError_t launch_set_counter(int *ctr, const int t0, cudaStream_t stream) {
   set_counter_kernel<<<1, 1, 0, stream>>>(ctr, t0);
   return cudaGetLastError();

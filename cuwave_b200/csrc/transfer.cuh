@@ -204,9 +204,4 @@ __global__ void pml_aux_kernel(const PmlAuxParams<T> p) {
   finish_step(p.ctr, p.flags & K_ADV);
 }
 
-__global__ void set_counter_kernel(int *ctr, const int t0) {
-  ctr[0] = t0;
-  ctr[1] = 0;
-}
-
 }  // namespace cwb

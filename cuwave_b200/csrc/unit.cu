@@ -1,5 +1,7 @@
 // One (precision, dimension, radius) of the step and adjoint kernels, selected by
 // CWB_REAL, CWB_NDIM and CWB_RADIUS at compile time.
+#include <algorithm>
+
 #include "adjoint.cuh"
 #include "launch.cuh"
 #include "step.cuh"
@@ -128,6 +130,27 @@ bool step2d_built() {
 }
 
 template <typename T, int R>
+cudaError_t march2d_unit(const March2Params<T> &mp, const int sms, cudaStream_t s) {
+  if constexpr (!Step2Shape<T, R>::SUPPORTED) {
+    return cudaErrorInvalidValue;
+  } else {
+    const auto k = march2d_kernel<T, R>;
+    int per = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, S2_THREADS, 0);
+    if (e != cudaSuccess)
+      return e;
+    if (per < 1)
+      return cudaErrorInvalidConfiguration;
+    const long long want = (mp.units + S2_THREADS - 1) / S2_THREADS;
+    const unsigned blocks = (unsigned)std::min<long long>(want, (long long)per * sms);
+    void *args[] = {const_cast<March2Params<T> *>(&mp)};
+    e = cudaLaunchCooperativeKernel(reinterpret_cast<const void *>(k), dim3(blocks),
+                                    dim3(S2_THREADS), args, 0, s);
+    return e;
+  }
+}
+
+template <typename T, int R>
 cudaError_t adjoint2d_unit(const AdjointParams<T> &p, const int mode, const dim3 grid,
                            cudaStream_t s) {
   if constexpr (!Adj2Shape<T, R>::SUPPORTED) {
@@ -183,6 +206,8 @@ template int step_tma_halo<CWB_REAL, CWB_NDIM, CWB_RADIUS>();
 template cudaError_t step2d_unit<CWB_REAL, CWB_RADIUS>(const StepParams<CWB_REAL> &, bool, dim3,
                                                        cudaStream_t);
 template bool step2d_built<CWB_REAL, CWB_RADIUS>();
+template cudaError_t march2d_unit<CWB_REAL, CWB_RADIUS>(const March2Params<CWB_REAL> &, int,
+                                                         cudaStream_t);
 template cudaError_t adjoint2d_unit<CWB_REAL, CWB_RADIUS>(const AdjointParams<CWB_REAL> &, int,
                                                           dim3, cudaStream_t);
 #endif
