@@ -199,6 +199,19 @@ def test_quad_2d_uniform_step_matches_oracle(R, dirichlet, pml, damping):
     np.testing.assert_array_equal(traces, ref_traces)
 
 
+def test_quad_2d_step_by_step_on_a_large_grid():
+    """A 2D grid past the multi-step march's size runs the quad step launch by launch
+    (sources and refill as their own launches): still equal to the oracle's."""
+    case, meta = _random_case(2, 4, dirichlet=0b0110, pml=5, uniform=True, seed=77, nsrc=3,
+                              nsens=9, Nx=(603, 1101))
+    meta["N"] = 20
+    case.signal = case.signal[:20]
+    field, traces = _product(case, meta)
+    ref_field, ref_traces = case.forward(meta["N"])
+    np.testing.assert_array_equal(field, ref_field)
+    np.testing.assert_array_equal(traces, ref_traces)
+
+
 @pytest.mark.parametrize("ndim,R,dirichlet,pml,damping,Nx", [
     (2, 1, 0b0000, 0, False, (67, 91)), (2, 2, 0b0110, 0, False, (81, 73)),
     (2, 3, 0b1001, 4, False, (67, 91)), (2, 4, 0b0110, 5, False, (75, 139)),
