@@ -163,7 +163,9 @@ def sensitivity(sim: Simulation, source: Source, indicator, sensors, objective: 
     plan.march(ops, 0, N)
     del memory
     sensor_lin = flatten_indices(sim, sensors)
-    um = V[2:].reshape(N, -1)[:, sensor_lin.long()]
+    # column-major, as numpy lays out the reference's V[2:][:, lin]: a sum over a
+    # reshaped record then adds in the same order
+    um = V[2:].reshape(N, -1).t().index_select(0, sensor_lin.long()).t()
     cost, dphi = _objective(objective, um)
 
     # --------------------------------------------------------------- backward pass

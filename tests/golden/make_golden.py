@@ -183,6 +183,91 @@ def run_gradients(case):
     return out
 
 
+def run_glue(case, shot_coords, receiver_coords):
+    """The shot glue of cuwave utils.py on off-node shots and receivers."""
+    from cuwave.sensitivity import l2_misfit, reconstruction_sensitivity, source_sensitivity
+    from cuwave.utils import (
+        Sensors, collect_source, energy, measure, misfit, misfit_gradient, point_source,
+        response_gradient, shots, stack,
+    )
+
+    sim = make_sim(case)
+    signal = case["signal"][:, 0]
+    sources = shots(sim, shot_coords, signal)
+    sensors = Sensors(sim, receiver_coords)
+    perturbed = design(case, sim).copy()
+    perturbed *= 0.95
+    observed = [np.asarray(o) for o in measure(sim, sources, perturbed, sensors)]
+    cost = misfit(sim, sources, design(case, sim).copy(), sensors, observed)
+    gcost, gradient = misfit_gradient(sim, sources, design(case, sim).copy(), sensors, observed)
+    rcost, rgradient = misfit_gradient(
+        sim, sources, design(case, sim).copy(), sensors, observed,
+        adjoint=reconstruction_sensitivity,
+    )
+    stacked = stack(sources)
+    stacked_traces = measure(sim, [stacked], design(case, sim).copy(), sensors)[0]
+    ecost, egradient = response_gradient(
+        sim, stacked, design(case, sim).copy(), sensors.nodes, sensors.objective(energy(sim))
+    )
+    one = point_source(sim, shot_coords[:1], signal)
+    scost, scolumns, _, _ = source_sensitivity(
+        sim, one, design(case, sim).copy(), sensors.nodes,
+        sensors.objective(l2_misfit(observed[0])),
+    )
+    out = dict(case)
+    out.update(
+        shot_coords=np.asarray(shot_coords, dtype=float),
+        receiver_coords=np.asarray(receiver_coords, dtype=float),
+        sensor_nodes=np.asarray(sensors.nodes), sensor_weights=np.asarray(sensors.weights),
+        observed=np.stack(observed), misfit=np.array(cost), gradient_cost=np.array(gcost),
+        gradient=np.asarray(gradient), rec_cost=np.array(rcost),
+        rec_gradient=np.asarray(rgradient), stacked_position=np.asarray(stacked.position),
+        stacked_signal=np.asarray(stacked.signal), stacked_traces=np.asarray(stacked_traces),
+        energy_cost=np.array(ecost), energy_gradient=np.asarray(egradient),
+        source_cost=np.array(scost), source_columns=np.asarray(scolumns),
+        source_signal_gradient=np.asarray(collect_source(sim, shot_coords[:1], scolumns)),
+    )
+    for k, s in enumerate(sources):
+        out[f"shot{k}_position"] = np.asarray(s.position)
+        out[f"shot{k}_signal"] = np.asarray(s.signal)
+    return out
+
+
+def run_distribute(name, Nx, dx, precision, seed):
+    """`distribute`, `point_source` and `collect_source` alone on a grid of uneven spacing."""
+    from cuwave.scalar import AcousticWave
+    from cuwave.utils import collect_source, distribute, point_source
+
+    rng = np.random.default_rng(seed)
+    ndim = len(Nx)
+    sim = AcousticWave(
+        Nx=Nx, dx=dx, N=7, dt=0.1, threads=(8,) * (ndim - 1) + (32,), precision=precision,
+        space_order=4,
+        rho1=1.0, rho2=1.0, kappa1=1.0, kappa2=0.5,
+    )
+    length = np.array([(n - 3) * d for n, d in zip(Nx, dx)])
+    coords = [rng.uniform(0, 1, ndim) * length for _ in range(5)]
+    coords += [np.zeros(ndim), length.copy(), length * (1 + 1e-9)]  # walls, just past one
+    coords += [np.array([2 * d for d in dx])]  # on a node
+    corner = length.copy()
+    corner[0] = 0.0
+    coords += [corner]
+    coords = np.array(coords)
+    nodes, weights = distribute(sim, coords)
+    scaled_nodes, scaled_weights = distribute(sim, coords, direction=[[-1.5]])
+    signal = rng.standard_normal((7, len(coords)))
+    source = point_source(sim, coords, signal)
+    columns = rng.standard_normal((7, len(coords) * 2**ndim)).astype(sim.dtype)
+    collected = collect_source(sim, coords, columns)
+    return dict(
+        name=name, Nx=np.array(Nx), dx=np.array(dx), precision=precision, coords=coords,
+        nodes=np.asarray(nodes), weights=np.asarray(weights),
+        scaled_nodes=np.asarray(scaled_nodes), scaled_weights=np.asarray(scaled_weights),
+        signal=signal, position=np.asarray(source.position), columns_out=np.asarray(source.signal),
+        columns_in=columns, collected=np.asarray(collected),
+    )
+
+
 FORWARD = [
     dict(name="fwd2d_r1", ndim=2, Nx=(30, 37), order=2, N=80),
     dict(name="fwd2d_r2_mixed", ndim=2, Nx=(30, 40), order=4, N=80, faces="mixed"),
@@ -212,6 +297,21 @@ GRADIENTS = [
 ]
 
 
+GLUE = [
+    (dict(name="glue2d_r4", ndim=2, Nx=(40, 44), order=8, N=80),
+     [(12.3, 20.7), (25.6, 9.2)], [(3.5, 2.25 + 7.3 * k) for k in range(6)]),
+    (dict(name="glue3d_scalar_r2_pml", ndim=3, Nx=(22, 20, 24), order=4, N=40, pml=(4, 1.0),
+          scalar=True),
+     [(9.4, 8.1, 10.6)], [(5.5, 5.2, 5.0 + 3.1 * k) for k in range(4)]),
+]
+
+DISTRIBUTE = [
+    dict(name="distribute2d", Nx=(30, 25), dx=(0.7, 1.3), precision="float32", seed=3),
+    dict(name="distribute3d", Nx=(12, 14, 16), dx=(0.5, 0.9, 1.1), precision="float32", seed=4),
+    dict(name="distribute2d_f64", Nx=(21, 26), dx=(1.7, 0.3), precision="float64", seed=5),
+]
+
+
 def main(argv=None) -> int:
     parser = argparse.ArgumentParser(description=__doc__)
     parser.add_argument("--reference", default="/root/reference")
@@ -229,6 +329,18 @@ def main(argv=None) -> int:
         if args.only and args.only not in spec["name"]:
             continue
         out = run_gradients(build_case(**spec))
+        np.savez_compressed(HERE / f"{spec['name']}.npz", **out)
+        print(spec["name"], "ok", flush=True)
+    for spec, shot_coords, receiver_coords in GLUE:
+        if args.only and args.only not in spec["name"]:
+            continue
+        out = run_glue(build_case(**spec), shot_coords, receiver_coords)
+        np.savez_compressed(HERE / f"{spec['name']}.npz", **out)
+        print(spec["name"], "ok", flush=True)
+    for spec in DISTRIBUTE:
+        if args.only and args.only not in spec["name"]:
+            continue
+        out = run_distribute(**spec)
         np.savez_compressed(HERE / f"{spec['name']}.npz", **out)
         print(spec["name"], "ok", flush=True)
     return 0
