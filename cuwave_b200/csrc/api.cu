@@ -617,7 +617,8 @@ int translate(cwb_plan *p, const cwb_op &op, const size_t slot, cudaStream_t str
   const int bytes = sizeof(T);
   int rc;
   switch (op.kind) {
-  case CWB_OP_STEP: {
+  case CWB_OP_STEP:
+  case CWB_OP_SUPERPOSED: {
     cwb::StepTmaParams<T> tp;
     std::memset(&tp, 0, sizeof tp);
     cwb::StepParams<T> &sp = tp.s;
@@ -625,6 +626,19 @@ int translate(cwb_plan *p, const cwb_op &op, const size_t slot, cudaStream_t str
     int flags = 0;
     if ((rc = step_setup<T>(p, op, sp, flags, uniform)))
       return rc;
+    // the superposed step: the plain kernel with the density epilogue, lossless only
+    const bool super = op.kind == CWB_OP_SUPERPOSED;
+    if (super) {
+      if ((flags & (cwb::K_PML | cwb::K_DAMP)))
+        return fail(CWB_ERR_UNSUPPORTED, "the superposed step is lossless: no pml, no damping");
+      if (!op.g_mass || !op.g_stiff)
+        return fail(CWB_ERR_ARG, "the superposed step needs both accumulators");
+      flags |= cwb::K_SUPER;
+      sp.acc_mass = static_cast<T *>(op.g_mass);
+      sp.acc_stiff = static_cast<T *>(op.g_stiff);
+      sp.ft = (T)op.scale;
+      sp.fs = (T)op.factors[0];
+    }
     // 3D, a uniform stiffness: the blocked kernel. It stores rows of four and keeps the
     // taps it mirrors in its own run, so it wants an output level on 16-byte boundaries
     // and axes of at least 3R nodes. Elsewhere the TMA row kernel, else the plain one.
@@ -635,10 +649,10 @@ int translate(cwb_plan *p, const cwb_op &op, const size_t slot, cudaStream_t str
                            (op.c.stride * (long long)sizeof(T)) % 16 == 0;
     const bool roomy = ndim == 3 && g.n[0] >= 3 * R && g.n[1] >= 3 * R && g.n[2] >= 3 * R;
     const int H3 = ndim == 3 ? step3d_halo_r<T>(R) : -1;
-    const bool blocked = p->tma && p->blocked3 && uniform && c_aligned && roomy && H3 >= 0 &&
+    const bool blocked = !super && p->tma && p->blocked3 && uniform && c_aligned && roomy && H3 >= 0 &&
                          tma_maps<T>(p, op, derive, sp.minv, s3, cwb::S3_BX, cwb::S3_BY, H3);
     const int Hrow = ndim == 3 ? tma_halo_nd<T, 3>(R) : tma_halo_nd<T, 2>(R);
-    const bool tma = !blocked && p->tma &&
+    const bool tma = !blocked && !super && p->tma &&
                      tma_maps<T>(p, op, derive, sp.minv, tp, ndim == 3 ? cwb::TMA_BX3 : cwb::TMA_BX2,
                                  ndim == 3 ? cwb::TMA_BY3 : 1, Hrow);
     // 2D, a uniform stiffness, float, radius <= 4: the quad step, which reads u^(t-1),
@@ -646,7 +660,7 @@ int translate(cwb_plan *p, const cwb_op &op, const size_t slot, cudaStream_t str
     const auto aligned16 = [](const void *ptr, const long long stride_elems) {
       return reinterpret_cast<uintptr_t>(ptr) % 16 == 0 && (stride_elems * (long long)sizeof(T)) % 16 == 0;
     };
-    const bool quad2 = ndim == 2 && p->blocked3 && uniform && step2d_built_r<T>(R) &&
+    const bool quad2 = !super && ndim == 2 && p->blocked3 && uniform && step2d_built_r<T>(R) &&
                        aligned16(op.a.base, op.a.stride) && aligned16(op.b.base, op.b.stride) &&
                        aligned16(op.c.base, op.c.stride) && (derive || aligned16(sp.minv, 0)) &&
                        g.n[0] >= 3 * R && g.n[1] >= 3 * R;
@@ -857,6 +871,31 @@ int translate(cwb_plan *p, const cwb_op &op, const size_t slot, cudaStream_t str
       if (adv)
         q.flags |= cwb::K_ADV;
       return adjoint_dispatch<T>(q, ndim, R, uniform, mode, grid, s);
+    });
+    return CWB_OK;
+  }
+  case CWB_OP_FRECHET: {
+    if ((rc = check_level(op.a, "a")) || (rc = check_level(op.b, "b")) ||
+        (rc = check_level(op.c, "c")))
+      return rc;
+    if (!op.g_mass || !op.g_stiff)
+      return fail(CWB_ERR_ARG, "the Frechet densities need both accumulators");
+    cwb::FrechetParams<T> fp;
+    std::memset(&fp, 0, sizeof fp);
+    fp.g = g;
+    fp.a = to_level(op.a, bytes);
+    fp.b = to_level(op.b, bytes);
+    fp.c = to_level(op.c, bytes);
+    fp.acc_mass = static_cast<T *>(op.g_mass);
+    fp.acc_stiff = static_cast<T *>(op.g_stiff);
+    fp.ft = (T)op.scale;
+    for (int d = 0; d < 3; ++d)
+      fp.F[d] = (T)op.factors[d];
+    fp.ctr = p->ctr;
+    out.push_back([fp](cudaStream_t s, bool adv) {
+      cwb::FrechetParams<T> q = fp;
+      q.flags = adv ? cwb::K_ADV : 0;
+      return cwb::launch_frechet<T>(q, s);
     });
     return CWB_OK;
   }

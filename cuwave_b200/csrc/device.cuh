@@ -21,6 +21,7 @@ enum : int {
   K_ADV = 32,     // this launch ends the step: the last block advances the counter
   K_GRAD = 64,    // adjoint: accumulate g_mass, g_stiff
   K_MASS = 128,   // load: the adjoint load's inertia share
+  K_SUPER = 256,  // step: add the superposition densities of the triplet (acc_mass, acc_stiff)
 };
 
 struct DLevel {

@@ -72,6 +72,8 @@ cudaError_t launch_transfer(int kind, const TransferParams<T> &p, T *g_mass, int
                             int threads_total, cudaStream_t stream);
 template <typename T>
 cudaError_t launch_pml_aux(const PmlAuxParams<T> &p, cudaStream_t stream);
+template <typename T>
+cudaError_t launch_frechet(const FrechetParams<T> &p, cudaStream_t stream);
 cudaError_t launch_set_counter(int *ctr, int t0, cudaStream_t stream);
 
 enum : int { TR_EXCITE = 0, TR_LOAD = 1, TR_RECORD = 2, TR_REPLAY = 3, TR_REFILL = 4 };

@@ -29,6 +29,9 @@ struct StepParams {
   const T *src_weight;
   const T *signal;
   int nsrc, sig_mul, sig_add;
+  // K_SUPER: acc_mass += ft (b - c_old)^2, acc_stiff += fs sum_d f_d (b[+s_d] - b[-s_d])^2
+  T *acc_mass, *acc_stiff;
+  T ft, fs;
   int *ctr;
 };
 
@@ -62,6 +65,18 @@ struct TransferParams {
   void *record;
   int num, row_mul, row_add, store;  // store: 0 T, 1 bfloat16 bits, 2 float32
   T scale;
+  int flags;
+  int *ctr;
+};
+
+// both Frechet densities of a triplet a, b, c (frechet_kernel)
+template <typename T>
+struct FrechetParams {
+  Geometry g;
+  DLevel a, b, c;
+  T *acc_mass, *acc_stiff;
+  T ft;     // the mass density factor
+  T F[3];   // the stiffness density factors, per axis
   int flags;
   int *ctr;
 };

@@ -251,6 +251,20 @@ __global__ void __launch_bounds__(BX *BY) step_kernel(const StepParams<T> p) {
       }
       if ((flags & K_REFILL) && held)
         v = (T)0;
+      if (flags & K_SUPER) {
+        // superposed_kernel (scalar_sensitivity.cu:600-668): the mass density of the
+        // triplet before, whose oldest level c still holds, and the stiffness density of
+        // this one, central differences of its middle level read as stored
+        const T dudt = uc - u2[idx];
+        p.acc_mass[idx] += p.ft * dudt * dudt;
+        T sum = (T)0;
+#pragma unroll
+        for (int d = 0; d < NDIM; ++d) {
+          const T gd = u1[idx + strides[d]] - u1[idx - strides[d]];
+          sum = d == 0 ? p.f[0] * gd * gd : sum + p.f[d] * gd * gd;
+        }
+        p.acc_stiff[idx] += p.fs * sum;
+      }
       u2[idx] = v;
       if (flags & K_REFILL) {
 #pragma unroll

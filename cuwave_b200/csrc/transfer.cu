@@ -30,6 +30,16 @@ cudaError_t launch_pml_aux(const PmlAuxParams<T> &p, cudaStream_t stream) {
   return cudaGetLastError();
 }
 
+template <typename T>
+cudaError_t launch_frechet(const FrechetParams<T> &p, cudaStream_t stream) {
+  const long long total = (long long)p.g.n[0] * p.g.s[0];
+  const long long blocks = (total + TRANSFER_THREADS - 1) / TRANSFER_THREADS;
+  if (blocks <= 0 || blocks > 0x7fffffffLL)
+    return cudaErrorInvalidValue;
+  frechet_kernel<T><<<(unsigned)blocks, TRANSFER_THREADS, 0, stream>>>(p);
+  return cudaGetLastError();
+}
+
 __global__ void set_counter_kernel(int *ctr, const int t0) {
   ctr[0] = t0;
   ctr[1] = 0;
@@ -44,6 +54,8 @@ template cudaError_t launch_transfer<float>(int, const TransferParams<float> &, 
                                             int, cudaStream_t);
 template cudaError_t launch_transfer<double>(int, const TransferParams<double> &, double *,
                                              int, int, cudaStream_t);
+template cudaError_t launch_frechet<float>(const FrechetParams<float> &, cudaStream_t);
+template cudaError_t launch_frechet<double>(const FrechetParams<double> &, cudaStream_t);
 template cudaError_t launch_pml_aux<float>(const PmlAuxParams<float> &, cudaStream_t);
 template cudaError_t launch_pml_aux<double>(const PmlAuxParams<double> &, cudaStream_t);
 

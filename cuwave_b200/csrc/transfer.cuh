@@ -204,4 +204,38 @@ __global__ void pml_aux_kernel(const PmlAuxParams<T> p) {
   finish_step(p.ctr, p.flags & K_ADV);
 }
 
+// Both Frechet densities of one triplet a, b, c of the interior, added into the
+// accumulators: ft (c - a)^2 to acc_mass and sum_d F_d (b[+s_d] - b[-s_d])^2 to
+// acc_stiff (frechet_kernel, cuwave/kernels/scalar_sensitivity.cu:353-385). One thread
+// per node of the padded grid.
+template <typename T>
+__global__ void frechet_kernel(const FrechetParams<T> p) {
+  const int t = step_index(p.ctr);
+  const Geometry &g = p.g;
+  const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long total = (long long)g.n[0] * g.s[0];
+  if (k < total) {
+    int rest = (int)k, inside = 1;
+    for (int d = 0; d < g.ndim; ++d) {
+      const int a = rest / g.s[d];
+      rest -= a * g.s[d];
+      inside &= a > 0 && a < g.n[d] - 1;
+    }
+    if (inside) {
+      const T *a = level<T>(p.a, t);
+      const T *b = level<T>(p.b, t);
+      const T *c = level<T>(p.c, t);
+      const T dudt = c[k] - a[k];
+      p.acc_mass[k] += p.ft * dudt * dudt;
+      T sum = (T)0;
+      for (int d = 0; d < g.ndim; ++d) {
+        const T gd = b[k + g.s[d]] - b[k - g.s[d]];
+        sum = d == 0 ? p.F[0] * gd * gd : sum + p.F[d] * gd * gd;
+      }
+      p.acc_stiff[k] += sum;
+    }
+  }
+  finish_step(p.ctr, p.flags & K_ADV);
+}
+
 }  // namespace cwb

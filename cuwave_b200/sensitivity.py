@@ -1,6 +1,8 @@
-"""Adjoint sensitivities: `sensitivity`, `reconstruction_sensitivity`, `source_sensitivity`.
+"""Adjoint sensitivities: `sensitivity`, `reconstruction_sensitivity`,
+`superposition_sensitivity`, `source_sensitivity`.
 
-Same arguments and returns as cuwave `sensitivity.py` (384-497, 500-750, 1054-1111):
+Same arguments and returns as cuwave `sensitivity.py` (384-497, 500-750, 753-893,
+1054-1111):
 `(cost, {"mass": dJ/dm, "stiff": dJ/dk}, traces, info)` with the gradients over the
 padded grid, cell-weighted and zeroed in a pml layer, or `(cost, dJ/dsignal, traces,
 info)` for the source. The adjoint marches run in the native library: the transposed
@@ -11,6 +13,7 @@ the gather inside the step) and the adjoint load (CWB_OP_LOAD).
 from __future__ import annotations
 
 import math
+import warnings
 from collections.abc import Callable
 from dataclasses import replace
 
@@ -44,6 +47,10 @@ STRIP_DTYPES = {
 }
 # round-off growth past which a damped node is recorded rather than run backwards
 REVERSIBLE_GROWTH = {"float32": 1e2, "float64": 1e6}
+# lines the adjoint up with the reconstructed forward triplet (cuwave sensitivity.py:45)
+ADJOINT_DELAY = 1
+# cancellation past which B(w, w) - B(u, u) has eaten too much of the mantissa to trust
+CANCELLATION_LIMIT = {"float32": 1e5, "float64": 1e12}
 
 
 def l2_misfit(observed) -> Callable:
@@ -215,6 +222,134 @@ def source_sensitivity(sim: Simulation, source: Source, indicator, sensors, obje
     plan.march(ops, 0, sim.N)
     gradient = lam.flip(0) * sim.adjoint_weights(position)
     return cost, gradient.contiguous(), um, {}
+
+
+# ------------------------------------------------------------------- superposition
+def require_lossless(sim: Simulation) -> None:
+    """Raise for a damping field or a pml: time reversal needs a lossless step (cuwave sensitivity.py:130-136)."""
+    if sim.damping is not None or sim.pml is not None:
+        raise NotImplementedError(
+            "superposition_sensitivity rebuilds the forward field by running it backwards, "
+            "which only a lossless operator allows; use sensitivity"
+        )
+
+
+def _accumulated(accs: dict) -> float:
+    """The norm over every accumulator (cuwave sensitivity.py:85-88)."""
+    return math.sqrt(sum(float(torch.linalg.vector_norm(f)) ** 2 for f in accs.values()))
+
+
+def _density_factors(sim: Simulation, sign: float) -> tuple[float, float]:
+    """(mass, stiffness) density factors of the superposed step, rounded to the
+    simulation's dtype (cuwave scalar.py:813-838)."""
+    factors = sim.step_factors()
+    ratios = [-sign / (2.0 * d) ** 2 / float(f) for d, f in zip(sim.dx, factors)]
+    if not np.allclose(ratios, ratios[0]):
+        raise ValueError(f"step factors {factors} are not proportional to 1 / dx**2")
+    return (float(sim.np_dtype(sign / (2.0 * sim.dt) ** 2)), float(sim.np_dtype(ratios[0])))
+
+
+def superposition_sensitivity(sim: Simulation, source: Source, indicator, sensors,
+                              objective: Callable, scale: float = 1.0):
+    """Cost and gradients as `sensitivity`, in three field slots instead of N + 2
+    (cuwave sensitivity.py:753-893).
+
+    The gradient densities are bilinear in the forward and adjoint fields, so the cross
+    term is read off B(u + k lambda) - B(u): the forward march subtracts B(u, u) as it
+    steps (CWB_OP_SUPERPOSED), then the lossless field runs back in time from its last
+    two levels carrying w = u + k lambda (the source reversed, the adjoint load scaled
+    by k and one step late) and adds B(w, w); the Frechet kernel (CWB_OP_FRECHET) closes
+    each pass with its last triplet's mass density. The difference over 2k is the
+    gradient, cell weighted. `scale` is k: the cancellation it leaves is returned in
+    info["cancellation"], with a warning past what the precision can carry.
+    """
+    require_lossless(sim)
+    require_interior(sim, sensors, "sensor")
+    require_interior(sim, source.position, "source")
+    dev = device()
+    mat = sim.build_materials(indicator)
+    shot = prepare_shot(sim, mat, source.position, source.signal)
+    require_off_held_walls(sim, shot.position)
+    plan = sim.plan()
+    N = sim.N
+    material = sim.material(mat)
+    accs = sim.gradient_fields(mat)
+    U = torch.zeros((3, *sim.Nx_padded), dtype=sim.dtype, device=dev)
+    sensor_lin = flatten_indices(sim, sensors)
+    um = torch.zeros((N, sensor_lin.numel()), dtype=sim.dtype, device=dev)
+    zero = (0.0, 0.0, 0.0)
+
+    def frechet(a, b, c, ft):
+        return nat.op(nat.OP_FRECHET, a=nat.level(U, mul=0, add=a), b=nat.level(U, mul=0, add=b),
+                      c=nat.level(U, mul=0, add=c), g_mass=accs["mass"],
+                      g_stiff=accs["stiff"], scale=ft, factors=zero)
+
+    # ---------------------------------------------------------------- forward pass
+    # step t: U[t % 3], U[(t + 1) % 3] -> U[(t + 2) % 3], the mass density one triplet late
+    ft, fs = _density_factors(sim, -1.0)
+    a = nat.level(U, add=0, period=3)
+    b = nat.level(U, add=1, period=3)
+    c = nat.level(U, add=2, period=3)
+    ops = [nat.op(nat.OP_SUPERPOSED, a=a, b=b, c=c, mat=material, g_mass=accs["mass"],
+                  g_stiff=accs["stiff"], scale=ft, factors=(fs, 0.0, 0.0))]
+    src = shot.points()
+    if src.num:
+        ops.append(nat.op(nat.OP_EXCITE, a=c, points=src))
+    ops.append(nat.op(nat.OP_REFILL, a=c))
+    if sensor_lin.numel():
+        ops.append(nat.op(nat.OP_RECORD, a=c, points=nat.points(sensor_lin, um)))
+    plan.march(ops, 0, N)
+    t = N - 1
+    plan.march([frechet(t % 3, (t + 1) % 3, (t + 2) % 3, ft)], 0, 1, graph=False)
+    cost, dphi = _objective(objective, um)
+
+    # ----------------------------------------------------------- adjoint excitation
+    before = _accumulated(accs)
+    position = torch.cat((as_position(sim, sensors), shot.position), dim=1)
+    lin = flatten_indices(sim, position)
+    signal = torch.cat(
+        (adjoint_signal(sim, dphi, sensors, scale, ADJOINT_DELAY), shot.signal[:N].flip(0)),
+        dim=1,
+    ).contiguous()
+    weight = sim.excitation_weights(mat, lin)
+    load = nat.points(lin, signal, weight=weight)
+
+    # --------------------------------------------------------------- backward pass
+    # step t: U[(N + 1 - t) % 3], U[(N - t) % 3] -> U[(N + 2 - t) % 3], from u^(N-1), u^(N-2)
+    ft, fs = _density_factors(sim, 1.0)
+
+    def backward_ops(mass_factor):
+        a = nat.level(U, mul=-1, add=N + 1, period=3)
+        b = nat.level(U, mul=-1, add=N, period=3)
+        c = nat.level(U, mul=-1, add=N + 2, period=3)
+        return [
+            nat.op(nat.OP_SUPERPOSED, a=a, b=b, c=c, mat=material, g_mass=accs["mass"],
+                   g_stiff=accs["stiff"], scale=mass_factor, factors=(fs, 0.0, 0.0)),
+            nat.op(nat.OP_EXCITE, a=c, points=load),
+            nat.op(nat.OP_REFILL, a=c),
+        ]
+
+    # the first triplet before is the forward's last, already counted
+    plan.march(backward_ops(0.0), 0, 1, graph=False)
+    plan.march(backward_ops(ft), 1, N - 1)
+    plan.march([frechet(2, 1, 0, ft)], 0, 1, graph=False)
+
+    after = _accumulated(accs)
+    cancellation = before / after if after > 0.0 else float("inf")
+    limit = CANCELLATION_LIMIT[sim.precision]
+    if cancellation > limit:
+        warnings.warn(
+            f"superposition scale={scale:g} leaves a cancellation of {cancellation:.1e} in "
+            f"{sim.precision}, past the usable {limit:.0e}: the gradient is largely "
+            f"round-off. Raise scale by about {cancellation / limit:.0e}.",
+            RuntimeWarning,
+            stacklevel=2,
+        )
+    norm = float(sim.np_dtype(1.0 / (2.0 * scale)))
+    accs = sim.finalize_gradients(accs)
+    for f in accs.values():
+        f *= norm
+    return cost, accs, um, {"scale": scale, "cancellation": cancellation}
 
 
 # ------------------------------------------------------------------- reconstruction

@@ -126,6 +126,16 @@ enum {
    * against d = lambda^t, with scale = 1 / dt^2 and factors F_d. Replaces
    * gradient_kernel (scalar_sensitivity.cu:303-350). */
   CWB_OP_GRADIENT = 9,
+  /* The leapfrog update of CWB_OP_STEP (a, b read, c written; lossless: no pml, no
+   * damping) that first adds the superposition densities into g_mass and g_stiff: the
+   * mass density of the triplet before, scale * (b - c)^2 with c's old value, and the
+   * stiffness density of this triplet, factors[0] * sum_d f_d (b[+s_d] - b[-s_d])^2.
+   * c must not alias a. Replaces superposed_kernel (scalar_sensitivity.cu:600-668). */
+  CWB_OP_SUPERPOSED = 10,
+  /* Both Frechet densities of the triplet a, b, c over the interior: g_mass +=
+   * scale * (c - a)^2, g_stiff += sum_d factors[d] * (b[+s_d] - b[-s_d])^2. Replaces
+   * frechet_kernel (scalar_sensitivity.cu:353-385). */
+  CWB_OP_FRECHET = 11,
 };
 
 /* op flags */
@@ -143,8 +153,10 @@ typedef struct cwb_op {
   void *memory[3];   /* pml memory per lined axis: 3 slab rows forward, 5 adjoint */
   void *g_mass;
   void *g_stiff;
-  double scale;      /* ADJOINT / LOAD: 1 / dt^2; GRADIENT: 1 / dt^2 */
-  double factors[3]; /* GRADIENT: F_d = f_d / dt^2 */
+  double scale;      /* ADJOINT / LOAD / GRADIENT: 1 / dt^2; SUPERPOSED / FRECHET: the
+                        mass density factor */
+  double factors[3]; /* GRADIENT: F_d = f_d / dt^2; SUPERPOSED: [0] the stiffness density
+                        factor; FRECHET: the per-axis stiffness density factors */
 } cwb_op;
 
 /* Create and destroy a plan. Replaces compile_kernels (cuwave/wave.py:637-647): one

@@ -13,6 +13,9 @@ reference kernel launch) and, here in numpy, the setup and the drivers around th
     simulate               cuwave/wave.py:1071-1163 (plain step order, 1119-1127)
     sensitivity            cuwave/sensitivity.py:384-497 (fused adjoint, 468-480)
     source_sensitivity     cuwave/sensitivity.py:1054-1111
+    superposition          cuwave/sensitivity.py:753-893 (superposed_kernel /
+                           frechet_kernel, cuwave/kernels/scalar_sensitivity.cu:353-385,
+                           600-668, restated in numpy)
 
 Pinned against the reference's own outputs: tests/golden/*.npz, produced by running
 the reference package itself (tests/golden/make_golden.py).
@@ -382,6 +385,103 @@ class Case:
             lam[m] = l0.ravel()[self.source_lin]
         gradient = lam[::-1] * self.sensor_weights(self.source_lin)
         return cost, np.ascontiguousarray(gradient), um
+
+
+    # ------------------------------------------------------------ superposition
+    def densities(self, acc_mass, acc_stiff, before, middle, newest, ft, F):
+        """Both Frechet densities of one triplet over the interior, in place.
+
+        acc_mass += ft (newest - before)^2 and acc_stiff += sum_d F_d (middle[+s_d] -
+        middle[-s_d])^2, each product rounded in the kernel's order (frechet_kernel,
+        cuwave/kernels/scalar_sensitivity.cu:353-385; superposed_kernel 637-654 with
+        newest = the middle level and before = the level it is about to overwrite).
+        """
+        dt_ = self.dtype
+        inner = tuple(slice(1, n - 1) for n in self.Nx)
+        dudt = newest[inner] - before[inner]
+        acc_mass[inner] += (dt_(ft) * dudt) * dudt
+        total = None
+        for d in range(self.ndim):
+            hi = tuple(slice(2, n) if e == d else slice(1, n - 1) for e, n in enumerate(self.Nx))
+            lo = tuple(slice(0, n - 2) if e == d else slice(1, n - 1) for e, n in enumerate(self.Nx))
+            g = middle[hi] - middle[lo]
+            term = (dt_(F[d]) * g) * g
+            total = term if total is None else total + term
+        acc_stiff[inner] += total
+
+    def superposed(self, u0, u1, u2, acc_mass, acc_stiff, ft, fs):
+        """superposed_kernel (scalar_sensitivity.cu:600-668): the densities against u2's
+        old value, then the plain step into u2."""
+        dt_ = self.dtype
+        # the kernel forms sum_d f_d g_d^2, then scales it by fs
+        inner = tuple(slice(1, n - 1) for n in self.Nx)
+        dudt = u1[inner] - u2[inner]
+        acc_mass[inner] += (dt_(ft) * dudt) * dudt
+        total = None
+        for d in range(self.ndim):
+            hi = tuple(slice(2, n) if e == d else slice(1, n - 1) for e, n in enumerate(self.Nx))
+            lo = tuple(slice(0, n - 2) if e == d else slice(1, n - 1) for e, n in enumerate(self.Nx))
+            g = u1[hi] - u1[lo]
+            term = (self.f[d] * g) * g
+            total = term if total is None else total + term
+        acc_stiff[inner] += dt_(fs) * total
+        self.step(u0, u1, u2)
+
+    def superposition(self, N, dphi_of, scale=1.0, dx=None):
+        """Gradients in three slots by superposition (cuwave sensitivity.py:753-893).
+
+        Forward: the superposed step subtracts B(u, u) while it records; backward, the
+        field runs back in time carrying w = u + k lambda (the source reversed and the
+        adjoint load scaled by k, one step late) and adds B(w, w); the gradients are the
+        difference over 2k, cell weighted. Returns cost, {"mass", "stiff"}, traces,
+        cancellation.
+        """
+        dt_ = self.dtype
+        dx = dx or (1.0,) * self.ndim
+        U = np.zeros((3, *self.shape), dt_)
+        um = np.zeros((N, self.sensor_lin.size), dt_)
+        acc = {"mass": np.zeros(self.shape, dt_), "stiff": np.zeros(self.shape, dt_)}
+
+        def factors(sign):
+            ratios = [-sign / (2.0 * d) ** 2 / float(f) for d, f in zip(dx, self.f[: self.ndim])]
+            return dt_(sign / (2.0 * self.dt) ** 2), dt_(ratios[0])
+
+        ft, fs = factors(-1.0)
+        for t in range(N):
+            u0, u1, u2 = U[t % 3], U[(t + 1) % 3], U[(t + 2) % 3]
+            self.superposed(u0, u1, u2, acc["mass"], acc["stiff"], ft, fs)
+            if self.source_lin.size:
+                self.excite(u2, self.source_lin, self.source_weight, self.signal[t])
+            self.refill(u2)
+            um[t] = u2.ravel()[self.sensor_lin]
+        t = N - 1
+        self.densities(acc["mass"], acc["stiff"], U[t % 3], U[(t + 1) % 3], U[(t + 2) % 3],
+                       ft, [0.0] * self.ndim)
+        cost, dphi = dphi_of(um)
+        before = np.sqrt(sum(float(np.linalg.norm(f)) ** 2 for f in acc.values()))
+
+        # the adjoint load one step late and scaled by k, beside the source reversed
+        signal = np.asarray(dphi, dt_)[::-1] / self.sensor_weights(self.sensor_lin)
+        signal = np.concatenate((signal[1:], np.zeros_like(signal[:1])))
+        signal = dt_(scale) * signal
+        lin = np.concatenate((self.sensor_lin, self.source_lin)).astype(np.int32)
+        rows = np.ascontiguousarray(
+            np.concatenate((signal, self.signal[:N][::-1]), axis=1), dt_)
+        weight = self.excitation_weights(lin)
+        ft, fs = factors(1.0)
+        for t in range(N):
+            u0, u1, u2 = (U[(N + i - t) % 3] for i in (1, 0, 2))
+            self.superposed(u0, u1, u2, acc["mass"], acc["stiff"], ft if t else dt_(0.0), fs)
+            self.excite(u2, lin, weight, rows[t])
+            self.refill(u2)
+        self.densities(acc["mass"], acc["stiff"], U[2], U[1], U[0], ft, [0.0] * self.ndim)
+        after = np.sqrt(sum(float(np.linalg.norm(f)) ** 2 for f in acc.values()))
+        cancellation = before / after if after > 0.0 else float("inf")
+        norm = dt_(1.0 / (2.0 * scale))
+        for f in acc.values():
+            self.cell_weights(f)
+            f *= norm
+        return cost, acc, um, cancellation
 
 
 def l2(observed):

@@ -183,6 +183,30 @@ def run_gradients(case):
     return out
 
 
+def run_superposition(case, scale):
+    """superposition_sensitivity of cuwave's sensitivity.py on a lossless case."""
+    from cuwave.sensitivity import l2_misfit, superposition_sensitivity
+    from cuwave.wave import Source, simulate
+
+    sim = make_sim(case)
+    source = Source(case["source"].copy(), case["signal"].astype(sim.dtype))
+    perturbed = design(case, sim).copy()
+    perturbed *= 0.95
+    _, observed = simulate(sim, source, perturbed, case["sensors"].copy())
+    observed = np.asarray(observed)
+    cost, grads, um, info = superposition_sensitivity(
+        sim, source, design(case, sim).copy(), case["sensors"].copy(), l2_misfit(observed),
+        scale=scale,
+    )
+    out = dict(case)
+    out.update(
+        observed=observed, scale=np.array(scale), cost=np.array(cost), traces=np.asarray(um),
+        g_mass=np.asarray(grads["mass"]), g_stiff=np.asarray(grads["stiff"]),
+        cancellation=np.array(info["cancellation"]),
+    )
+    return out
+
+
 def run_glue(case, shot_coords, receiver_coords):
     """The shot glue of cuwave utils.py on off-node shots and receivers."""
     from cuwave.sensitivity import l2_misfit, reconstruction_sensitivity, source_sensitivity
@@ -297,6 +321,15 @@ GRADIENTS = [
 ]
 
 
+SUPERPOSITION = [
+    (dict(name="sup2d_r4", ndim=2, Nx=(34, 38), order=8, N=70), 3e4),
+    (dict(name="sup2d_r2_mixed", ndim=2, Nx=(30, 33), order=4, N=60, faces="mixed"), 0.01),
+    (dict(name="sup2d_r1_dir_taylor", ndim=2, Nx=(28, 30), order=2, N=50, faces="dirichlet",
+          stencil="taylor"), 3e4),
+    (dict(name="sup3d_scalar_r2", ndim=3, Nx=(18, 20, 22), order=4, N=40, scalar=True), 1e4),
+    (dict(name="sup2d_r4_f64", ndim=2, Nx=(32, 36), order=8, N=60, precision="float64"), 1e3),
+]
+
 GLUE = [
     (dict(name="glue2d_r4", ndim=2, Nx=(40, 44), order=8, N=80),
      [(12.3, 20.7), (25.6, 9.2)], [(3.5, 2.25 + 7.3 * k) for k in range(6)]),
@@ -329,6 +362,12 @@ def main(argv=None) -> int:
         if args.only and args.only not in spec["name"]:
             continue
         out = run_gradients(build_case(**spec))
+        np.savez_compressed(HERE / f"{spec['name']}.npz", **out)
+        print(spec["name"], "ok", flush=True)
+    for spec, scale in SUPERPOSITION:
+        if args.only and args.only not in spec["name"]:
+            continue
+        out = run_superposition(build_case(**spec), scale)
         np.savez_compressed(HERE / f"{spec['name']}.npz", **out)
         print(spec["name"], "ok", flush=True)
     for spec, shot_coords, receiver_coords in GLUE:

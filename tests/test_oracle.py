@@ -73,3 +73,32 @@ def test_float32_error_against_float64(name):
     err = np.linalg.norm(f32.astype(np.float64) - f64) / np.linalg.norm(f64)
     terr = np.linalg.norm(t32.astype(np.float64) - t64) / np.linalg.norm(t64)
     assert 0 < err < 1e-5 and 0 < terr < 1e-5, (err, terr)
+
+
+SUPERPOSITION = sorted(p.stem for p in cases.GOLDEN.glob("sup*.npz"))
+
+
+@pytest.mark.parametrize("name", SUPERPOSITION)
+def test_superposition_matches_reference(name):
+    """The three-slot superposition adjoint, bit for bit with the reference's."""
+    fx = cases.load(name)
+    case = cases.oracle_case(fx)
+    scale = float(fx["scale"])
+    cost, grads, traces, cancellation = case.superposition(
+        int(fx["N"]), o.l2(fx["observed"]), scale=scale)
+    np.testing.assert_array_equal(traces, fx["traces"])
+    np.testing.assert_array_equal(grads["mass"], fx["g_mass"])
+    np.testing.assert_array_equal(grads["stiff"], fx["g_stiff"])
+    assert cost == pytest.approx(float(fx["cost"]), rel=1e-5)
+    assert cancellation == pytest.approx(float(fx["cancellation"]), rel=1e-3)
+
+
+def test_superposition_cancellation_tracks_the_scale():
+    """The cancellation B(w, w) - B(u, u) leaves scales as 1 / k while the cross term
+    dominates the k^2 one (cuwave sensitivity_test.py:847-855)."""
+    fx = cases.load("sup2d_r4_f64")
+    objective = o.l2(fx["observed"])
+    N = int(fx["N"])
+    loose = cases.oracle_case(fx).superposition(N, objective, scale=10.0)[3]
+    tight = cases.oracle_case(fx).superposition(N, objective, scale=100.0)[3]
+    assert loose / tight == pytest.approx(10.0, rel=0.03)
