@@ -18,7 +18,7 @@ ERRORS = {-1: "bad argument", -2: "CUDA error", -3: "unsupported", -4: "allocati
 
 OP_STEP, OP_EXCITE, OP_REPLAY, OP_REFILL, OP_RECORD = 1, 2, 3, 4, 5
 OP_PML_AUX, OP_ADJOINT, OP_LOAD, OP_GRADIENT = 6, 7, 8, 9
-OP_SUPERPOSED, OP_FRECHET = 10, 11
+OP_SUPERPOSED, OP_FRECHET, OP_DFT = 10, 11, 12
 PML, FOLD_SOURCES, FOLD_REFILL, GRAD = 1, 2, 4, 8
 STORE_NATIVE, STORE_BF16, STORE_F32 = 0, 1, 2
 
@@ -89,6 +89,7 @@ class Op(ctypes.Structure):
         ("g_stiff", ctypes.c_void_p),
         ("scale", ctypes.c_double),
         ("factors", ctypes.c_double * 3),
+        ("columns", ctypes.c_int32),
     ]
 
 

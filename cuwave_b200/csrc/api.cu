@@ -940,6 +940,7 @@ int translate(cwb_plan *p, const cwb_op &op, const size_t slot, cudaStream_t str
   case CWB_OP_LOAD:
   case CWB_OP_RECORD:
   case CWB_OP_REPLAY:
+  case CWB_OP_DFT:
   case CWB_OP_REFILL: {
     if ((rc = check_level(op.a, "a")))
       return rc;
@@ -983,7 +984,14 @@ int translate(cwb_plan *p, const cwb_op &op, const size_t slot, cudaStream_t str
       kind = op.kind == CWB_OP_EXCITE   ? cwb::TR_EXCITE
              : op.kind == CWB_OP_LOAD   ? cwb::TR_LOAD
              : op.kind == CWB_OP_RECORD ? cwb::TR_RECORD
+             : op.kind == CWB_OP_DFT    ? cwb::TR_DFT
                                         : cwb::TR_REPLAY;
+      if (op.kind == CWB_OP_DFT) {
+        if (!op.g_mass || op.columns <= 0 || pt.store != 0)
+          return fail(CWB_ERR_ARG, "a DFT needs an accumulator, its columns and a native table");
+        tp.columns = op.columns;
+        g_mass = static_cast<T *>(op.g_mass);
+      }
       if (op.kind == CWB_OP_LOAD && op.g_mass) {
         if ((rc = check_level(op.c, "c")))
           return rc;

@@ -76,6 +76,6 @@ template <typename T>
 cudaError_t launch_frechet(const FrechetParams<T> &p, cudaStream_t stream);
 cudaError_t launch_set_counter(int *ctr, int t0, cudaStream_t stream);
 
-enum : int { TR_EXCITE = 0, TR_LOAD = 1, TR_RECORD = 2, TR_REPLAY = 3, TR_REFILL = 4 };
+enum : int { TR_EXCITE = 0, TR_LOAD = 1, TR_RECORD = 2, TR_REPLAY = 3, TR_REFILL = 4, TR_DFT = 5 };
 
 }  // namespace cwb

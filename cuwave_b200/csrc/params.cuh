@@ -64,6 +64,7 @@ struct TransferParams {
   const T *weight;
   void *record;
   int num, row_mul, row_add, store;  // store: 0 T, 1 bfloat16 bits, 2 float32
+  int columns;                       // DFT: phase factors per table row
   T scale;
   int flags;
   int *ctr;

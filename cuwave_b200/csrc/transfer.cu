@@ -16,6 +16,7 @@ cudaError_t launch_transfer(const int kind, const TransferParams<T> &p, T *g_mas
   case TR_RECORD: record_kernel<T><<<blocks, TRANSFER_THREADS, 0, stream>>>(p); break;
   case TR_REPLAY: replay_kernel<T><<<blocks, TRANSFER_THREADS, 0, stream>>>(p); break;
   case TR_REFILL: refill_kernel<T><<<blocks, TRANSFER_THREADS, 0, stream>>>(p, faces); break;
+  case TR_DFT: dft_kernel<T><<<blocks, TRANSFER_THREADS, 0, stream>>>(p, g_mass); break;
   default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();

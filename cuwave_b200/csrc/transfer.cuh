@@ -204,6 +204,23 @@ __global__ void pml_aux_kernel(const PmlAuxParams<T> p) {
   finish_step(p.ctr, p.flags & K_ADV);
 }
 
+// A running DFT at the points: acc[k * num + j] += table[row * columns + k] * a[lin[j]],
+// one thread per point (dft_kernel, cuwave/kernels/common.cuh:506-518).
+template <typename T>
+__global__ void dft_kernel(const TransferParams<T> p, T *acc) {
+  const int t = step_index(p.ctr);
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j < p.num) {
+    const T *a = level<T>(p.a, t);
+    const T uc = a[p.lin[j]];
+    const T *table = reinterpret_cast<const T *>(p.record) +
+                     ((long long)p.row_mul * t + p.row_add) * p.columns;
+    for (int k = 0; k < p.columns; ++k)
+      acc[(long long)k * p.num + j] += table[k] * uc;
+  }
+  finish_step(p.ctr, p.flags & K_ADV);
+}
+
 // Both Frechet densities of one triplet a, b, c of the interior, added into the
 // accumulators: ft (c - a)^2 to acc_mass and sum_d F_d (b[+s_d] - b[-s_d])^2 to
 // acc_stiff (frechet_kernel, cuwave/kernels/scalar_sensitivity.cu:353-385). One thread

@@ -1,8 +1,8 @@
 """Adjoint sensitivities: `sensitivity`, `reconstruction_sensitivity`,
-`superposition_sensitivity`, `source_sensitivity`.
+`superposition_sensitivity`, `spectral_sensitivity`, `source_sensitivity`.
 
 Same arguments and returns as cuwave `sensitivity.py` (384-497, 500-750, 753-893,
-1054-1111):
+896-1051, 1054-1111):
 `(cost, {"mass": dJ/dm, "stiff": dJ/dk}, traces, info)` with the gradients over the
 padded grid, cell-weighted and zeroed in a pml layer, or `(cost, dJ/dsignal, traces,
 info)` for the source. The adjoint marches run in the native library: the transposed
@@ -51,6 +51,11 @@ REVERSIBLE_GROWTH = {"float32": 1e2, "float64": 1e6}
 ADJOINT_DELAY = 1
 # cancellation past which B(w, w) - B(u, u) has eaten too much of the mantissa to trust
 CANCELLATION_LIMIT = {"float32": 1e5, "float64": 1e12}
+# share of the spectrum the last period still adds, past which the run stopped short
+DECAY_LIMIT = 1e-2
+# dcost/dtraces off the sinusoids at `frequencies` by more than this is not spectral
+FIT_LIMIT = {"float32": 1e-4, "float64": 1e-10}
+PULSE_PERIODS = 1.0  # spread of the adjoint pulse envelope, in periods
 
 
 def l2_misfit(observed) -> Callable:
@@ -350,6 +355,205 @@ def superposition_sensitivity(sim: Simulation, source: Source, indicator, sensor
     for f in accs.values():
         f *= norm
     return cost, accs, um, {"scale": scale, "cancellation": cancellation}
+
+
+# ------------------------------------------------------------------------ spectral
+def phase_table(sim: Simulation, frequencies) -> np.ndarray:
+    """(N, 2F) host table of cos(omega t) and -sin(omega t), interleaved per frequency,
+    built in float64 (cuwave sensitivity.py:295-303)."""
+    t = np.arange(sim.N, dtype=np.float64) * sim.dt
+    phase = 2.0 * np.pi * t[:, None] * np.asarray(frequencies, np.float64)[None, :]
+    table = np.empty((sim.N, 2 * phase.shape[1]))
+    table[:, 0::2] = np.cos(phase)
+    table[:, 1::2] = -np.sin(phase)
+    return table
+
+
+def spectral_load(sim: Simulation, dphi, table: np.ndarray) -> tuple[np.ndarray, float]:
+    """The complex load alpha + i beta per frequency with dphi = sum alpha cos + beta sin,
+    by least squares on the host, and the fit's relative residual (cuwave
+    sensitivity.py:306-321)."""
+    basis = np.empty_like(table)
+    basis[:, 0::2], basis[:, 1::2] = table[:, 0::2], -table[:, 1::2]
+    if isinstance(dphi, torch.Tensor):
+        dphi = dphi.detach().cpu().numpy()
+    target = np.asarray(dphi).astype(np.float64)
+    coef = np.linalg.lstsq(basis, target, rcond=None)[0]
+    norm = float(np.linalg.norm(target))
+    fit = float(np.linalg.norm(target - basis @ coef)) / norm if norm > 0.0 else 0.0
+    return coef[0::2] + 1j * coef[1::2], fit
+
+
+def spectral_pulse(sim: Simulation, frequency: float, load: np.ndarray) -> np.ndarray:
+    """(N, num) Gaussian-windowed pulses whose DTFT at `frequency` is `load`
+    (cuwave sensitivity.py:324-342)."""
+    sigma = PULSE_PERIODS / frequency
+    t = np.arange(sim.N, dtype=np.float64) * sim.dt
+    if 8.0 * sigma > t[-1]:
+        raise ValueError(
+            f"the adjoint pulse spans {8.0 * sigma:.3g}, longer than the run {t[-1]:.3g}"
+        )
+    envelope = np.exp(-0.5 * ((t - 4.0 * sigma) / sigma) ** 2)
+    omega = 2.0 * np.pi * frequency
+    carriers = envelope * np.stack((np.cos(omega * t), np.sin(omega * t)))
+    spectra_ = carriers @ np.exp(-1j * omega * t)
+    system = np.array([spectra_.real, spectra_.imag])
+    amplitudes = np.linalg.solve(system, np.stack((load.real, load.imag)))
+    return carriers.T @ amplitudes
+
+
+def settled(sim: Simulation, spectrum: np.ndarray, last: np.ndarray, frequency: float):
+    """The DFT continued past step N as the constant the run settled to, its geometric
+    tail summed in closed form (cuwave sensitivity.py:345-354)."""
+    z = np.exp(-2j * np.pi * frequency * sim.dt)
+    return spectrum + last * (z**sim.N / (1.0 - z))
+
+
+def spectra(sim: Simulation, acc: np.ndarray, last: np.ndarray, frequency: float, steps: int):
+    """One frequency's settled DFT from its (4, num) accumulator (whole run, then the last
+    `steps`), and the share of it the last steps added, the settled constant taken out
+    (cuwave sensitivity.py:357-380). Host arithmetic in numpy complex128."""
+    whole = acc[0].astype(np.complex128) + 1j * acc[1]
+    tail = acc[2].astype(np.complex128) + 1j * acc[3]
+    z = np.exp(-2j * np.pi * frequency * sim.dt)
+    tail = tail - last * complex(np.sum(z ** np.arange(sim.N - steps, sim.N)))
+    norm = float(np.linalg.norm(whole))
+    share = float(np.linalg.norm(tail)) / norm if norm > 0.0 else 0.0
+    return settled(sim, whole, last, frequency), share
+
+
+def _dilated(sim: Simulation, region: torch.Tensor, reach: int) -> torch.Tensor:
+    """`region` grown by `reach` nodes in the max norm (a square structuring element
+    applied `reach` times), over the padded grid."""
+    x = region.to(torch.float32)[None, None]
+    pool = torch.nn.functional.max_pool2d if sim.ndim == 2 else torch.nn.functional.max_pool3d
+    return pool(x, kernel_size=2 * reach + 1, stride=1, padding=reach)[0, 0] > 0
+
+
+def spectral_sensitivity(sim: Simulation, source: Source, indicator, sensors,
+                         objective: Callable, frequencies, region=None):
+    """Cost and gradients as `sensitivity` for a cost read off the record's spectrum
+    (cuwave sensitivity.py:896-1051).
+
+    Both passes run forwards in time and keep a running DFT (CWB_OP_DFT) at the nodes
+    around `region` instead of a history: the forward run under the source, then per
+    frequency an adjoint run under a decaying pulse with the same spectral load. The
+    settled spectra of the two, paired as the triplet (z^-2, z^-1, 1) and the adjoint,
+    drive the gradient kernel (CWB_OP_GRADIENT) once for the real and once for the
+    imaginary half of the bilinear form. Exact once both runs have decayed;
+    info["decay"] says how far they have, info["fit"] how spectral the cost is.
+    """
+    require_interior(sim, sensors, "sensor")
+    require_interior(sim, source.position, "source")
+    dev = device()
+    frequencies = np.atleast_1d(np.asarray(frequencies, dtype=np.float64))
+    logical = torch.zeros(sim.Nx_padded, dtype=torch.bool, device=dev)
+    logical[tuple(slice(0, n) for n in sim.Nx)] = True
+    region = logical if region is None else as_device(region, torch.bool)
+    # the gradient at a node reads its neighbours, ghosts included, so the DFT does too
+    kept = _dilated(sim, region, sim.reach + 1) & logical
+    nodes = torch.stack(torch.nonzero(kept, as_tuple=True)).to(torch.int32)
+    lin = flatten_indices(sim, nodes)
+    num = lin.numel()
+
+    mat = sim.build_materials(indicator)
+    shot = prepare_shot(sim, mat, source.position, source.signal)
+    require_off_held_walls(sim, shot.position)
+    plan = sim.plan()
+    N = sim.N
+    material = sim.material(mat)
+    grads = sim.gradient_fields(mat)
+    grad_factors = [float(sim.np_dtype(float(f) / sim.dt**2)) for f in sim.step_factors()]
+
+    host_table = phase_table(sim, frequencies)
+    period = math.ceil(1.0 / (float(frequencies.min()) * sim.dt))
+    # the same factors again over the last period alone, for how far the run settled
+    tail = host_table.copy()
+    tail[: N - period] = 0.0
+    table = torch.as_tensor(np.concatenate((host_table, tail), axis=1), device=dev)
+    table = table.to(sim.dtype).contiguous()
+    F = len(frequencies)
+    u_hat = torch.zeros((4 * F, num), dtype=sim.dtype, device=dev)
+    U = torch.zeros((2, *sim.Nx_padded), dtype=sim.dtype, device=dev)
+    sensor_lin = flatten_indices(sim, sensors)
+    um = torch.zeros((N, sensor_lin.numel()), dtype=sim.dtype, device=dev)
+
+    # ---------------------------------------------------------------- forward pass
+    memory = pml_memory(sim, 3, dev)
+    c = nat.level(U, add=0, period=2)
+    ops = forward_ops(sim, mat, c, nat.level(U, add=1, period=2), c, shot, memory,
+                      records=[(sensor_lin, um, 1, 0, nat.STORE_NATIVE)])
+    ops.append(nat.op(nat.OP_DFT, a=c, points=nat.points(lin, table), g_mass=u_hat,
+                      columns=4 * F))
+    plan.march(ops, 0, N)
+    del memory
+    u_last = U[(N - 1) % 2].reshape(-1)[lin.long()].double().cpu().numpy()
+    u_acc = u_hat.cpu().numpy()
+    cost, dphi = _objective(objective, um)
+
+    # ----------------------------------------------------------- adjoint excitation
+    load, fit = spectral_load(sim, dphi, host_table)
+    if fit > FIT_LIMIT[sim.precision]:
+        raise ValueError(
+            f"dcost/dtraces is off the sinusoids at {frequencies} by {fit:.1e}: the cost "
+            f"is not spectral there, use sensitivity"
+        )
+    weights = sim.adjoint_weights(as_position(sim, sensors)).cpu().numpy().astype(np.float64)
+    weight = sim.excitation_weights(mat, sensor_lin)
+
+    # --------------------------------------------------------------- backward pass
+    lam_hat = torch.zeros((4, num), dtype=sim.dtype, device=dev)
+    fields = torch.zeros((4, *sim.Nx_padded), dtype=sim.dtype, device=dev)
+    flat_fields = fields.reshape(4, -1)
+    gradient = nat.op(nat.OP_GRADIENT, a=nat.level(fields, mul=0, add=0),
+                      b=nat.level(fields, mul=0, add=1), c=nat.level(fields, mul=0, add=2),
+                      d=nat.level(fields, mul=0, add=3), mat=material, g_mass=grads["mass"],
+                      g_stiff=grads["stiff"], scale=sim.adjoint_mass_factor(),
+                      factors=grad_factors)
+    decay = 0.0
+    for f, frequency in enumerate(frequencies):
+        signal = spectral_pulse(sim, frequency, load[f]) / weights
+        signal = torch.as_tensor(signal, device=dev).to(sim.dtype).contiguous()
+        U.zero_()
+        lam_hat.zero_()
+        # a fresh pml memory per run, from rest
+        eta = pml_memory(sim, 5, dev)
+        columns = [2 * f, 2 * f + 1, 2 * F + 2 * f, 2 * F + 2 * f + 1]
+        ftable = table[:, columns].contiguous()
+        ops = _adjoint_ops(sim, mat, U, eta, load=(sensor_lin, signal, weight))
+        l0 = nat.level(U, add=0, period=2)
+        ops.append(nat.op(nat.OP_REFILL, a=l0))
+        ops.append(nat.op(nat.OP_DFT, a=l0, points=nat.points(lin, ftable), g_mass=lam_hat,
+                          columns=4))
+        plan.march(ops, 0, N)
+        lam_last = U[(N - 1) % 2].reshape(-1)[lin.long()].double().cpu().numpy()
+
+        spectrum, share = spectra(sim, u_acc[columns], u_last, frequency, period)
+        adjoint_hat, adjoint_share = spectra(sim, lam_hat.cpu().numpy(), lam_last, frequency,
+                                             period)
+        decay = max(decay, share, adjoint_share)
+        # lambda^t pairs with (u^(t - 2), u^(t - 1), u^t): the triplet is z^-2, z^-1, 1
+        shift = np.exp(-2j * np.pi * frequency * sim.dt)
+        triplet = (spectrum * shift**2, spectrum * shift, spectrum)
+        # Re(a b) = Re a Re b - Im a Im b, the two halves of the bilinear form
+        for part, sign in ((np.real, 1.0), (np.imag, -1.0)):
+            values = np.stack([part(v) for v in (*triplet, sign * adjoint_hat)])
+            flat_fields[:, lin.long()] = torch.as_tensor(values.astype(sim.np_dtype), device=dev)
+            plan.march([gradient], 0, 1, graph=False)
+
+    grads = frozen(sim, sim.finalize_gradients(grads))
+    outside = ~region
+    for g in grads.values():
+        g[outside] = 0.0
+    if decay > DECAY_LIMIT:
+        warnings.warn(
+            f"the last period still adds more than {DECAY_LIMIT:.0e} of the spectrum: the "
+            f"gradient misses the tail the run cut off (info['decay'] says how much). "
+            f"Lengthen the run or damp the faces.",
+            RuntimeWarning,
+            stacklevel=2,
+        )
+    return cost, grads, um, {"decay": decay, "fit": fit}
 
 
 # ------------------------------------------------------------------- reconstruction

@@ -136,6 +136,10 @@ enum {
    * scale * (c - a)^2, g_stiff += sum_d factors[d] * (b[+s_d] - b[-s_d])^2. Replaces
    * frechet_kernel (scalar_sensitivity.cu:353-385). */
   CWB_OP_FRECHET = 11,
+  /* A running DFT at `points`: acc[k * num + j] += table[row * columns + k] * a[lin[j]]
+   * for the `columns` phase factors of table row `row` (points.record is the (rows,
+   * columns) table), acc = g_mass. Replaces dft_kernel (common.cuh:506-518). */
+  CWB_OP_DFT = 12,
 };
 
 /* op flags */
@@ -157,6 +161,7 @@ typedef struct cwb_op {
                         mass density factor */
   double factors[3]; /* GRADIENT: F_d = f_d / dt^2; SUPERPOSED: [0] the stiffness density
                         factor; FRECHET: the per-axis stiffness density factors */
+  int32_t columns;   /* DFT: phase factors per table row, rows of the accumulator */
 } cwb_op;
 
 /* Create and destroy a plan. Replaces compile_kernels (cuwave/wave.py:637-647): one

@@ -13,6 +13,8 @@ reference kernel launch) and, here in numpy, the setup and the drivers around th
     simulate               cuwave/wave.py:1071-1163 (plain step order, 1119-1127)
     sensitivity            cuwave/sensitivity.py:384-497 (fused adjoint, 468-480)
     source_sensitivity     cuwave/sensitivity.py:1054-1111
+    spectral               cuwave/sensitivity.py:295-380, 896-1051 (dft_kernel,
+                           cuwave/kernels/common.cuh:506-518, restated in numpy)
     superposition          cuwave/sensitivity.py:753-893 (superposed_kernel /
                            frechet_kernel, cuwave/kernels/scalar_sensitivity.cu:353-385,
                            600-668, restated in numpy)
@@ -482,6 +484,135 @@ class Case:
             self.cell_weights(f)
             f *= norm
         return cost, acc, um, cancellation
+
+
+    # ----------------------------------------------------------------- spectral
+    def gradient(self, u0, u1, u2, l1, g_mass, g_stiff):
+        """gradient_kernel (scalar_sensitivity.cu:303-350) with F_d = f_d / dt^2."""
+        F = np.zeros(3, self.dtype)
+        F[: self.ndim] = [self.dtype(float(f) / self.dt**2) for f in self.f[: self.ndim]]
+        self.fn("orc_gradient")(ctypes.byref(self.geo), _p(self.w), _p(F), _p(u0), _p(u1),
+                                _p(u2), _p(l1), _p(g_mass), _p(g_stiff), _p(self.stiff),
+                                _r(self.dtype, 1.0 / self.dt**2))
+
+    def adjoint_run_step(self, l0, l1, eta):
+        """The transposed step alone, pml memory included (scalar.py:318-344)."""
+        geo = ctypes.byref(self.geo)
+        self.fn("orc_adjoint")(geo, _p(self.w), _p(self.f), _r(self.dtype, self.dt), _p(l0),
+                               _p(l1), _p(l0), None, None, None, _p(self.stiff),
+                               _p(self.minv), _p(self.damping), int(self.derive),
+                               _r(self.dtype, 0.0), 0)
+        for d in self.lined():
+            self.fn("orc_pml_aux")(geo, d, _r(self.dtype, self.f[d]), _p(l1), _p(self.stiff),
+                                   _p(eta[d]), _p(self.profiles[d]))
+            self.fn("orc_pml_adjoint")(geo, _p(self.w), d, _r(self.dtype, self.f[d]), _p(l0),
+                                       None, None, _r(self.dtype, 0.0), 0, _p(self.stiff),
+                                       _p(self.minv), int(self.derive), _p(eta[d]),
+                                       _p(self.profiles[d]))
+
+    def spectral(self, N, dphi_of, frequencies, region=None, reach=None):
+        """Gradients of a spectral cost by two forward-in-time runs with running DFTs
+        (cuwave sensitivity.py:896-1051). Returns cost, {"mass", "stiff"}, traces, info."""
+        from scipy import ndimage
+
+        dt_ = self.dtype
+        freqs = np.atleast_1d(np.asarray(frequencies, np.float64))
+        logical = np.zeros(self.shape, bool)
+        logical[tuple(slice(0, n) for n in self.Nx)] = True
+        region = logical if region is None else np.asarray(region, bool)
+        square = ndimage.generate_binary_structure(self.ndim, self.ndim)
+        reach = self.R if reach is None else reach
+        kept = ndimage.binary_dilation(region, structure=square, iterations=reach + 1,
+                                       brute_force=True)
+        lin = np.flatnonzero(kept & logical).astype(np.int32)
+
+        t = np.arange(N, dtype=np.float64) * self.dt
+        phase = 2.0 * np.pi * t[:, None] * freqs[None, :]
+        host = np.empty((N, 2 * len(freqs)))
+        host[:, 0::2], host[:, 1::2] = np.cos(phase), -np.sin(phase)
+        period = int(np.ceil(1.0 / (float(freqs.min()) * self.dt)))
+        tail = host.copy()
+        tail[: N - period] = 0.0
+        table = np.concatenate((host, tail), axis=1).astype(dt_)
+        F = len(freqs)
+
+        U = np.zeros((2, *self.shape), dt_)
+        mem = self.memory()
+        um = np.zeros((N, self.sensor_lin.size), dt_)
+        u_hat = np.zeros((4 * F, lin.size), dt_)
+        for step in range(N):
+            u0, u1 = U[step % 2], U[1 - step % 2]
+            self.step(u0, u1, u0)
+            self.pml(u1, u0, mem)
+            if self.source_lin.size:
+                self.excite(u0, self.source_lin, self.source_weight, self.signal[step])
+            self.refill(u0)
+            um[step] = u0.ravel()[self.sensor_lin]
+            u_hat += table[step][:, None] * u0.ravel()[lin][None, :]
+        u_last = U[(N - 1) % 2].ravel()[lin].astype(np.float64)
+        cost, dphi = dphi_of(um)
+
+        basis = np.empty_like(host)
+        basis[:, 0::2], basis[:, 1::2] = host[:, 0::2], -host[:, 1::2]
+        target = np.asarray(dphi).astype(np.float64)
+        coef = np.linalg.lstsq(basis, target, rcond=None)[0]
+        norm = float(np.linalg.norm(target))
+        fit = float(np.linalg.norm(target - basis @ coef)) / norm if norm > 0.0 else 0.0
+        load = coef[0::2] + 1j * coef[1::2]
+        weights = self.sensor_weights(self.sensor_lin).astype(np.float64)
+        sensor_weight = self.excitation_weights(self.sensor_lin)
+
+        def settled_spectrum(acc, last, f):
+            whole = acc[0].astype(np.complex128) + 1j * acc[1]
+            late = acc[2].astype(np.complex128) + 1j * acc[3]
+            z = np.exp(-2j * np.pi * f * self.dt)
+            late = late - last * complex(np.sum(z ** np.arange(N - period, N)))
+            n = float(np.linalg.norm(whole))
+            share = float(np.linalg.norm(late)) / n if n > 0.0 else 0.0
+            return whole + last * (z**N / (1.0 - z)), share
+
+        g_mass = np.zeros(self.shape, dt_)
+        g_stiff = np.zeros(self.shape, dt_)
+        fields = np.zeros((4, *self.shape), dt_)
+        decay = 0.0
+        for k, f in enumerate(freqs):
+            sigma = 1.0 / f
+            if 8.0 * sigma > t[-1]:
+                raise ValueError("the adjoint pulse is longer than the run")
+            envelope = np.exp(-0.5 * ((t - 4.0 * sigma) / sigma) ** 2)
+            omega = 2.0 * np.pi * f
+            carriers = envelope * np.stack((np.cos(omega * t), np.sin(omega * t)))
+            spec = carriers @ np.exp(-1j * omega * t)
+            amplitudes = np.linalg.solve(np.array([spec.real, spec.imag]),
+                                         np.stack((load[k].real, load[k].imag)))
+            pulse = np.ascontiguousarray((carriers.T @ amplitudes) / weights, dt_)
+            columns = [2 * k, 2 * k + 1, 2 * F + 2 * k, 2 * F + 2 * k + 1]
+            ftable = table[:, columns]
+            P = np.zeros((2, *self.shape), dt_)
+            eta = {d: np.zeros((5, self.slab_size(d)), dt_) for d in self.lined()}
+            lam_hat = np.zeros((4, lin.size), dt_)
+            for step in range(N):
+                l0, l1 = P[step % 2], P[1 - step % 2]
+                self.adjoint_run_step(l0, l1, eta)
+                self.excite(l0, self.sensor_lin, sensor_weight, pulse[step])
+                self.refill(l0)
+                lam_hat += ftable[step][:, None] * l0.ravel()[lin][None, :]
+            lam_last = P[(N - 1) % 2].ravel()[lin].astype(np.float64)
+            spectrum, share = settled_spectrum(u_hat[columns], u_last, f)
+            adjoint_hat, adjoint_share = settled_spectrum(lam_hat, lam_last, f)
+            decay = max(decay, share, adjoint_share)
+            shift = np.exp(-2j * np.pi * f * self.dt)
+            triplet = (spectrum * shift**2, spectrum * shift, spectrum)
+            for part, sign in ((np.real, 1.0), (np.imag, -1.0)):
+                for j, value in enumerate((*triplet, sign * adjoint_hat)):
+                    fields[j].ravel()[lin] = part(value)
+                self.gradient(fields[0], fields[1], fields[2], fields[3], g_mass, g_stiff)
+        grads = {"mass": self.cell_weights(g_mass), "stiff": self.cell_weights(g_stiff)}
+        layer = self.pml_nodes()
+        for g in grads.values():
+            g[layer] = 0
+            g[~region] = 0.0
+        return cost, grads, um, {"decay": decay, "fit": fit}
 
 
 def l2(observed):

@@ -207,6 +207,54 @@ def run_superposition(case, scale):
     return out
 
 
+def spectral_coefficients(case, frequencies, dt, seed=11):
+    """(N, nsens) sinusoids at `frequencies`: the derivative of a cost linear in the record."""
+    rng = np.random.default_rng(seed)
+    N, nsens = int(case["N"]), case["sensors"].shape[1]
+    t = np.arange(N) * dt
+    coef = np.zeros((N, nsens))
+    for f in frequencies:
+        a, b = rng.standard_normal((2, nsens))
+        coef += a * np.cos(2 * np.pi * f * t)[:, None] + b * np.sin(2 * np.pi * f * t)[:, None]
+    return coef.astype(case["precision"])
+
+
+def run_spectral(case, frequencies, box=None):
+    """spectral_sensitivity of cuwave's sensitivity.py, under a cost linear in the record
+    (its derivative an input, so the whole run is deterministic) and under `intensity`."""
+    from cuwave.sensitivity import spectral_sensitivity
+    from cuwave.utils import intensity
+    from cuwave.wave import Source
+
+    sim = make_sim(case)
+    source = Source(case["source"].copy(), case["signal"].astype(sim.dtype))
+    coef = spectral_coefficients(case, frequencies, sim.dt)
+
+    def linear(traces):
+        return float(np.sum(coef * traces)), coef.copy()
+
+    region = None
+    if box is not None:
+        region = np.zeros(sim.Nx_padded, dtype=bool)
+        region[tuple(slice(lo, hi) for lo, hi in box)] = True
+    out = dict(case)
+    out.update(frequencies=np.array(frequencies), coef=coef,
+               region=region if region is not None else np.zeros(0, bool))
+    for tag, objective in (("", linear), ("i_", intensity(sim, frequencies))):
+        cost, grads, um, info = spectral_sensitivity(
+            sim, source, design(case, sim).copy(), case["sensors"].copy(), objective,
+            frequencies, region,
+        )
+        out.update({
+            f"{tag}cost": np.array(cost), f"{tag}traces": np.asarray(um),
+            f"{tag}g_mass": np.asarray(grads["mass"]), f"{tag}g_stiff": np.asarray(grads["stiff"]),
+            f"{tag}decay": np.array(info["decay"]), f"{tag}fit": np.array(info["fit"]),
+        })
+    if sim.damping is not None:
+        out["damping_field"] = np.asarray(sim.damping)
+    return out
+
+
 def run_glue(case, shot_coords, receiver_coords):
     """The shot glue of cuwave utils.py on off-node shots and receivers."""
     from cuwave.sensitivity import l2_misfit, reconstruction_sensitivity, source_sensitivity
@@ -330,6 +378,15 @@ SUPERPOSITION = [
     (dict(name="sup2d_r4_f64", ndim=2, Nx=(32, 36), order=8, N=60, precision="float64"), 1e3),
 ]
 
+SPECTRAL = [
+    (dict(name="spec2d_r4_pml", ndim=2, Nx=(44, 50), order=8, N=700, pml=(8, 1.3)),
+     (0.12, 0.15), None),
+    (dict(name="spec2d_r2_damped_region", ndim=2, Nx=(34, 38), order=4, N=700, damping=True),
+     (0.12,), ((8, 20), (10, 24))),
+    (dict(name="spec3d_r2_pml", ndim=3, Nx=(22, 20, 24), order=4, N=500, pml=(5, 1.3)),
+     (0.15,), None),
+]
+
 GLUE = [
     (dict(name="glue2d_r4", ndim=2, Nx=(40, 44), order=8, N=80),
      [(12.3, 20.7), (25.6, 9.2)], [(3.5, 2.25 + 7.3 * k) for k in range(6)]),
@@ -368,6 +425,12 @@ def main(argv=None) -> int:
         if args.only and args.only not in spec["name"]:
             continue
         out = run_superposition(build_case(**spec), scale)
+        np.savez_compressed(HERE / f"{spec['name']}.npz", **out)
+        print(spec["name"], "ok", flush=True)
+    for spec, frequencies, box in SPECTRAL:
+        if args.only and args.only not in spec["name"]:
+            continue
+        out = run_spectral(build_case(**spec), frequencies, box)
         np.savez_compressed(HERE / f"{spec['name']}.npz", **out)
         print(spec["name"], "ok", flush=True)
     for spec, shot_coords, receiver_coords in GLUE:

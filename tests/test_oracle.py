@@ -102,3 +102,32 @@ def test_superposition_cancellation_tracks_the_scale():
     loose = cases.oracle_case(fx).superposition(N, objective, scale=10.0)[3]
     tight = cases.oracle_case(fx).superposition(N, objective, scale=100.0)[3]
     assert loose / tight == pytest.approx(10.0, rel=0.03)
+
+
+SPECTRAL = sorted(p.stem for p in cases.GOLDEN.glob("spec*.npz"))
+
+
+def _spectral_case(fx):
+    case = cases.oracle_case(fx)
+    region = fx["region"] if fx["region"].size else None
+    coef = fx["coef"]
+
+    def linear(traces):
+        return float(np.sum(coef * traces)), coef.copy()
+
+    return case, region, linear
+
+
+@pytest.mark.parametrize("name", SPECTRAL)
+def test_spectral_matches_reference(name):
+    """The spectral adjoint (running DFTs, decaying adjoint pulses), bit for bit with the
+    reference's under a cost linear in the record."""
+    fx = cases.load(name)
+    case, region, linear = _spectral_case(fx)
+    cost, grads, traces, info = case.spectral(int(fx["N"]), linear, fx["frequencies"], region)
+    np.testing.assert_array_equal(traces, fx["traces"])
+    np.testing.assert_array_equal(grads["mass"], fx["g_mass"])
+    np.testing.assert_array_equal(grads["stiff"], fx["g_stiff"])
+    assert cost == pytest.approx(float(fx["cost"]), rel=1e-5)
+    assert info["decay"] == pytest.approx(float(fx["decay"]), rel=1e-6)
+    assert info["fit"] == pytest.approx(float(fx["fit"]), rel=1e-3, abs=1e-12)
