@@ -59,6 +59,8 @@ class Material(ctypes.Structure):
         ("derive_inertia", ctypes.c_int32),
         ("stiff_uniform", ctypes.c_int32),
         ("stiff_value", ctypes.c_double),
+        ("cells", ctypes.c_void_p),
+        ("cell_table", ctypes.c_void_p),
     ]
 
 

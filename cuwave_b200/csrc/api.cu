@@ -626,6 +626,17 @@ int translate(cwb_plan *p, const cwb_op &op, const size_t slot, cudaStream_t str
     int flags = 0;
     if ((rc = step_setup<T>(p, op, sp, flags, uniform)))
       return rc;
+    // a masked domain: the plain kernel with the cell radii, no pml
+    const bool masked = op.mat.cells != nullptr;
+    if (masked) {
+      if (flags & cwb::K_PML)
+        return fail(CWB_ERR_UNSUPPORTED, "a pml takes no domain mask");
+      if (!op.mat.cell_table)
+        return fail(CWB_ERR_ARG, "a masked domain needs its cell table");
+      flags |= cwb::K_CELLS;
+      sp.cells = op.mat.cells;
+      sp.ctab = static_cast<const T *>(op.mat.cell_table);
+    }
     // the superposed step: the plain kernel with the density epilogue, lossless only
     const bool super = op.kind == CWB_OP_SUPERPOSED;
     if (super) {
@@ -649,10 +660,10 @@ int translate(cwb_plan *p, const cwb_op &op, const size_t slot, cudaStream_t str
                            (op.c.stride * (long long)sizeof(T)) % 16 == 0;
     const bool roomy = ndim == 3 && g.n[0] >= 3 * R && g.n[1] >= 3 * R && g.n[2] >= 3 * R;
     const int H3 = ndim == 3 ? step3d_halo_r<T>(R) : -1;
-    const bool blocked = !super && p->tma && p->blocked3 && uniform && c_aligned && roomy && H3 >= 0 &&
+    const bool blocked = !super && !masked && p->tma && p->blocked3 && uniform && c_aligned && roomy && H3 >= 0 &&
                          tma_maps<T>(p, op, derive, sp.minv, s3, cwb::S3_BX, cwb::S3_BY, H3);
     const int Hrow = ndim == 3 ? tma_halo_nd<T, 3>(R) : tma_halo_nd<T, 2>(R);
-    const bool tma = !blocked && !super && p->tma &&
+    const bool tma = !blocked && !super && !masked && p->tma &&
                      tma_maps<T>(p, op, derive, sp.minv, tp, ndim == 3 ? cwb::TMA_BX3 : cwb::TMA_BX2,
                                  ndim == 3 ? cwb::TMA_BY3 : 1, Hrow);
     // 2D, a uniform stiffness, float, radius <= 4: the quad step, which reads u^(t-1),
@@ -660,7 +671,7 @@ int translate(cwb_plan *p, const cwb_op &op, const size_t slot, cudaStream_t str
     const auto aligned16 = [](const void *ptr, const long long stride_elems) {
       return reinterpret_cast<uintptr_t>(ptr) % 16 == 0 && (stride_elems * (long long)sizeof(T)) % 16 == 0;
     };
-    const bool quad2 = !super && ndim == 2 && p->blocked3 && uniform && step2d_built_r<T>(R) &&
+    const bool quad2 = !super && !masked && ndim == 2 && p->blocked3 && uniform && step2d_built_r<T>(R) &&
                        aligned16(op.a.base, op.a.stride) && aligned16(op.b.base, op.b.stride) &&
                        aligned16(op.c.base, op.c.stride) && (derive || aligned16(sp.minv, 0)) &&
                        g.n[0] >= 3 * R && g.n[1] >= 3 * R;
@@ -779,6 +790,10 @@ int translate(cwb_plan *p, const cwb_op &op, const size_t slot, cudaStream_t str
   }
   case CWB_OP_ADJOINT:
   case CWB_OP_GRADIENT: {
+    if (op.mat.cells)
+      return fail(CWB_ERR_UNSUPPORTED,
+                  "the transposed and gradient kernels grade no masked wall: step a masked "
+                  "domain's adjoint with CWB_OP_STEP, its own transpose");
     const bool grad_only = op.kind == CWB_OP_GRADIENT;
     cwb::AdjointParams<T> ap;
     std::memset(&ap, 0, sizeof ap);
@@ -1050,7 +1065,8 @@ bool march2d_path(cwb_plan *p, const cwb_op *ops, const int nops, const int t0, 
   const Geometry &g = p->geo;
   const int R = p->grid.radius;
   if (!p->blocked3 || g.ndim != 2 || steps < 16 || nops < 1 || nops > 1 + cwb::MARCH2_RECORDS ||
-      ops[0].kind != CWB_OP_STEP || !step2d_built_r<T>(R) || g.n[0] < 3 * R || g.n[1] < 3 * R)
+      ops[0].kind != CWB_OP_STEP || ops[0].mat.cells || !step2d_built_r<T>(R) ||
+      g.n[0] < 3 * R || g.n[1] < 3 * R)
     return false;
   for (int i = 1; i < nops; ++i)
     if (ops[i].kind != CWB_OP_RECORD || ops[i].points.num <= 0 || !ops[i].points.lin ||

@@ -22,7 +22,12 @@ enum : int {
   K_GRAD = 64,    // adjoint: accumulate g_mass, g_stiff
   K_MASS = 128,   // load: the adjoint load's inertia share
   K_SUPER = 256,  // step: add the superposition densities of the triplet (acc_mass, acc_stiff)
+  K_CELLS = 512,  // step: a masked domain, per-node cell radii in `cells`
 };
+
+// cell codes of a masked domain
+constexpr int CELL_DEEP = 1 << 30;  // every cell of the node at the full radius
+constexpr int CELL_HELD = 7;        // a cell open onto a node held at zero
 
 struct DLevel {
   char *base;

@@ -32,6 +32,9 @@ struct StepParams {
   // K_SUPER: acc_mass += ft (b - c_old)^2, acc_stiff += fs sum_d f_d (b[+s_d] - b[-s_d])^2
   T *acc_mass, *acc_stiff;
   T ft, fs;
+  // K_CELLS: per-node cell codes and the (R, R) table of OP_W rows
+  const int *cells;
+  const T *ctab;
   int *ctr;
 };
 

@@ -64,6 +64,41 @@ __device__ __forceinline__ void diffs_plain(const Tap &u, const T uc, const T *w
   }
 }
 
+// One axis of a masked node's operator: each cell at its own radius from the table
+// rows, a closed cell carrying no flux and a held one a flux onto a zero at its
+// midpoint, taps read as stored (flux_divergence_cells, cuwave/kernels/scalar.cu:86-118).
+template <typename T, int R, bool UNIF>
+__device__ __forceinline__ T cell_axis(const StepParams<T> &p, const T *__restrict__ u1,
+                                       const long long idx, const long long s, const T uc,
+                                       const T sc, const T f, const int rp, const int rm) {
+  T Dp = (T)0, Dm = (T)0;
+  if (rp == CELL_HELD) {
+    Dp = -uc * sc;
+  } else if (rp) {
+    const T sp = UNIF ? p.sconst : p.stiff[idx + s];
+    const T *w = p.ctab + (rp - 1) * R;
+    Dp = w[0] * (u1[idx + s] - uc);
+#pragma unroll
+    for (int k = 2; k <= R; ++k)
+      if (k <= rp)
+        Dp += w[k - 1] * (u1[idx + k * s] - u1[idx - (k - 1) * s]);
+    Dp *= sc * sp / (sc + sp);
+  }
+  if (rm == CELL_HELD) {
+    Dm = uc * sc;
+  } else if (rm) {
+    const T sm = UNIF ? p.sconst : p.stiff[idx - s];
+    const T *w = p.ctab + (rm - 1) * R;
+    Dm = w[0] * (uc - u1[idx - s]);
+#pragma unroll
+    for (int k = 2; k <= R; ++k)
+      if (k <= rm)
+        Dm += w[k - 1] * (u1[idx + (k - 1) * s] - u1[idx - k * s]);
+    Dm *= sc * sm / (sc + sm);
+  }
+  return f * (Dp - Dm);
+}
+
 template <int NDIM, int R, int BX, int BY>
 struct StepShape {
   static constexpr int HY = NDIM == 3 ? R : 0;
@@ -192,6 +227,21 @@ __global__ void __launch_bounds__(BX *BY) step_kernel(const StepParams<T> p) {
       else
         lap = fma_rn(p.f[2], dd[2 % NDIM], fma_rn(p.f[0], dd[0], mul_rn(p.f[1], dd[1 % NDIM])));
 
+      // a masked domain: a node outside is not stepped; a node by its wall takes each
+      // cell at its own radius, the axes summed plainly (wall_laplacian, scalar.cu:131-158)
+      bool stepped = true;
+      if (flags & K_CELLS) {
+        const int code = p.cells[idx];
+        stepped = code != 0;
+        if (stepped && !(code & CELL_DEEP)) {
+#pragma unroll
+          for (int d = 0; d < NDIM; ++d) {
+            const T term = cell_axis<T, R, UNIF>(p, u1, idx, strides[d], uc, sc, p.f[d],
+                                                 (code >> (6 * d)) & 7, (code >> (6 * d + 3)) & 7);
+            lap = d == 0 ? term : lap + term;
+          }
+        }
+      }
       const T mi = (flags & K_DERIVE) ? (T)1 / sc : p.minv[idx];
       const T old = u0[idx];
       T v;
@@ -251,29 +301,32 @@ __global__ void __launch_bounds__(BX *BY) step_kernel(const StepParams<T> p) {
       }
       if ((flags & K_REFILL) && held)
         v = (T)0;
-      if (flags & K_SUPER) {
-        // superposed_kernel (scalar_sensitivity.cu:600-668): the mass density of the
-        // triplet before, whose oldest level c still holds, and the stiffness density of
-        // this one, central differences of its middle level read as stored
-        const T dudt = uc - u2[idx];
-        p.acc_mass[idx] += p.ft * dudt * dudt;
-        T sum = (T)0;
+      // outside a masked domain nothing is written
+      if (stepped) {
+        if (flags & K_SUPER) {
+          // superposed_kernel (scalar_sensitivity.cu:600-668): the mass density of the
+          // triplet before, whose oldest level c still holds, and the stiffness density
+          // of this one, central differences of its middle level read as stored
+          const T dudt = uc - u2[idx];
+          p.acc_mass[idx] += p.ft * dudt * dudt;
+          T sum = (T)0;
 #pragma unroll
-        for (int d = 0; d < NDIM; ++d) {
-          const T gd = u1[idx + strides[d]] - u1[idx - strides[d]];
-          sum = d == 0 ? p.f[0] * gd * gd : sum + p.f[d] * gd * gd;
+          for (int d = 0; d < NDIM; ++d) {
+            const T gd = u1[idx + strides[d]] - u1[idx - strides[d]];
+            sum = d == 0 ? p.f[0] * gd * gd : sum + p.f[d] * gd * gd;
+          }
+          p.acc_stiff[idx] += p.fs * sum;
         }
-        p.acc_stiff[idx] += p.fs * sum;
-      }
-      u2[idx] = v;
-      if (flags & K_REFILL) {
+        u2[idx] = v;
+        if (flags & K_REFILL) {
 #pragma unroll
-        for (int d = 0; d < NDIM; ++d) {
-          const int a = A[d], N = g.n[d], st = strides[d];
-          if (((p.refill >> (2 * d)) & 1) && a == 2)
-            u2[idx - 2 * st] = ((g.dir >> (2 * d)) & 1) ? -v : v;
-          if (((p.refill >> (2 * d + 1)) & 1) && a == N - 3)
-            u2[idx + 2 * st] = ((g.dir >> (2 * d + 1)) & 1) ? -v : v;
+          for (int d = 0; d < NDIM; ++d) {
+            const int a = A[d], N = g.n[d], st = strides[d];
+            if (((p.refill >> (2 * d)) & 1) && a == 2)
+              u2[idx - 2 * st] = ((g.dir >> (2 * d)) & 1) ? -v : v;
+            if (((p.refill >> (2 * d + 1)) & 1) && a == N - 3)
+              u2[idx + 2 * st] = ((g.dir >> (2 * d + 1)) & 1) ? -v : v;
+          }
         }
       }
     }

@@ -13,7 +13,15 @@ import numpy as np
 import torch
 
 from . import _native as nat
-from .wave import Simulation, apply_cell_weights, as_device, mirror_ghosts, sensor_cell_weights
+from .stencils import cell_table
+from .wave import (
+    Simulation,
+    apply_cell_weights,
+    as_device,
+    domain_cells,
+    mirror_ghosts,
+    sensor_cell_weights,
+)
 
 
 @dataclass
@@ -43,6 +51,11 @@ class PressureWave(Simulation):
         first = logical.reshape(-1)[0]
         mat["uniform"] = bool((logical == first).all())
         mat["stiff_value"] = float(first)
+        mat["cells"] = mat["cell_table"] = None
+        if self.masked:
+            mat["cells"] = domain_cells(self)
+            table = cell_table(self.space_order, self.stencil).astype(self.np_dtype)
+            mat["cell_table"] = torch.as_tensor(table, device=stiff.device)
         return mat
 
     def _indicator(self, indicator) -> torch.Tensor:
@@ -71,6 +84,9 @@ class PressureWave(Simulation):
         m.derive_inertia = int(self.derive_inertia)
         m.stiff_uniform = int(mat["uniform"])
         m.stiff_value = mat["stiff_value"]
+        if mat.get("cells") is not None:
+            m.cells = mat["cells"].data_ptr()
+            m.cell_table = mat["cell_table"].data_ptr()
         return m
 
     def excitation_weights(self, mat: dict, lin_index: torch.Tensor) -> torch.Tensor:

@@ -95,6 +95,15 @@ def require_interior(sim: Simulation, position, what: str) -> None:
             )
 
 
+def require_full_domain(sim: Simulation) -> None:
+    """Raise for a masked domain: the gradient kernels grade no wall (cuwave sensitivity.py:121-127)."""
+    if sim.masked:
+        raise NotImplementedError(
+            "the gradient kernels read every cell at the full radius, where a domain closes "
+            "some; unset domain, or use source_sensitivity, which needs none"
+        )
+
+
 def frozen(sim: Simulation, grads: dict) -> dict:
     """`grads` zeroed in the pml layer, assigned so a NaN cannot survive (cuwave sensitivity.py:198-205)."""
     if sim.pml is not None:
@@ -160,6 +169,7 @@ def sensitivity(sim: Simulation, source: Source, indicator, sensors, objective: 
     """
     require_interior(sim, sensors, "sensor")
     require_interior(sim, source.position, "source")
+    require_full_domain(sim)
     dev = device()
     mat = sim.build_materials(indicator) if _mat is None else _mat
     shot = prepare_shot(sim, mat, source.position, source.signal)
@@ -222,8 +232,20 @@ def source_sensitivity(sim: Simulation, source: Source, indicator, sensors, obje
     P = torch.zeros((2, *sim.Nx_padded), dtype=sim.dtype, device=dev)
     eta = pml_memory(sim, 5, dev)
     lam = torch.zeros((sim.N, source_lin.numel()), dtype=sim.dtype, device=dev)
-    ops = _adjoint_ops(sim, mat, P, eta, load=(sensor_lin, signal, weight),
-                       probe=(source_lin, lam))
+    if sim.masked:
+        # a masked domain steps its adjoint with the graded forward step itself, its own
+        # transpose (cuwave scalar.py:322-324), the ghosts refilled as the walls read them
+        l0 = nat.level(P, add=0, period=2)
+        ops = [
+            nat.op(nat.OP_STEP, a=l0, b=nat.level(P, add=1, period=2), c=l0,
+                   mat=sim.material(mat)),
+            nat.op(nat.OP_EXCITE, a=l0, points=nat.points(sensor_lin, signal, weight=weight)),
+            nat.op(nat.OP_REFILL, a=l0),
+            nat.op(nat.OP_RECORD, a=l0, points=nat.points(source_lin, lam)),
+        ]
+    else:
+        ops = _adjoint_ops(sim, mat, P, eta, load=(sensor_lin, signal, weight),
+                           probe=(source_lin, lam))
     plan.march(ops, 0, sim.N)
     gradient = lam.flip(0) * sim.adjoint_weights(position)
     return cost, gradient.contiguous(), um, {}
@@ -271,6 +293,7 @@ def superposition_sensitivity(sim: Simulation, source: Source, indicator, sensor
     require_lossless(sim)
     require_interior(sim, sensors, "sensor")
     require_interior(sim, source.position, "source")
+    require_full_domain(sim)
     dev = device()
     mat = sim.build_materials(indicator)
     shot = prepare_shot(sim, mat, source.position, source.signal)
@@ -445,6 +468,7 @@ def spectral_sensitivity(sim: Simulation, source: Source, indicator, sensors,
     """
     require_interior(sim, sensors, "sensor")
     require_interior(sim, source.position, "source")
+    require_full_domain(sim)
     dev = device()
     frequencies = np.atleast_1d(np.asarray(frequencies, dtype=np.float64))
     logical = torch.zeros(sim.Nx_padded, dtype=torch.bool, device=dev)
@@ -658,6 +682,7 @@ def reconstruction_sensitivity(sim: Simulation, source: Source, indicator, senso
     """
     require_interior(sim, sensors, "sensor")
     require_interior(sim, source.position, "source")
+    require_full_domain(sim)
     if checkpoints is not None and checkpoints < 0:
         raise ValueError(f"checkpoints must be non-negative: {checkpoints}")
     stored = STRIP_DTYPES.get((strip_dtype, sim.precision), sim.dtype)

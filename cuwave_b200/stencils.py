@@ -85,6 +85,19 @@ def operator_row(space_order: int, stencil: str = "optimized") -> np.ndarray:
     return cell_coefficients(radius, stencil)
 
 
+def cell_table(space_order: int, stencil: str = "optimized") -> np.ndarray:
+    """(R, R) float64: row r - 1 holds OP_W(r, 1..r), the rows below R Taylor and row R
+    `stencil`, zero past r (cuwave stencils.py:186-196). A masked domain grades the cells
+    by its walls down these rows."""
+    radius = space_order // 2
+    table = np.zeros((radius, radius))
+    for r in range(1, radius + 1):
+        table[r - 1, :r] = cell_coefficients(r, stencil if r == radius else "taylor")
+    if radius == 1:
+        table[0, 0] = 1.0  # the operator weight is the literal 1 at radius 1
+    return table
+
+
 def stable_dt(
     dx: tuple[float, ...],
     wavespeed: float,

@@ -32,6 +32,9 @@ from .stencils import STENCILS, operator_row, stable_dt  # noqa: F401  (re-expor
 
 # a record of this dtype holds bfloat16: the high half of each float32
 BFLOAT16 = torch.uint16
+# cell codes of a masked domain (cuwave wave.py:662-663)
+CELL_DEEP = 1 << 30  # a node whose cells all take the full radius
+CELL_HELD = 7  # the radius code of a cell open onto a node held at zero
 
 
 def padded_shape(Nx: tuple[int, ...]) -> tuple[int, ...]:
@@ -67,8 +70,9 @@ class Simulation:
     """Grid, timestepping and configuration of the scalar step (cuwave wave.py:479-630).
 
     `threads` is accepted for compatibility with the reference's signature; the native
-    kernels choose their own launch shapes. `domain` and `dirichlet` masks are not
-    stepped by this build, and `devices` names one GPU at most.
+    kernels choose their own launch shapes. `domain` (the nodes stepped) and `dirichlet`
+    (the nodes held at zero) are boolean masks over the padded grid, graded at their
+    walls (`domain_cells`); `devices` names one GPU at most.
     """
 
     Nx: tuple[int, ...]
@@ -111,8 +115,12 @@ class Simulation:
             raise ValueError(f"unknown stencil {self.stencil!r}, expected one of {STENCILS}")
         if self.ndim not in (2, 3):
             raise NotImplementedError("the B200 step is 2D or 3D")
-        if self.domain is not None or self.dirichlet is not None:
-            raise NotImplementedError("domain and dirichlet masks are not stepped by this build")
+        for name in ("domain", "dirichlet"):
+            mask = getattr(self, name)
+            if mask is not None and tuple(mask.shape) != self.Nx_padded:
+                raise ValueError(f"{name} mask {tuple(mask.shape)} != {self.Nx_padded}")
+        if self.masked and self.space_order // 2 >= CELL_HELD:
+            raise ValueError(f"space_order {self.space_order} overflows the 3-bit cell radius")
         if self.devices is not None and len(tuple(self.devices)) > 1:
             raise NotImplementedError("the scalar path runs on one GPU: devices=(0,)")
         self.comp_stride = int(np.prod(self.Nx_padded))
@@ -198,6 +206,86 @@ def mirror_ghosts(sim: Simulation, field: torch.Tensor) -> torch.Tensor:
             src[d] = mirror
             field[tuple(dst)] = field[tuple(src)]
     return field
+
+
+def stepped_nodes(sim: Simulation) -> torch.Tensor:
+    """The nodes the step updates: `domain` (all by default) less `dirichlet` (cuwave wave.py:665-672)."""
+    stepped = torch.ones(sim.Nx_padded, dtype=torch.bool, device=device())
+    if sim.domain is not None:
+        stepped &= as_device(sim.domain, torch.bool)
+    if sim.dirichlet is not None:
+        stepped &= ~as_device(sim.dirichlet, torch.bool)
+    return stepped
+
+
+def domain_cells(sim: Simulation) -> torch.Tensor:
+    """Per node of a masked grid, the radii of its two cells along each axis, packed
+    (cuwave wave.py:675-726).
+
+    A cell's taps may only reach stepped nodes (ghosts count as stepped), so each radius
+    is capped by the run of stepped nodes on either side and by the box wall; a cell
+    leaving the stepped set is closed (radius 0) unless the node across is held, which
+    opens it onto a zero at its midpoint (CELL_HELD). The code is 0 for a node not
+    stepped, CELL_DEEP where every radius is the full one, else
+    (r_plus | r_minus << 3) << 6 d summed over the axes.
+    """
+    R = sim.radius
+    dev = device()
+    shape = sim.Nx_padded
+    interior = tuple(slice(1, n - 1) for n in sim.Nx)
+    inside = torch.ones(shape, dtype=torch.bool, device=dev)
+    inside[interior] = stepped_nodes(sim)[interior]
+    held = torch.zeros(shape, dtype=torch.bool, device=dev)
+    if sim.dirichlet is not None:
+        held[interior] = as_device(sim.dirichlet, torch.bool)[interior]
+
+    def shifted(mask, d, k, fill):
+        """mask[i + k] along axis d, `fill` past the array."""
+        out = torch.full_like(mask, fill)
+        n = shape[d]
+        if abs(k) >= n:
+            return out
+        dst = [slice(None)] * sim.ndim
+        src = [slice(None)] * sim.ndim
+        dst[d] = slice(0, n - k) if k >= 0 else slice(-k, n)
+        src[d] = slice(k, n) if k >= 0 else slice(0, n + k)
+        out[tuple(dst)] = mask[tuple(src)]
+        return out
+
+    code = torch.zeros(shape, dtype=torch.int32, device=dev)
+    deep = inside.clone()
+    for d in range(sim.ndim):
+        view = [1] * sim.ndim
+        view[d] = -1
+        a = torch.arange(shape[d], device=dev, dtype=torch.int32).reshape(view)
+        wall = torch.clamp(torch.minimum(a, sim.Nx[d] - 1 - a), max=R)
+
+        def run(sign):
+            count = torch.zeros(shape, dtype=torch.int32, device=dev)
+            on = torch.ones_like(inside)
+            for k in range(1, R + 1):
+                on &= shifted(inside, d, sign * k, True)
+                count += (on & (k <= wall)).to(torch.int32)
+            return count
+
+        up, down = run(1), run(-1)
+        rp = torch.minimum(wall, torch.minimum(1 + down, up))
+        rm = torch.minimum(wall, torch.minimum(down, 1 + up))
+        rp = torch.where((rp == 0) & shifted(held, d, 1, False), CELL_HELD, rp)
+        rm = torch.where((rm == 0) & shifted(held, d, -1, False), CELL_HELD, rm)
+        code |= (rp | (rm << 3)) << (6 * d)
+        deep &= (rp == wall) & (rm == wall)
+    code = torch.where(deep, CELL_DEEP, code)
+    return torch.where(inside, code, 0).to(torch.int32).contiguous()
+
+
+def require_stepped(sim: Simulation, position: torch.Tensor, what: str) -> None:
+    """Raise for a point on a node a masked step never updates (cuwave wave.py:964-967)."""
+    if not sim.masked or position.numel() == 0:
+        return
+    stepped = stepped_nodes(sim)
+    if not bool(stepped[tuple(grid_rows(sim, position).long())].all()):
+        raise ValueError(f"a {what} reaches a node that is never stepped")
 
 
 def grid_coords(Nx, dx, dtype=torch.float64) -> list[torch.Tensor]:
@@ -327,7 +415,7 @@ def forward_ops(sim: Simulation, mat: dict, a: nat.Level, b: nat.Level, c: nat.L
     store) tuples written after the refill.
     """
     material = sim.material(mat)
-    folded = fold and replay is None and (shot is None or shot.foldable)
+    folded = fold and replay is None and (shot is None or shot.foldable) and not sim.masked
     flags = (nat.PML if sim.pml is not None else 0)
     mul, add = source_row
     src = shot.points(row_add=add, row_mul=mul) if shot is not None else nat.points(None, None)
@@ -371,6 +459,7 @@ def simulate(sim: Simulation, source: Source, indicator, sensors=None, record_ev
     mat = sim.build_materials(indicator) if _mat is None else _mat
     shot = prepare_shot(sim, mat, source.position, source.signal)
     require_off_held_walls(sim, shot.position)
+    require_stepped(sim, shot.position, "source")
     if shot.signal.shape[0] < sim.N:
         raise ValueError(f"the signal has {shot.signal.shape[0]} rows for {sim.N} steps")
     plan = sim.plan()
@@ -379,6 +468,7 @@ def simulate(sim: Simulation, source: Source, indicator, sensors=None, record_ev
     records = []
     um = None
     if sensors is not None:
+        require_stepped(sim, as_position(sim, sensors), "sensor")
         sensor_lin = flatten_indices(sim, sensors)
         um = torch.zeros((sim.N, sensor_lin.numel()), dtype=sim.dtype, device=dev)
         records.append((sensor_lin, um, 1, 0, nat.STORE_NATIVE))

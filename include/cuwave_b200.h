@@ -74,6 +74,13 @@ typedef struct cwb_material {
   int32_t derive_inertia;  /* 1 / m = 1 / k (ScalarWave) */
   int32_t stiff_uniform;   /* k is stiff_value everywhere the step reads it */
   double stiff_value;
+  /* A masked domain, or NULL: per node of the padded grid 0 (not stepped), 1 << 30
+   * (every cell at the full radius), else the radii of its two cells along each axis d,
+   * (r_plus | r_minus << 3) << 6 d, 7 for a cell open onto a held node. Replaces the
+   * cells of cuwave/wave.py:675-726 read by fd_kernel under USE_DOMAIN (scalar.cu:86-158,
+   * 434-452). */
+  const int32_t *cells;
+  const void *cell_table;  /* with cells: (R, R) OP_W(r, k) at [r - 1][k - 1] */
 } cwb_material;
 
 /* A transfer list: `num` flat node indices, a per-point weight and a (rows, num)

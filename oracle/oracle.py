@@ -158,6 +158,60 @@ def pml_profiles(Nx, dx, dt, widths, width, wavespeed, reflection, frequency, dt
     return out
 
 
+def cell_table(radius: int, stencil: str, dtype) -> np.ndarray:
+    """(R, R) rows OP_W(r, 1..r): Taylor below R, `stencil` at R (cuwave stencils.py:186-196)."""
+    table = np.zeros((radius, radius))
+    for r in range(1, radius + 1):
+        table[r - 1, :r] = cell_coefficients(r, stencil if r == radius else "taylor")
+    if radius == 1:
+        table[0, 0] = 1.0  # OP_W is the literal 1 at radius 1 (common.cuh:25-27)
+    return table.astype(dtype)
+
+
+def domain_cells(Nx, R, stepped, held=None):
+    """Cell codes of a masked domain over the padded grid (cuwave wave.py:675-726): 0 not
+    stepped, 1 << 30 all cells at the full radius, else the packed radii per axis."""
+    shape = padded(Nx)
+    ndim = len(Nx)
+    interior = tuple(slice(1, n - 1) for n in Nx)
+    inside = np.ones(shape, bool)
+    inside[interior] = np.asarray(stepped, bool)[interior]
+    hold = np.zeros(shape, bool)
+    if held is not None:
+        hold[interior] = np.asarray(held, bool)[interior]
+
+    def moved(mask, d, k, fill):
+        padded_ = np.pad(mask, R, constant_values=fill)
+        window = [slice(R, R + n) for n in shape]
+        window[d] = slice(R + k, R + k + shape[d])
+        return padded_[tuple(window)]
+
+    code = np.zeros(shape, np.int64)
+    deep = inside.copy()
+    for d in range(ndim):
+        view = [1] * ndim
+        view[d] = -1
+        a = np.arange(shape[d]).reshape(view)
+        wall = np.minimum(R, np.minimum(a, Nx[d] - 1 - a))
+        runs = []
+        for sign in (1, -1):
+            count = np.zeros(shape, np.int64)
+            on = np.ones(shape, bool)
+            for k in range(1, R + 1):
+                on &= moved(inside, d, sign * k, True)
+                count += on & (k <= wall)
+            runs.append(count)
+        up, down = runs
+        rp = np.minimum(wall, np.minimum(1 + down, up))
+        rm = np.minimum(wall, np.minimum(down, 1 + up))
+        rp = np.where((rp == 0) & moved(hold, d, 1, False), 7, rp)
+        rm = np.where((rm == 0) & moved(hold, d, -1, False), 7, rm)
+        code |= (rp | rm << 3) << (6 * d)
+        deep &= (rp == wall) & (rm == wall)
+    code = np.where(deep, 1 << 30, code)
+    return np.where(inside, code, 0).astype(np.int32)
+
+
 def acoustic_materials(Nx, indicator, rho1, rho2, kappa1, kappa2, dtype):
     """(stiff, minv) of AcousticWave, ghosts mirrored (cuwave scalar.py:927-934, 407-415)."""
     ind = np.asarray(indicator, dtype=dtype)
@@ -188,6 +242,8 @@ class Case:
     source_weight: np.ndarray | None = None
     signal: np.ndarray | None = None   # (N, nsrc)
     sensor_lin: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int32))
+    cells: np.ndarray | None = None    # a masked domain's cell codes (domain_cells)
+    table: np.ndarray | None = None    # with cells: (R, R) OP_W rows (cell_table)
 
     def __post_init__(self):
         self.ndim = len(self.Nx)
@@ -236,6 +292,15 @@ class Case:
 
     # ------------------------------------------------------------ single launches
     def step(self, u0, u1, u2):
+        if self.cells is not None:
+            # held in locals so the buffers outlive the call
+            table = np.ascontiguousarray(self.table, self.dtype)
+            cells = np.ascontiguousarray(self.cells, np.int32)
+            self.fn("orc_step_cells")(
+                ctypes.byref(self.geo), _p(self.w), _p(self.f), _r(self.dtype, self.dt),
+                _p(u0), _p(u1), _p(u2), _p(self.stiff), _p(self.minv), _p(self.damping),
+                int(self.derive), _p(cells), _p(table))
+            return
         self.fn("orc_step")(ctypes.byref(self.geo), _p(self.w), _p(self.f), _r(self.dtype, self.dt),
                             _p(u0), _p(u1), _p(u2), _p(self.stiff), _p(self.minv),
                             _p(self.damping), int(self.derive))
@@ -369,6 +434,16 @@ class Case:
         eta = {d: np.zeros((3, self.slab_size(d)), self.dtype) for d in self.lined()}
         lam = np.zeros((N, self.source_lin.size), self.dtype)
         geo = ctypes.byref(self.geo)
+        if self.cells is not None:
+            # a masked domain is stepped backwards by its own graded step (scalar.py:322-324)
+            for m in range(N):
+                l0, l1 = P[m % 2], P[1 - m % 2]
+                self.step(l0, l1, l0)
+                self.excite(l0, self.sensor_lin, weight, signal[m])
+                self.refill(l0)
+                lam[m] = l0.ravel()[self.source_lin]
+            gradient = lam[::-1] * self.sensor_weights(self.source_lin)
+            return cost, np.ascontiguousarray(gradient), um
         for m in range(N):
             l0, l1 = P[m % 2], P[1 - m % 2]
             self.fn("orc_adjoint")(geo, _p(self.w), _p(self.f), _r(self.dtype, self.dt), _p(l0),

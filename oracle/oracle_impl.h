@@ -149,6 +149,86 @@ void FN(orc_step)(const orc_geo *g, const REAL *w, const REAL *f, REAL dt, const
   }
 }
 
+/* flux_divergence_cells (scalar.cu:86-118): one axis with each cell at its own radius,
+ * taps as stored; table row r - 1 holds OP_W(r, 1..r), 7 marks a cell onto a held node */
+static REAL FN(cells_axis)(const orc_geo *g, const REAL *table, const REAL *u1,
+                           const REAL *stiff, long idx, long s, REAL uc, REAL sc, REAL f,
+                           int rp, int rm) {
+  const int R = g->R;
+  REAL Dp = 0, Dm = 0;
+  if (rp == 7) {
+    Dp = -uc * sc;
+  } else if (rp) {
+    const REAL sp = stiff[idx + s];
+    const REAL *w = table + (rp - 1) * R;
+    Dp = w[0] * (u1[idx + s] - uc);
+    for (int k = 2; k <= rp; ++k)
+      Dp += w[k - 1] * (u1[idx + k * s] - u1[idx - (k - 1) * s]);
+    Dp *= sc * sp / (sc + sp);
+  }
+  if (rm == 7) {
+    Dm = uc * sc;
+  } else if (rm) {
+    const REAL sm = stiff[idx - s];
+    const REAL *w = table + (rm - 1) * R;
+    Dm = w[0] * (uc - u1[idx - s]);
+    for (int k = 2; k <= rm; ++k)
+      Dm += w[k - 1] * (u1[idx + (k - 1) * s] - u1[idx - k * s]);
+    Dm *= sc * sm / (sc + sm);
+  }
+  return f * (Dp - Dm);
+}
+
+/* fd_kernel under USE_DOMAIN (scalar.cu:434-452): a node of code 0 is not written, a
+ * node by a wall (code without bit 30) takes wall_laplacian (scalar.cu:131-158) */
+void FN(orc_step_cells)(const orc_geo *g, const REAL *w, const REAL *f, REAL dt,
+                        const REAL *u0, const REAL *u1, REAL *u2, const REAL *stiff,
+                        const REAL *minv, const REAL *damping, int derive, const int *cells,
+                        const REAL *table) {
+  const long total = FN(total)(g);
+#pragma omp parallel for schedule(static)
+  for (long idx = 0; idx < total; ++idx) {
+    int A[3];
+    FN(coords)(g, idx, A);
+    if (!FN(interior)(g, A))
+      continue;
+    const int code = cells[idx];
+    if (!code)
+      continue;
+    const REAL uc = u1[idx], sc = stiff[idx];
+    REAL lap;
+    if (g->ndim == 2) {
+      const REAL d0 = FN(flux_axis)(g, w, u1, stiff, idx, 0, A[0], uc, sc);
+      const REAL d1 = FN(flux_axis)(g, w, u1, stiff, idx, 1, A[1], uc, sc);
+      lap = g->R == 1 ? FN(fma_r)(f[0], d0, f[1] * d1) : FN(fma_r)(f[1], d1, f[0] * d0);
+    } else {
+      const REAL d0 = FN(flux_axis)(g, w, u1, stiff, idx, 0, A[0], uc, sc);
+      const REAL d1 = FN(flux_axis)(g, w, u1, stiff, idx, 1, A[1], uc, sc);
+      const REAL d2 = FN(flux_axis)(g, w, u1, stiff, idx, 2, A[2], uc, sc);
+      lap = FN(fma_r)(f[2], d2, FN(fma_r)(f[0], d0, f[1] * d1));
+    }
+    if (!(code >> 30)) {
+      lap = 0;
+      for (int d = 0; d < g->ndim; ++d) {
+        const REAL term = FN(cells_axis)(g, table, u1, stiff, idx, g->s[d], uc, sc, f[d],
+                                         (code >> (6 * d)) & 7, (code >> (6 * d + 3)) & 7);
+        lap = d == 0 ? term : lap + term;
+      }
+    }
+    const REAL mi = derive ? (REAL)1 / sc : minv[idx];
+    REAL v;
+    if (damping) {
+      const REAL beta = (REAL)0.5 * mi * damping[idx] * dt;
+      v = ((REAL)2 * uc - u0[idx] * ((REAL)1 - beta) + mi * lap) / ((REAL)1 + beta);
+    } else {
+      v = -u0[idx] + (REAL)2 * uc + mi * lap;
+    }
+    if (FN(held_node)(g, A))
+      v = 0;
+    u2[idx] = v;
+  }
+}
+
 /* slab row of node a on a lined axis, -1 off the slab */
 static inline int FN(slab_row)(int a, int N, int lo, int hi) {
   if (lo && a >= 1 && a <= lo)

@@ -255,6 +255,59 @@ def run_spectral(case, frequencies, box=None):
     return out
 
 
+def masks(case, kind):
+    """(domain, dirichlet) boolean masks over the padded grid: a disk or ball, an obstacle
+    held at zero inside it, or a held row across the box."""
+    from cuwave.wave import padded_shape
+
+    Nx = tuple(int(n) for n in case["Nx"])
+    shape = padded_shape(Nx)
+    grids = np.meshgrid(*[np.arange(n, dtype=np.float64) for n in shape], indexing="ij")
+    centre = [(n - 1) / 2 for n in Nx]
+    r2 = sum((g - c) ** 2 for g, c in zip(grids, centre))
+    radius = 0.45 * min(Nx)
+    domain = dirichlet = None
+    if kind in ("disk", "obstacle"):
+        domain = r2 <= radius**2
+    if kind == "obstacle":
+        off = [c + 0.3 * radius * (1 if d == 0 else -1) for d, c in enumerate(centre)]
+        dirichlet = sum((g - c) ** 2 for g, c in zip(grids, off)) <= (0.25 * radius) ** 2
+    if kind == "row":
+        dirichlet = np.zeros(shape, bool)
+        dirichlet[int(0.7 * Nx[0])] = True
+    return domain, dirichlet
+
+
+def run_masked(case, kind):
+    """simulate and source_sensitivity of cuwave on a masked domain."""
+    from cuwave.sensitivity import l2_misfit, source_sensitivity
+    from cuwave.wave import Source, domain_cells, simulate
+
+    sim = make_sim(case)
+    domain, dirichlet = masks(case, kind)
+    sim.domain, sim.dirichlet = domain, dirichlet
+    Nx = tuple(int(n) for n in case["Nx"])
+    centre = [n // 2 for n in Nx]
+    src = np.array([[c] for c in centre], np.int32)
+    offsets = [(-3, 2, -4), (1, -1, 2), (-2, 3, 4)]
+    offsets = offsets[:1] + offsets[1:-1][: len(Nx) - 2] + offsets[-1:]
+    sens = np.array([[c + o for o in offs] for c, offs in zip(centre, offsets)], np.int32)
+    source = Source(src, case["signal"].astype(sim.dtype))
+    field, um = simulate(sim, source, design(case, sim).copy(), sens.copy())
+    observed = np.asarray(um) * sim.dtype(0.7)
+    cost, gradient, _, _ = source_sensitivity(
+        sim, source, design(case, sim).copy(), sens.copy(), l2_misfit(observed))
+    out = dict(case)
+    out.update(
+        kind=kind, domain=domain if domain is not None else np.zeros(0, bool),
+        dirichlet_mask=dirichlet if dirichlet is not None else np.zeros(0, bool),
+        source=src, sensors=sens, field=np.asarray(field), traces=np.asarray(um),
+        observed=observed, source_cost=np.array(cost), source_gradient=np.asarray(gradient),
+        cells=np.asarray(domain_cells(sim)),
+    )
+    return out
+
+
 def run_glue(case, shot_coords, receiver_coords):
     """The shot glue of cuwave utils.py on off-node shots and receivers."""
     from cuwave.sensitivity import l2_misfit, reconstruction_sensitivity, source_sensitivity
@@ -387,6 +440,17 @@ SPECTRAL = [
      (0.15,), None),
 ]
 
+MASKED = [
+    (dict(name="mask2d_disk_r2", ndim=2, Nx=(40, 44), order=4, N=120), "disk"),
+    (dict(name="mask2d_obstacle_r4_mixed", ndim=2, Nx=(42, 40), order=8, N=110, faces="mixed"),
+     "obstacle"),
+    (dict(name="mask2d_row_r1_f64", ndim=2, Nx=(36, 34), order=2, N=100, precision="float64"),
+     "row"),
+    (dict(name="mask2d_obstacle_r6_scalar", ndim=2, Nx=(44, 46), order=12, N=90, scalar=True,
+          stencil="taylor"), "obstacle"),
+    (dict(name="mask3d_obstacle_r2", ndim=3, Nx=(22, 24, 26), order=4, N=50), "obstacle"),
+]
+
 GLUE = [
     (dict(name="glue2d_r4", ndim=2, Nx=(40, 44), order=8, N=80),
      [(12.3, 20.7), (25.6, 9.2)], [(3.5, 2.25 + 7.3 * k) for k in range(6)]),
@@ -431,6 +495,12 @@ def main(argv=None) -> int:
         if args.only and args.only not in spec["name"]:
             continue
         out = run_spectral(build_case(**spec), frequencies, box)
+        np.savez_compressed(HERE / f"{spec['name']}.npz", **out)
+        print(spec["name"], "ok", flush=True)
+    for spec, kind in MASKED:
+        if args.only and args.only not in spec["name"]:
+            continue
+        out = run_masked(build_case(**spec), kind)
         np.savez_compressed(HERE / f"{spec['name']}.npz", **out)
         print(spec["name"], "ok", flush=True)
     for spec, shot_coords, receiver_coords in GLUE:

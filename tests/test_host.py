@@ -94,8 +94,13 @@ def test_simulation_validation():
         AcousticWave(**base, space_order=3)
     with pytest.raises(ValueError):
         AcousticWave(**base, stencil="nope")
-    with pytest.raises(NotImplementedError):
-        AcousticWave(**base, domain=np.ones((20, 32), bool))
+    with pytest.raises(ValueError):
+        AcousticWave(**base, domain=np.ones((20, 20), bool))  # not over the padded grid
+    with pytest.raises(ValueError):
+        AcousticWave(**base, domain=np.ones((20, 32), bool), pml=Pml(width=4, wavespeed=1.0))
+    with pytest.raises(ValueError):
+        AcousticWave(**{**base, "Nx": (30, 30)}, domain=np.ones((30, 32), bool), space_order=14)
+    assert AcousticWave(**base, domain=np.ones((20, 32), bool)).masked
     with pytest.raises(NotImplementedError):
         AcousticWave(**base, devices=(0, 1))
     with pytest.raises(ValueError):

@@ -131,3 +131,38 @@ def test_spectral_matches_reference(name):
     assert cost == pytest.approx(float(fx["cost"]), rel=1e-5)
     assert info["decay"] == pytest.approx(float(fx["decay"]), rel=1e-6)
     assert info["fit"] == pytest.approx(float(fx["fit"]), rel=1e-3, abs=1e-12)
+
+
+MASKED = sorted(p.stem for p in cases.GOLDEN.glob("mask*.npz"))
+
+
+def masked_oracle_case(fx):
+    """The oracle Case of a masked fixture: its cell codes and table rows."""
+    case = cases.oracle_case(fx)
+    Nx = tuple(int(n) for n in fx["Nx"])
+    stepped = np.ones(o.padded(Nx), bool)
+    if fx["domain"].size:
+        stepped &= fx["domain"]
+    held = fx["dirichlet_mask"] if fx["dirichlet_mask"].size else None
+    if held is not None:
+        stepped &= ~held
+    case.cells = o.domain_cells(Nx, case.R, stepped, held)
+    case.table = o.cell_table(case.R, str(fx["stencil"]), case.dtype)
+    return case
+
+
+@pytest.mark.parametrize("name", MASKED)
+def test_masked_domain_matches_reference(name):
+    """A domain mask graded at its walls and held obstacles, bit for bit: the cell codes,
+    the forward run and the signal gradient stepped back by the graded step itself."""
+    fx = cases.load(name)
+    case = masked_oracle_case(fx)
+    Nx = tuple(int(n) for n in fx["Nx"])
+    interior = tuple(slice(1, n - 1) for n in Nx)
+    np.testing.assert_array_equal(case.cells[interior], fx["cells"][interior])
+    field, traces = case.forward(int(fx["N"]))
+    np.testing.assert_array_equal(field[tuple(slice(0, n) for n in Nx)], fx["field"])
+    np.testing.assert_array_equal(traces, fx["traces"])
+    cost, gradient, _ = case.source_sensitivity(int(fx["N"]), o.l2(fx["observed"]))
+    np.testing.assert_array_equal(gradient, fx["source_gradient"])
+    assert cost == pytest.approx(float(fx["source_cost"]), rel=1e-5)
