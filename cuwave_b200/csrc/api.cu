@@ -492,92 +492,83 @@ void fill_weights(const cwb_plan *p, T *w, T *f) {
 }
 
 template <typename T>
-cudaError_t pml_step_r(const cwb::PmlStepParams<T> &p, const int ndim, const int R,
-                       const bool u, const dim3 grid, cudaStream_t s) {
-  switch (ndim * 16 + R) {
-#define CWB_PML_CASE(D, RR) \
-  case D * 16 + RR: return cwb::pml_step_unit<T, D, RR>(p, u, grid, s);
-    CWB_PML_CASE(2, 1) CWB_PML_CASE(2, 2) CWB_PML_CASE(2, 3) CWB_PML_CASE(2, 4)
-    CWB_PML_CASE(2, 5) CWB_PML_CASE(2, 6) CWB_PML_CASE(2, 7) CWB_PML_CASE(2, 8)
-    CWB_PML_CASE(3, 1) CWB_PML_CASE(3, 2) CWB_PML_CASE(3, 3) CWB_PML_CASE(3, 4)
-    CWB_PML_CASE(3, 5) CWB_PML_CASE(3, 6) CWB_PML_CASE(3, 7) CWB_PML_CASE(3, 8)
-#undef CWB_PML_CASE
+cudaError_t pml3d_r(const cwb::Pml3Params<T> &p, const int R, const int axis, const dim3 grid,
+                    cudaStream_t s) {
+  switch (R) {
+  case 1: return cwb::pml3d_unit<T, 1>(p, axis, grid, s);
+  case 2: return cwb::pml3d_unit<T, 2>(p, axis, grid, s);
+  case 3: return cwb::pml3d_unit<T, 3>(p, axis, grid, s);
+  case 4: return cwb::pml3d_unit<T, 4>(p, axis, grid, s);
+  case 5: return cwb::pml3d_unit<T, 5>(p, axis, grid, s);
+  case 6: return cwb::pml3d_unit<T, 6>(p, axis, grid, s);
+  case 7: return cwb::pml3d_unit<T, 7>(p, axis, grid, s);
+  case 8: return cwb::pml3d_unit<T, 8>(p, axis, grid, s);
   }
   return cudaErrorInvalidValue;
 }
 
-// The pml launch of axes 1 and 2 after the blocked step (which advanced axis 0's memory in
-// its march): their slab union cut into disjoint boxes (axis-1 slabs over every interior
-// plane; axis-2 slabs over the axis-1 interior), so each slab node is visited once. The
-// launch's threads count quads of four fast-axis nodes.
+// The pml launches of axes 1 and 2 after the blocked 3D step (which advanced axis 0's
+// memory in its march): a launch per lined axis, axis 1 first, so a node in both slabs
+// takes its shares in the reference's order.
 template <typename T>
-void pml_launch(const cwb_plan *p, const cwb::StepParams<T> &sp, const bool uniform,
-                std::vector<Launch> &out) {
+int pml_launch(const cwb_plan *p, const cwb::StepParams<T> &sp, std::vector<Launch> &out) {
   const Geometry &g = p->geo;
-  const int nd = g.ndim, R = p->grid.radius;
-  cwb::PmlStepParams<T> pp;
+  const int R = p->grid.radius;
+  if (g.ndim != 3)
+    return fail(CWB_ERR_UNSUPPORTED, "the pml slab launches step 3D grids");
+  cwb::Pml3Params<T> pp;
   std::memset(&pp, 0, sizeof pp);
   pp.g = g;
   for (int k = 0; k < cwb::MAXR; ++k)
     pp.w[k] = sp.w[k];
-  for (int d = 0; d < 3; ++d) {
-    pp.f[d] = sp.f[d];
-    pp.prof[d] = sp.prof[d];
-    pp.aux[d] = sp.aux[d];
-    pp.auxrow[d] = sp.auxrow[d];
-  }
   pp.gconst = sp.gconst;
   pp.sconst = sp.sconst;
   pp.flags = sp.flags & cwb::K_DERIVE;
   pp.u1 = sp.u1;
   pp.u2 = sp.u2;
-  pp.stiff = sp.stiff;
   pp.minv = sp.minv;
   pp.ctr = sp.ctr;
-  // interior range of each axis, narrowed past the slabs of the axes before it (axis 0,
-  // whose memory the blocked step advances in its march, stays whole)
-  int first[3], count[3];
-  for (int d = 0; d < nd; ++d) {
-    first[d] = 1;
-    count[d] = g.n[d] - 2;
+  if (g.lo[1] + g.hi[1] > 0) {
+    cwb::Pml3Params<T> q1 = pp;
+    q1.f = sp.f[1];
+    q1.prof = sp.prof[1];
+    q1.aux = sp.aux[1];
+    q1.auxrow = sp.auxrow[1];
+    const int quads = (g.n[2] - 2) / 4 + 1;
+    const dim3 grid((quads + cwb::PML1_THREADS - 1) / cwb::PML1_THREADS, g.lo[1] + g.hi[1],
+                    g.n[0] - 2);
+    out.push_back([q1, R, grid](cudaStream_t s, bool adv) {
+      cwb::Pml3Params<T> q = q1;
+      if (adv)
+        q.flags |= cwb::K_ADV;
+      return pml3d_r<T>(q, R, 1, grid, s);
+    });
   }
-  long long total = 0;
-  for (int d = 1; d < nd; ++d) {
-    for (int side = 0; side < 2; ++side) {
-      const int w = side ? g.hi[d] : g.lo[d];
-      if (w <= 0)
-        continue;
-      for (int e = 0; e < nd; ++e) {
-        pp.org[pp.nbox][e] = first[e];
-        pp.ext[pp.nbox][e] = count[e];
-      }
-      pp.org[pp.nbox][d] = side ? g.n[d] - 1 - g.hi[d] : 1;
-      pp.ext[pp.nbox][d] = w;
-      bool empty = false;
-      for (int e = 0; e < nd; ++e)
-        empty |= pp.ext[pp.nbox][e] <= 0;
-      if (empty)
-        continue;
-      // a thread per quad of four fast-axis nodes (16-byte aligned) of one row
-      const int F = nd - 1, x0 = pp.org[pp.nbox][F], x1 = x0 + pp.ext[pp.nbox][F] - 1;
-      long long threads = (x1 >> 2) - (x0 >> 2) + 1;
-      for (int e = 0; e < F; ++e)
-        threads *= pp.ext[pp.nbox][e];
-      total += threads;
-      pp.end[pp.nbox++] = total;
-    }
-    first[d] = 1 + g.lo[d];
-    count[d] = g.n[d] - 2 - g.lo[d] - g.hi[d];
+  if (g.lo[2] + g.hi[2] > 0) {
+    cwb::Pml3Params<T> q2 = pp;
+    q2.f = sp.f[2];
+    q2.prof = sp.prof[2];
+    q2.aux = sp.aux[2];
+    q2.auxrow = sp.auxrow[2];
+    const int NF = g.n[2];
+    // quads of four holding a slab node: x in 1 .. lo on the low side, NF - 1 - hi ..
+    // NF - 2 on the high side
+    q2.nlo = g.lo[2] > 0 ? g.lo[2] / 4 + 1 : 0;
+    q2.xhi = (NF - 1 - g.hi[2]) / 4 * 4;
+    q2.nhi = g.hi[2] > 0 ? (NF - 2) / 4 - (NF - 1 - g.hi[2]) / 4 + 1 : 0;
+    const int nq = q2.nlo + q2.nhi;
+    if (nq > cwb::PML2_THREADS)
+      return fail(CWB_ERR_UNSUPPORTED, "pml slabs wider than 500 nodes along axis 2");
+    const int rows = cwb::PML2_THREADS / nq;
+    const dim3 grid(1, (g.n[1] - 2 + rows - 1) / rows, g.n[0] - 2);
+    out.push_back([q2, R, grid](cudaStream_t s, bool adv) {
+      cwb::Pml3Params<T> q = q2;
+      if (adv)
+        q.flags |= cwb::K_ADV;
+      return pml3d_r<T>(q, R, 2, grid, s);
+    });
   }
-  if (total == 0)
-    return;
-  const dim3 grid((unsigned)((total + cwb::PML_THREADS - 1) / cwb::PML_THREADS));
-  out.push_back([pp, nd, R, uniform, grid](cudaStream_t s, bool adv) {
-    cwb::PmlStepParams<T> q = pp;
-    if (adv)
-      q.flags |= cwb::K_ADV;
-    return pml_step_r<T>(q, nd, R, uniform, grid, s);
-  });
+  return CWB_OK;
 }
 
 // The step op's common parameters: geometry, stencil row, factors, materials, pml memory.
@@ -714,8 +705,8 @@ int translate(cwb_plan *p, const cwb_op &op, const size_t slot, cudaStream_t str
             q.s.flags |= cwb::K_ADV;
           return step3d_r<T>(q, R, uniform, grid, s);
         });
-        if (op.flags & CWB_PML)
-          pml_launch<T>(p, sp, uniform, out);
+        if ((op.flags & CWB_PML) && (rc = pml_launch<T>(p, sp, out)))
+          return rc;
       }
       if ((op.flags & CWB_FOLD_SOURCES) && op.points.num > 0) {
         if (!op.points.weight || !op.points.record)

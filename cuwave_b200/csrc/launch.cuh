@@ -57,11 +57,12 @@ template <typename T, int R>
 cudaError_t march2d_unit(const March2Params<T> &p, int sms, cudaStream_t stream);
 
 template <typename T>
-struct PmlStepParams;
+struct Pml3Params;
 
-// the pml memory update of a step over the slab nodes (after the blocked step)
-template <typename T, int NDIM, int R>
-cudaError_t pml_step_unit(const PmlStepParams<T> &p, bool uniform, dim3 grid, cudaStream_t stream);
+// the pml memory update of a 3D step along axis 1 or 2, over its slab nodes (after the
+// blocked step)
+template <typename T, int R>
+cudaError_t pml3d_unit(const Pml3Params<T> &p, int axis, dim3 grid, cudaStream_t stream);
 
 template <typename T, int NDIM, int R>
 cudaError_t adjoint_unit(const AdjointParams<T> &p, bool uniform, int mode, dim3 grid,

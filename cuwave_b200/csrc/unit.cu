@@ -167,15 +167,18 @@ cudaError_t adjoint2d_unit(const AdjointParams<T> &p, const int mode, const dim3
 }
 #endif
 
-template <typename T, int NDIM, int R>
-cudaError_t pml_step_unit(const PmlStepParams<T> &p, const bool uniform, const dim3 grid,
-                          cudaStream_t s) {
-  if (uniform)
-    pml_step_kernel<T, NDIM, R, true><<<grid, PML_THREADS, 0, s>>>(p);
+#if CWB_NDIM == 3
+template <typename T, int R>
+cudaError_t pml3d_unit(const Pml3Params<T> &p, const int axis, const dim3 grid, cudaStream_t s) {
+  if (axis == 1)
+    pml_axis1_kernel<T, R><<<grid, PML1_THREADS, 0, s>>>(p);
+  else if (axis == 2)
+    pml_axis2_kernel<T, R><<<grid, PML2_THREADS, 0, s>>>(p);
   else
-    pml_step_kernel<T, NDIM, R, false><<<grid, PML_THREADS, 0, s>>>(p);
+    return cudaErrorInvalidValue;
   return cudaGetLastError();
 }
+#endif
 
 template <typename T, int NDIM, int R>
 cudaError_t step_unit(const StepParams<T> &p, const bool uniform, const dim3 grid,
@@ -215,9 +218,9 @@ template cudaError_t adjoint2d_unit<CWB_REAL, CWB_RADIUS>(const AdjointParams<CW
 template cudaError_t step3d_unit<CWB_REAL, CWB_RADIUS>(const Step3Params<CWB_REAL> &, bool, dim3,
                                                        cudaStream_t);
 template int step3d_halo<CWB_REAL, CWB_RADIUS>();
+template cudaError_t pml3d_unit<CWB_REAL, CWB_RADIUS>(const Pml3Params<CWB_REAL> &, int, dim3,
+                                                      cudaStream_t);
 #endif
-template cudaError_t pml_step_unit<CWB_REAL, CWB_NDIM, CWB_RADIUS>(
-    const PmlStepParams<CWB_REAL> &, bool, dim3, cudaStream_t);
 template cudaError_t adjoint_unit<CWB_REAL, CWB_NDIM, CWB_RADIUS>(
     const AdjointParams<CWB_REAL> &, bool, int, dim3, cudaStream_t);
 
