@@ -95,6 +95,15 @@ class Op(ctypes.Structure):
     ]
 
 
+class BatchItem(ctypes.Structure):
+    _fields_ = [
+        ("plan", ctypes.c_void_p),
+        ("step", Op),
+        ("record", Points),
+        ("steps", ctypes.c_int32),
+    ]
+
+
 _lib = None
 
 
@@ -122,6 +131,18 @@ def library() -> ctypes.CDLL:
             ctypes.c_void_p,
         ]
         lib.cwb_march.restype = ctypes.c_int
+        lib.cwb_batch_create.argtypes = [ctypes.POINTER(BatchItem), ctypes.c_int32,
+                                         ctypes.POINTER(ctypes.c_void_p)]
+        lib.cwb_batch_create.restype = ctypes.c_int
+        lib.cwb_batch_tune.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p]
+        lib.cwb_batch_tune.restype = ctypes.c_int
+        lib.cwb_batch_march.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,
+                                        ctypes.c_int32, ctypes.c_void_p]
+        lib.cwb_batch_march.restype = ctypes.c_int
+        lib.cwb_batch_threads.argtypes = [ctypes.c_void_p]
+        lib.cwb_batch_threads.restype = ctypes.c_int64
+        lib.cwb_batch_destroy.argtypes = [ctypes.c_void_p]
+        lib.cwb_batch_destroy.restype = ctypes.c_int
         lib.cwb_pml_row.argtypes = [ctypes.c_void_p, ctypes.c_int32]
         lib.cwb_pml_row.restype = ctypes.c_int64
         lib.cwb_launches.restype = ctypes.c_int64
@@ -225,3 +246,34 @@ def op(kind: int, **fields) -> Op:
 def launches() -> int:
     """Kernels the library has launched in this process."""
     return int(library().cwb_launches())
+
+
+class Batch:
+    """A native batch of 2D forward steps (cwb_batch_*), one item a problem."""
+
+    def __init__(self, items: list[BatchItem]):
+        self._lib = library()
+        array = (BatchItem * len(items))(*items)
+        handle = ctypes.c_void_p()
+        check(self._lib.cwb_batch_create(array, len(items), ctypes.byref(handle)))
+        self.handle = handle
+
+    def tune(self, steps: int) -> int:
+        stream = torch.cuda.current_stream().cuda_stream
+        check(self._lib.cwb_batch_tune(self.handle, int(steps), ctypes.c_void_p(stream)))
+        return int(self._lib.cwb_batch_threads(self.handle))
+
+    def march(self, t0: int, steps: int, graph: bool = True) -> None:
+        stream = torch.cuda.current_stream().cuda_stream
+        check(self._lib.cwb_batch_march(self.handle, int(t0), int(steps), int(graph),
+                                        ctypes.c_void_p(stream)))
+
+    def __del__(self):
+        handle = getattr(self, "handle", None)
+        if handle is not None and handle.value:
+            try:
+                self._lib.cwb_batch_destroy(handle)
+            except Exception:  # interpreter shutdown
+                pass
+            self.handle = None
+

@@ -14,6 +14,7 @@
 #include "cuwave_b200.h"
 #include "launch.cuh"
 #include "pml.cuh"
+#include "batch.cuh"
 #include "adjoint2d.cuh"
 #include "step2d.cuh"
 #include "step3d.cuh"
@@ -657,7 +658,7 @@ int translate(cwb_plan *p, const cwb_op &op, const size_t slot, cudaStream_t str
     const bool tma = !blocked && !super && !masked && p->tma &&
                      tma_maps<T>(p, op, derive, sp.minv, tp, ndim == 3 ? cwb::TMA_BX3 : cwb::TMA_BX2,
                                  ndim == 3 ? cwb::TMA_BY3 : 1, Hrow);
-    // 2D, a uniform stiffness, float, radius <= 4: the quad step, which reads u^(t-1),
+    // 2D, a uniform stiffness, float: the quad step, which reads u^(t-1),
     // u^(t-2) and 1/m as 16-byte rows (levels and 1/m on 16-byte boundaries)
     const auto aligned16 = [](const void *ptr, const long long stride_elems) {
       return reinterpret_cast<uintptr_t>(ptr) % 16 == 0 && (stride_elems * (long long)sizeof(T)) % 16 == 0;
@@ -1046,7 +1047,7 @@ cudaError_t march2d_r(const cwb::March2Params<T> &mp, const int R, const int sms
   return cudaErrorInvalidValue;
 }
 
-// A 2D op list [step, records] of a uniform stiffness (float, radius <= 4) runs as one
+// A 2D op list [step, records] of a uniform stiffness (float) runs as one
 // cooperative launch of all its steps, sources and refill folded into the step and a
 // grid-wide barrier before the records (march2d_kernel). Returns false where the list is
 // another shape, leaving it to the per-step march.
@@ -1205,9 +1206,381 @@ int march(cwb_plan *p, const cwb_op *ops, const int nops, const int t0, const in
   return CWB_OK;
 }
 
+// ------------------------------------------------------------------------------ batches
+template <typename T>
+cudaError_t batch2d_r(const cwb::Batch2Params<T> &p, const int R, const dim3 grid,
+                      cudaStream_t s) {
+  switch (R) {
+  case 1: return cwb::batch2d_unit<T, 1>(p, grid, s);
+  case 2: return cwb::batch2d_unit<T, 2>(p, grid, s);
+  case 3: return cwb::batch2d_unit<T, 3>(p, grid, s);
+  case 4: return cwb::batch2d_unit<T, 4>(p, grid, s);
+  case 5: return cwb::batch2d_unit<T, 5>(p, grid, s);
+  case 6: return cwb::batch2d_unit<T, 6>(p, grid, s);
+  case 7: return cwb::batch2d_unit<T, 7>(p, grid, s);
+  case 8: return cwb::batch2d_unit<T, 8>(p, grid, s);
+  }
+  return cudaErrorInvalidValue;
+}
+
+}  // namespace
+
+struct cwb_batch {
+  std::vector<cwb_batch_item> items;
+  int *ctr = nullptr;
+  cudaStream_t lane = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr, t_begin = nullptr, t_end = nullptr;
+  int sms = 148;
+  long long want = 0;  // threads a launch aims at
+  struct Group {
+    int R = 0;
+    void *items = nullptr;  // device Batch2Item<float>[count]
+    int count = 0;
+    long long total = 0;
+  };
+  std::vector<Group> groups;
+  void *recs = nullptr;  // device BatchRecord<float>[items]
+  int *owner = nullptr, *col = nullptr;
+  int nsens = 0;
+  int max_steps = 0;
+};
+
+namespace {
+
+void batch_free_groups(cwb_batch *b) {
+  for (auto &g : b->groups)
+    if (g.items)
+      cudaFree(g.items);
+  b->groups.clear();
+}
+
+// Lay out the items' launches for a launch of about `want` threads: every item marches
+// chunks of the same number of rows (its own rows at most), so the threads carry equal
+// work; items padded to whole blocks, grouped by radius.
+int batch_layout(cwb_batch *b, const long long want) {
+  using T = float;
+  batch_free_groups(b);
+  b->want = want;
+  long long units = 0;
+  for (const auto &it : b->items) {
+    const Geometry &g = it.plan->geo;
+    units += (long long)(g.n[0] - 2) * ((g.n[1] - 2) / 4 + 1);
+  }
+  const long long rows_per = std::max<long long>(1, (units + want - 1) / want);
+  std::vector<int> radii;
+  for (const auto &it : b->items)
+    if (std::find(radii.begin(), radii.end(), it.plan->grid.radius) == radii.end())
+      radii.push_back(it.plan->grid.radius);
+  std::sort(radii.begin(), radii.end());
+  for (const int R : radii) {
+    std::vector<cwb::Batch2Item<T>> host;
+    long long first = 0;
+    for (const auto &it : b->items) {
+      if (it.plan->grid.radius != R)
+        continue;
+      cwb::Batch2Item<T> bi;
+      std::memset(&bi, 0, sizeof bi);
+      int flags = 0;
+      bool uniform = false;
+      int rc;
+      if ((rc = step_setup<T>(it.plan, it.step, bi.s, flags, uniform)))
+        return rc;
+      const Geometry &g = it.plan->geo;
+      const long long rows = g.n[0] - 2, quads = (g.n[1] - 2) / 4 + 1;
+      bi.s.chunk = (int)std::min<long long>(rows, rows_per);
+      bi.s.flags = flags;
+      bi.s.u0 = to_level(it.step.a, 4);
+      bi.s.u1 = to_level(it.step.b, 4);
+      bi.s.u2 = to_level(it.step.c, 4);
+      bi.s.ctr = b->ctr;
+      if ((it.step.flags & CWB_FOLD_SOURCES) && it.step.points.num > 0) {
+        const cwb_points &src = it.step.points;
+        bi.fold.lin = src.lin;
+        bi.fold.weight = static_cast<const T *>(src.weight);
+        bi.fold.signal = static_cast<const T *>(src.record);
+        bi.fold.nsrc = src.num;
+        bi.fold.sig_mul = src.row_mul;
+        bi.fold.sig_add = src.row_add;
+      }
+      if (it.step.flags & CWB_FOLD_REFILL)
+        bi.fold.refill = it.plan->grid.neumann | it.plan->grid.dirichlet;
+      bi.first = first;
+      bi.steps = it.steps;
+      const long long threads = quads * ((rows + bi.s.chunk - 1) / bi.s.chunk);
+      first += (threads + cwb::S2_THREADS - 1) / cwb::S2_THREADS * cwb::S2_THREADS;
+      host.push_back(bi);
+    }
+    cwb_batch::Group grp;
+    grp.R = R;
+    grp.count = (int)host.size();
+    grp.total = first;
+    CWB_CUDA(cudaMalloc(&grp.items, sizeof(cwb::Batch2Item<T>) * host.size()));
+    b->groups.push_back(grp);
+    CWB_CUDA(cudaMemcpy(grp.items, host.data(), sizeof(cwb::Batch2Item<T>) * host.size(),
+                        cudaMemcpyHostToDevice));
+  }
+  return CWB_OK;
+}
+
+// the launches of one step of the batch: a step per radius group, then the receivers
+std::vector<Launch> batch_launches(cwb_batch *b, const bool records) {
+  using T = float;
+  std::vector<Launch> out;
+  for (const auto &g : b->groups) {
+    cwb::Batch2Params<T> bp;
+    std::memset(&bp, 0, sizeof bp);
+    bp.items = static_cast<const cwb::Batch2Item<T> *>(g.items);
+    bp.count = g.count;
+    bp.total = g.total;
+    bp.ctr = b->ctr;
+    const dim3 grid((unsigned)((g.total + cwb::S2_THREADS - 1) / cwb::S2_THREADS));
+    const int R = g.R;
+    out.push_back([bp, R, grid](cudaStream_t s, bool adv) {
+      cwb::Batch2Params<T> q = bp;
+      q.flags = adv ? cwb::K_ADV : 0;
+      return batch2d_r<T>(q, R, grid, s);
+    });
+  }
+  if (records && b->nsens > 0) {
+    cwb::BatchRecordParams<T> rp;
+    std::memset(&rp, 0, sizeof rp);
+    rp.recs = static_cast<const cwb::BatchRecord<T> *>(b->recs);
+    rp.owner = b->owner;
+    rp.col = b->col;
+    rp.total = b->nsens;
+    rp.ctr = b->ctr;
+    out.push_back([rp](cudaStream_t s, bool adv) {
+      cwb::BatchRecordParams<T> q = rp;
+      q.flags = adv ? cwb::K_ADV : 0;
+      return cwb::launch_batch_record<T>(q, s);
+    });
+  }
+  return out;
+}
+
+int batch_run(cwb_batch *b, const std::vector<Launch> &launches, const int t0, const int steps,
+              const bool graph, cudaStream_t s) {
+  CWB_CUDA(cwb::launch_set_counter(b->ctr, t0, s));
+  ++g_launches;
+  int done = 0;
+  if (graph && steps >= 2 * GRAPH_STEPS) {
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    CWB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    int rc = CWB_OK;
+    for (int k = 0; k < GRAPH_STEPS && !rc; ++k)
+      rc = enqueue_step(launches, s);
+    const cudaError_t ce = cudaStreamEndCapture(s, &g);
+    if (rc)
+      return rc;
+    if (ce != cudaSuccess)
+      return fail(CWB_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
+    g_launches -= (long long)GRAPH_STEPS * launches.size();
+    CWB_CUDA(cudaGraphInstantiate(&exec, g, 0));
+    cudaGraphDestroy(g);
+    for (; done + GRAPH_STEPS <= steps; done += GRAPH_STEPS) {
+      const cudaError_t e = cudaGraphLaunch(exec, s);
+      if (e != cudaSuccess) {
+        cudaGraphExecDestroy(exec);
+        return fail(CWB_ERR_CUDA, std::string("graph launch: ") + cudaGetErrorString(e));
+      }
+      g_launches += (long long)GRAPH_STEPS * launches.size();
+    }
+    cudaGraphExecDestroy(exec);
+  }
+  for (; done < steps; ++done) {
+    const int rc = enqueue_step(launches, s);
+    if (rc)
+      return rc;
+  }
+  return CWB_OK;
+}
+
+// zero a level stack and the pml memory an item steps
+int batch_rest(const cwb_batch_item &it, cudaStream_t s) {
+  const cwb_level *levels[3] = {&it.step.a, &it.step.b, &it.step.c};
+  for (const cwb_level *L : levels) {
+    const long long count = std::max(1, L->count);
+    CWB_CUDA(cudaMemsetAsync(L->base, 0, (size_t)(count * L->stride) * 4, s));
+  }
+  for (int d = 0; d < 3; ++d)
+    if (it.step.memory[d] && it.plan->pml_row[d] > 0)
+      CWB_CUDA(cudaMemsetAsync(it.step.memory[d], 0, (size_t)(3 * it.plan->pml_row[d]) * 4, s));
+  return CWB_OK;
+}
+
 }  // namespace
 
 extern "C" {
+
+int cwb_batch_destroy(cwb_batch *b) {
+  if (!b)
+    return CWB_OK;
+  if (b->lane)
+    cudaStreamSynchronize(b->lane);
+  batch_free_groups(b);
+  if (b->recs)
+    cudaFree(b->recs);
+  if (b->owner)
+    cudaFree(b->owner);
+  if (b->col)
+    cudaFree(b->col);
+  if (b->ctr)
+    cudaFree(b->ctr);
+  cudaEvent_t events[4] = {b->fork, b->join, b->t_begin, b->t_end};
+  for (cudaEvent_t e : events)
+    if (e)
+      cudaEventDestroy(e);
+  if (b->lane)
+    cudaStreamDestroy(b->lane);
+  delete b;
+  return CWB_OK;
+}
+
+int cwb_batch_create(const cwb_batch_item *items, const int32_t n, cwb_batch **out) {
+  if (!items || n <= 0 || !out)
+    return fail(CWB_ERR_ARG, "null argument");
+  *out = nullptr;
+  const auto aligned16 = [](const void *ptr, const long long stride_elems) {
+    return reinterpret_cast<uintptr_t>(ptr) % 16 == 0 && (stride_elems * 4LL) % 16 == 0;
+  };
+  int max_steps = 0;
+  for (int i = 0; i < n; ++i) {
+    const cwb_batch_item &it = items[i];
+    const std::string at = "batch item " + std::to_string(i) + ": ";
+    if (!it.plan)
+      return fail(CWB_ERR_ARG, at + "no plan");
+    const cwb_plan *p = it.plan;
+    if (p->geo.ndim != 2 || p->grid.precision != 4)
+      return fail(CWB_ERR_UNSUPPORTED, at + "a batch steps 2D float grids");
+    if (p->geo.n[0] < 3 * p->grid.radius || p->geo.n[1] < 3 * p->grid.radius)
+      return fail(CWB_ERR_UNSUPPORTED, at + "axes of at least 3 radii");
+    const cwb_op &op = it.step;
+    if (op.kind != CWB_OP_STEP || !op.mat.stiff_uniform || op.mat.cells)
+      return fail(CWB_ERR_UNSUPPORTED, at + "a step of a uniform stiffness, unmasked");
+    if (!aligned16(op.a.base, op.a.stride) || !aligned16(op.b.base, op.b.stride) ||
+        !aligned16(op.c.base, op.c.stride) || (!op.mat.derive_inertia && !aligned16(op.mat.minv, 0)))
+      return fail(CWB_ERR_ARG, at + "levels and 1/m on 16-byte boundaries");
+    if ((op.flags & CWB_FOLD_SOURCES) && op.points.num > 0 &&
+        (op.points.num > 32 || !op.points.lin || !op.points.weight || !op.points.record))
+      return fail(CWB_ERR_ARG, at + "at most 32 folded sources, with weights and a signal");
+    if (it.record.num > 0 && (!it.record.lin || !it.record.record || it.record.store != 0))
+      return fail(CWB_ERR_ARG, at + "a record needs indices and native storage");
+    if (it.steps < 0)
+      return fail(CWB_ERR_ARG, at + "a negative step count");
+    max_steps = std::max(max_steps, it.steps);
+  }
+  cwb_batch *b = new cwb_batch();
+  b->items.assign(items, items + n);
+  b->max_steps = max_steps;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, dev);
+  if (cudaMalloc(&b->ctr, 2 * sizeof(int)) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&b->lane, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&b->join, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreate(&b->t_begin) != cudaSuccess || cudaEventCreate(&b->t_end) != cudaSuccess) {
+    cwb_batch_destroy(b);
+    return fail(CWB_ERR_ALLOC, "batch resources");
+  }
+  cudaMemset(b->ctr, 0, 2 * sizeof(int));
+  // the receivers: one table entry per item, one (owner, column) pair per sensor
+  std::vector<cwb::BatchRecord<float>> recs(n);
+  std::vector<int> owner, col;
+  for (int i = 0; i < n; ++i) {
+    const cwb_batch_item &it = items[i];
+    std::memset(&recs[i], 0, sizeof recs[i]);
+    recs[i].a = to_level(it.step.c, 4);
+    recs[i].lin = it.record.lin;
+    recs[i].record = static_cast<float *>(it.record.record);
+    recs[i].num = it.record.num;
+    recs[i].steps = it.steps;
+    for (int j = 0; j < it.record.num; ++j) {
+      owner.push_back(i);
+      col.push_back(j);
+    }
+  }
+  b->nsens = (int)owner.size();
+  int rc = CWB_OK;
+  if (cudaMalloc(&b->recs, sizeof(cwb::BatchRecord<float>) * n) != cudaSuccess ||
+      (b->nsens && (cudaMalloc(&b->owner, sizeof(int) * b->nsens) != cudaSuccess ||
+                    cudaMalloc(&b->col, sizeof(int) * b->nsens) != cudaSuccess))) {
+    cwb_batch_destroy(b);
+    return fail(CWB_ERR_ALLOC, "batch receivers");
+  }
+  cudaMemcpy(b->recs, recs.data(), sizeof(cwb::BatchRecord<float>) * n, cudaMemcpyHostToDevice);
+  if (b->nsens) {
+    cudaMemcpy(b->owner, owner.data(), sizeof(int) * b->nsens, cudaMemcpyHostToDevice);
+    cudaMemcpy(b->col, col.data(), sizeof(int) * b->nsens, cudaMemcpyHostToDevice);
+  }
+  if ((rc = batch_layout(b, (long long)b->sms * 1024))) {
+    cwb_batch_destroy(b);
+    return rc;
+  }
+  *out = b;
+  return CWB_OK;
+}
+
+int cwb_batch_tune(cwb_batch *b, const int32_t steps, void *stream) {
+  if (!b || steps <= 0)
+    return fail(CWB_ERR_ARG, "null batch or no steps");
+  cudaStream_t user = static_cast<cudaStream_t>(stream);
+  CWB_CUDA(cudaEventRecord(b->fork, user));
+  CWB_CUDA(cudaStreamWaitEvent(b->lane, b->fork, 0));
+  cudaStream_t s = b->lane;
+  const int run = std::min(steps, std::max(1, b->max_steps));
+  const long long candidates[] = {256, 512, 1024, 2048, 4096};
+  long long best = (long long)b->sms * 1024;
+  float best_ms = 1e30f;
+  int rc;
+  for (const long long per : candidates) {
+    if ((rc = batch_layout(b, per * b->sms)))
+      return rc;
+    const std::vector<Launch> launches = batch_launches(b, false);
+    if ((rc = batch_run(b, launches, 0, 1, false, s)))  // warm: the first launch loads code
+      return rc;
+    CWB_CUDA(cudaEventRecord(b->t_begin, s));
+    if ((rc = batch_run(b, launches, 0, run, false, s)))
+      return rc;
+    CWB_CUDA(cudaEventRecord(b->t_end, s));
+    CWB_CUDA(cudaEventSynchronize(b->t_end));
+    float ms = 0.f;
+    CWB_CUDA(cudaEventElapsedTime(&ms, b->t_begin, b->t_end));
+    if (ms < best_ms) {
+      best_ms = ms;
+      best = per * b->sms;
+    }
+  }
+  for (const auto &it : b->items)
+    if ((rc = batch_rest(it, s)))
+      return rc;
+  if ((rc = batch_layout(b, best)))
+    return rc;
+  CWB_CUDA(cudaEventRecord(b->join, s));
+  CWB_CUDA(cudaStreamWaitEvent(user, b->join, 0));
+  return CWB_OK;
+}
+
+int cwb_batch_march(cwb_batch *b, const int32_t t0, const int32_t steps, const int32_t graph,
+                    void *stream) {
+  if (!b)
+    return fail(CWB_ERR_ARG, "null batch");
+  if (steps <= 0)
+    return CWB_OK;
+  cudaStream_t user = static_cast<cudaStream_t>(stream);
+  CWB_CUDA(cudaEventRecord(b->fork, user));
+  CWB_CUDA(cudaStreamWaitEvent(b->lane, b->fork, 0));
+  const std::vector<Launch> launches = batch_launches(b, true);
+  int rc;
+  if ((rc = batch_run(b, launches, t0, steps, graph != 0, b->lane)))
+    return rc;
+  CWB_CUDA(cudaEventRecord(b->join, b->lane));
+  CWB_CUDA(cudaStreamWaitEvent(user, b->join, 0));
+  return CWB_OK;
+}
+
+int64_t cwb_batch_threads(const cwb_batch *b) { return b ? b->want : 0; }
 
 const char *cwb_last_error(void) { return g_error.c_str(); }
 

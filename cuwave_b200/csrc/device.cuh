@@ -132,6 +132,16 @@ __device__ __forceinline__ void mirror_run_lo(T *xr, const T s) {
     xr[H - 1 - m] = s * xr[H + 3 + m];
 }
 
+// mirror_run_lo for a run whose first `lead` values lie past the low wall: a run of halo
+// H that starts at node -lead (lead = H - x0 of its quad, a multiple of four up to H)
+template <typename T, int XR, int H>
+__device__ __forceinline__ void mirror_run_lo_at(T *xr, const T s, const int lead) {
+  if (lead == H)
+    mirror_run_lo<T, XR, H>(xr, s);
+  else if constexpr (H > 4)
+    mirror_run_lo_at<T, XR, H - 4>(xr, s, lead);
+}
+
 template <typename T, int XR, int E>
 __device__ __forceinline__ void mirror_run_hi(T *xr, const T s) {
 #pragma unroll

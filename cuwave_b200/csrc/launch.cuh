@@ -39,7 +39,7 @@ cudaError_t step3d_unit(const Step3Params<T> &p, bool uniform, dim3 grid, cudaSt
 template <typename T, int R>
 int step3d_halo();  // the staged box's axis-2 halo, -1 where the kernel is not built
 
-// the 2D quad step of a uniform stiffness (float, radius <= 4), 128 threads a block
+// the 2D quad step of a uniform stiffness (float), 128 threads a block
 template <typename T, int R>
 cudaError_t step2d_unit(const StepParams<T> &p, bool uniform, dim3 grid, cudaStream_t stream);
 template <typename T, int R>
@@ -76,6 +76,16 @@ cudaError_t launch_pml_aux(const PmlAuxParams<T> &p, cudaStream_t stream);
 template <typename T>
 cudaError_t launch_frechet(const FrechetParams<T> &p, cudaStream_t stream);
 cudaError_t launch_set_counter(int *ctr, int t0, cudaStream_t stream);
+
+template <typename T>
+struct Batch2Params;
+template <typename T>
+struct BatchRecordParams;
+// one step of a batch's items of radius R (2D quad step)
+template <typename T, int R>
+cudaError_t batch2d_unit(const Batch2Params<T> &p, dim3 grid, cudaStream_t stream);
+template <typename T>
+cudaError_t launch_batch_record(const BatchRecordParams<T> &p, cudaStream_t stream);
 
 enum : int { TR_EXCITE = 0, TR_LOAD = 1, TR_RECORD = 2, TR_REPLAY = 3, TR_REFILL = 4, TR_DFT = 5 };
 

@@ -209,7 +209,7 @@ __global__ void __launch_bounds__(PML2_THREADS) pml_axis2_kernel(const __grid_co
         }
       }
       if (xq - H < 0)
-        mirror_run_lo<T, XR, H>(xr, (dirF & 1) ? (T)-1 : (T)1);
+        mirror_run_lo_at<T, XR, H>(xr, (dirF & 1) ? (T)-1 : (T)1, H - xq);
       const int e_hi = NF - (xq - H);
       if (e_hi <= XR - 1)
         mirror_run_hi_at<T, XR, H + 2>(xr, (dirF & 2) ? (T)-1 : (T)1, e_hi);

@@ -31,8 +31,10 @@ template <typename T, int R>
 struct Step2Shape {
   static constexpr int H = (R + 3) / 4 * 4;  // the run's halo, whole quads
   static constexpr int XR = 4 + 2 * H;
-  // float up to radius 4 (its registers); the host sends other cases to the row kernel
-  static constexpr bool SUPPORTED = sizeof(T) == 4 && R <= 4;
+  // float (16-byte quads of four); the queue of 2R rows of four fits four blocks of 128
+  // threads an SM up to radius 5, two from 6 on
+  static constexpr bool SUPPORTED = sizeof(T) == 4 && R <= 8;
+  static constexpr int MIN_BLOCKS = R <= 5 ? 4 : 2;
 };
 
 // The sources and the ghost refill a multi-step march folds into the step: the sources
@@ -134,7 +136,7 @@ __device__ __forceinline__ void step2d_rows(const StepParams<T> &p, const int t,
         }
       }
       if (fix_lo)
-        mirror_run_lo<T, XR, H>(xr, slo);
+        mirror_run_lo_at<T, XR, H>(xr, slo, H - xq);
       if (fix_hi)
         mirror_run_hi_at<T, XR, H + 2>(xr, shi, e_hi);
       T old[4], mi[4];
@@ -293,9 +295,10 @@ __device__ __forceinline__ void step2d_rows(const StepParams<T> &p, const int t,
 }
 
 template <typename T, int R, bool UNIF>
-__global__ void __launch_bounds__(S2_THREADS, 4) step2d_kernel(const StepParams<T> p) {
+__global__ void __launch_bounds__(S2_THREADS, Step2Shape<T, R>::MIN_BLOCKS)
+    step2d_kernel(const StepParams<T> p) {
   static_assert(Step2Shape<T, R>::SUPPORTED && UNIF,
-                "the 2D quad step is built for float, radius <= 4, a uniform stiffness");
+                "the 2D quad step is built for float and a uniform stiffness");
   const Fold2<T> none{};
   step2d_rows<T, R>(p, step_index(p.ctr), (long long)blockIdx.x * S2_THREADS + threadIdx.x, none);
   finish_step(p.ctr, p.flags & K_ADV);
@@ -319,8 +322,9 @@ struct March2Params {
 };
 
 template <typename T, int R>
-__global__ void __launch_bounds__(S2_THREADS, 4) march2d_kernel(const __grid_constant__ March2Params<T> mp) {
-  static_assert(Step2Shape<T, R>::SUPPORTED, "the 2D quad step is built for float, radius <= 4");
+__global__ void __launch_bounds__(S2_THREADS, Step2Shape<T, R>::MIN_BLOCKS)
+    march2d_kernel(const __grid_constant__ March2Params<T> mp) {
+  static_assert(Step2Shape<T, R>::SUPPORTED, "the 2D quad step is built for float");
   namespace cg = cooperative_groups;
   cg::grid_group grid = cg::this_grid();
   const long long gtid = (long long)blockIdx.x * blockDim.x + threadIdx.x;

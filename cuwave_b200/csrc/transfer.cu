@@ -1,6 +1,7 @@
 // The transfer, refill and adjoint pml memory kernels of both precisions.
 #include "launch.cuh"
 #include "transfer.cuh"
+#include "batch.cuh"
 
 namespace cwb {
 
@@ -41,6 +42,15 @@ cudaError_t launch_frechet(const FrechetParams<T> &p, cudaStream_t stream) {
   return cudaGetLastError();
 }
 
+template <typename T>
+cudaError_t launch_batch_record(const BatchRecordParams<T> &p, cudaStream_t stream) {
+  const int blocks = (p.total + TRANSFER_THREADS - 1) / TRANSFER_THREADS;
+  if (blocks <= 0)
+    return cudaErrorInvalidValue;
+  batch_record_kernel<T><<<blocks, TRANSFER_THREADS, 0, stream>>>(p);
+  return cudaGetLastError();
+}
+
 __global__ void set_counter_kernel(int *ctr, const int t0) {
   ctr[0] = t0;
   ctr[1] = 0;
@@ -57,6 +67,8 @@ template cudaError_t launch_transfer<double>(int, const TransferParams<double> &
                                              int, int, cudaStream_t);
 template cudaError_t launch_frechet<float>(const FrechetParams<float> &, cudaStream_t);
 template cudaError_t launch_frechet<double>(const FrechetParams<double> &, cudaStream_t);
+template cudaError_t launch_batch_record<float>(const BatchRecordParams<float> &, cudaStream_t);
+template cudaError_t launch_batch_record<double>(const BatchRecordParams<double> &, cudaStream_t);
 template cudaError_t launch_pml_aux<float>(const PmlAuxParams<float> &, cudaStream_t);
 template cudaError_t launch_pml_aux<double>(const PmlAuxParams<double> &, cudaStream_t);
 

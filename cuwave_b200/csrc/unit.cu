@@ -7,6 +7,7 @@
 #include "step.cuh"
 #include "step_tma.cuh"
 #include "pml.cuh"
+#include "batch.cuh"
 #include "adjoint2d.cuh"
 #include "step2d.cuh"
 #include "step3d.cuh"
@@ -130,6 +131,16 @@ bool step2d_built() {
 }
 
 template <typename T, int R>
+cudaError_t batch2d_unit(const Batch2Params<T> &p, const dim3 grid, cudaStream_t s) {
+  if constexpr (!Step2Shape<T, R>::SUPPORTED) {
+    return cudaErrorInvalidValue;
+  } else {
+    batch2d_kernel<T, R><<<grid, S2_THREADS, 0, s>>>(p);
+    return cudaGetLastError();
+  }
+}
+
+template <typename T, int R>
 cudaError_t march2d_unit(const March2Params<T> &mp, const int sms, cudaStream_t s) {
   if constexpr (!Step2Shape<T, R>::SUPPORTED) {
     return cudaErrorInvalidValue;
@@ -209,6 +220,8 @@ template int step_tma_halo<CWB_REAL, CWB_NDIM, CWB_RADIUS>();
 template cudaError_t step2d_unit<CWB_REAL, CWB_RADIUS>(const StepParams<CWB_REAL> &, bool, dim3,
                                                        cudaStream_t);
 template bool step2d_built<CWB_REAL, CWB_RADIUS>();
+template cudaError_t batch2d_unit<CWB_REAL, CWB_RADIUS>(const Batch2Params<CWB_REAL> &, dim3,
+                                                        cudaStream_t);
 template cudaError_t march2d_unit<CWB_REAL, CWB_RADIUS>(const March2Params<CWB_REAL> &, int,
                                                          cudaStream_t);
 template cudaError_t adjoint2d_unit<CWB_REAL, CWB_RADIUS>(const AdjointParams<CWB_REAL> &, int,

@@ -200,6 +200,38 @@ int cwb_march(cwb_plan *plan, const cwb_op *ops, int32_t nops, int32_t t0,
 int cwb_march_static(const cwb_grid *grid, const cwb_op *ops, int32_t nops, int32_t t0,
                      int32_t steps, void *stream);
 
+/* ------------------------------------------------------------------ batches
+ * Many 2D problems (shots, designs of uneven size and order) stepped together: each
+ * item is one problem's forward step on its own plan, and the batch runs every item's
+ * step t in one launch per stencil radius, then every item's receivers in one launch,
+ * chunks of steps replayed as a CUDA graph. No counterpart in the reference, which runs
+ * a problem at a time (cuwave/utils.py:50-73 spreads shots over GPUs, one simulate
+ * each). */
+typedef struct cwb_batch cwb_batch;
+
+typedef struct cwb_batch_item {
+  cwb_plan *plan;     /* the item's plan: 2D, float */
+  cwb_op step;        /* CWB_OP_STEP of a uniform stiffness, sources (at most 32, interior
+                         nodes) and refill folded; levels, material and pml memory as
+                         cwb_march takes them, on 16-byte boundaries */
+  cwb_points record;  /* receivers read after every step into (steps, num) native
+                         values at row t, or num 0 */
+  int32_t steps;      /* the item's own step count: it rests from t = steps on */
+} cwb_batch_item;
+
+/* Check the items and lay out their launches; the pointers they hold must outlive the
+ * batch. */
+int cwb_batch_create(const cwb_batch_item *items, int32_t n, cwb_batch **batch);
+/* Choose the launches' thread count by timing `steps` steps of each candidate on the
+ * items' own fields, which it zeroes afterwards with their pml memory: call it before
+ * the march, on fields at rest. */
+int cwb_batch_tune(cwb_batch *batch, int32_t steps, void *stream);
+/* Steps t = t0 .. t0 + steps - 1 of every item, as cwb_march. */
+int cwb_batch_march(cwb_batch *batch, int32_t t0, int32_t steps, int32_t graph, void *stream);
+/* Threads a launch of the batch aims at (the tuned choice). */
+int64_t cwb_batch_threads(const cwb_batch *batch);
+int cwb_batch_destroy(cwb_batch *batch);
+
 /* Elements per row of the pml memory of axis d (0 for an unlined axis); a forward
  * memory holds 3 such rows, an adjoint one 5. */
 int64_t cwb_pml_row(const cwb_plan *plan, int32_t d);

@@ -186,6 +186,7 @@ def test_blocked_uniform_step_matches_oracle(R, dirichlet, pml, damping):
 @pytest.mark.parametrize("R,dirichlet,pml,damping", [
     (1, 0b0000, 0, False), (2, 0b0110, 0, False), (3, 0b1001, 3, False),
     (4, 0b0110, 4, False), (4, 0b0000, 0, True), (4, 0b1111, 0, False), (2, 0b0101, 6, False),
+    (5, 0b0110, 0, False), (6, 0b1001, 7, False), (7, 0b0000, 0, True), (8, 0b0101, 9, False),
 ])
 def test_quad_2d_uniform_step_matches_oracle(R, dirichlet, pml, damping):
     """The 2D quad step of a uniform stiffness on a grid of many row chunks and quads, an
@@ -297,3 +298,14 @@ def test_reconstruction_matches_sensitivity(name, checkpoints):
         b = ref[key][valid].cpu().numpy()
         assert cases.rel_l2(a, b) <= 1e-7, key
     assert info["drift"] < 1e-7
+
+
+@pytest.mark.parametrize("name", [n for n in cases.FORWARD + cases.GRADIENT if "damped" in n])
+def test_sponge_matches_reference(name):
+    """`sponge` builds the reference's damping field from the design (boundary.py:238-269)."""
+    from cuwave_b200 import sponge
+
+    fx = cases.load(name)
+    sim, design = cases.product_sim(fx)
+    field = sponge(sim, design.copy(), width=4, beta=0.3)
+    np.testing.assert_array_equal(field, fx["damping_field"])

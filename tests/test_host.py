@@ -37,7 +37,7 @@ def test_ctypes_layout_matches_header():
     from cuwave_b200 import _native as nat
 
     structs = {"cwb_grid": nat.Grid, "cwb_level": nat.Level, "cwb_material": nat.Material,
-               "cwb_points": nat.Points, "cwb_op": nat.Op}
+               "cwb_points": nat.Points, "cwb_op": nat.Op, "cwb_batch_item": nat.BatchItem}
     lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', "int main(void) {"]
     for cname, py in structs.items():
         lines.append(f'printf("{cname} %zu\\n", sizeof({cname}));')

@@ -81,8 +81,8 @@ def test_static_march_matches_plan_march(name):
 
 def test_static_march_refuses_lists_past_its_array():
     """A march whose source lists cannot fit the static array is refused, not truncated.
-    (A radius-8 march: its step folds the sources through per-block lists, which the
-    register-blocked steps of radius 4 and below do not build.)"""
+    (A heterogeneous stiffness: its step folds the sources through per-block lists,
+    which the register-blocked steps of a uniform stiffness do not build.)"""
     from cuwave_b200 import _native as nat
     from cuwave_b200.wave import prepare_shot
 
@@ -91,6 +91,8 @@ def test_static_march_refuses_lists_past_its_array():
     fx = cases.load("fwd2d_r8")
     sim, design = cases.product_sim(fx)
     mat = sim.build_materials(design.copy())
+    mat["stiff"] = mat["stiff"] * (1.0 + 0.1 * torch.rand_like(mat["stiff"]))
+    mat["uniform"] = False
     # 20000 sources on interior nodes: 320 kB of list entries, past the 256 kB array
     rng = np.random.default_rng(0)
     count = 20000
