@@ -143,6 +143,11 @@ def library() -> ctypes.CDLL:
         lib.cwb_batch_threads.restype = ctypes.c_int64
         lib.cwb_batch_destroy.argtypes = [ctypes.c_void_p]
         lib.cwb_batch_destroy.restype = ctypes.c_int
+        vp, i32 = ctypes.c_void_p, ctypes.c_int32
+        lib.cwb_conv_bf16_fwd.argtypes = [vp, vp, vp, vp, vp, vp, i32, i32, i32, i32, i32, i32, vp]
+        lib.cwb_conv_bf16_fwd.restype = ctypes.c_int
+        lib.cwb_conv_bf16_bwd.argtypes = [vp, vp, vp, vp, i32, i32, i32, i32, i32, vp]
+        lib.cwb_conv_bf16_bwd.restype = ctypes.c_int
         lib.cwb_pml_row.argtypes = [ctypes.c_void_p, ctypes.c_int32]
         lib.cwb_pml_row.restype = ctypes.c_int64
         lib.cwb_launches.restype = ctypes.c_int64
@@ -276,4 +281,23 @@ class Batch:
             except Exception:  # interpreter shutdown
                 pass
             self.handle = None
+
+
+def conv_fwd(x, w, bias, y16=None, y32=None, *, relu=False, mask=None) -> None:
+    """cwb_conv_bf16_fwd: x (B, H, W, cin) bf16, w (cout, kpad) bf16, into y16 / y32."""
+    B, H, W, cin = x.shape
+    out = y16 if y16 is not None else y32
+    cout = out.shape[-1]
+    stream = torch.cuda.current_stream().cuda_stream
+    check(library().cwb_conv_bf16_fwd(ptr(x), ptr(w), ptr(bias), ptr(mask), ptr(y16), ptr(y32),
+                                      B, H, W, cin, cout, int(relu), ctypes.c_void_p(stream)))
+
+
+def conv_bwd(dy, x, dw, db=None) -> None:
+    """cwb_conv_bf16_bwd: dw (cout, kpad) += weight gradient, db (cout) += bias gradient."""
+    B, H, W, cin = x.shape
+    cout = dy.shape[-1]
+    stream = torch.cuda.current_stream().cuda_stream
+    check(library().cwb_conv_bf16_bwd(ptr(dy), ptr(x), ptr(dw), ptr(db), B, H, W, cin, cout,
+                                      ctypes.c_void_p(stream)))
 

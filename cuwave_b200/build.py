@@ -69,6 +69,7 @@ def _jobs() -> list[tuple[Path, list[str]]]:
                 defines = [f"-DCWB_REAL={real}", f"-DCWB_NDIM={ndim}", f"-DCWB_RADIUS={radius}"]
                 jobs.append((obj, [str(CSRC / "unit.cu"), *defines]))
     jobs.append((BUILD / "transfer.o", [str(CSRC / "transfer.cu")]))
+    jobs.append((BUILD / "conv.o", [str(CSRC / "conv.cu")]))
     jobs.append((BUILD / "api.o", [str(CSRC / "api.cu")]))
     return jobs
 

@@ -15,6 +15,7 @@
 #include "launch.cuh"
 #include "pml.cuh"
 #include "batch.cuh"
+#include "conv.cuh"
 #include "adjoint2d.cuh"
 #include "step2d.cuh"
 #include "step3d.cuh"
@@ -1581,6 +1582,52 @@ int cwb_batch_march(cwb_batch *b, const int32_t t0, const int32_t steps, const i
 }
 
 int64_t cwb_batch_threads(const cwb_batch *b) { return b ? b->want : 0; }
+
+namespace {
+int conv_shape(const int32_t batch, const int32_t height, const int32_t width, const int32_t cin,
+               const int32_t cout, cwb::ConvShape &s) {
+  if (batch <= 0 || height <= 0 || width <= 0 || cin < 2 || cin % 2 || cout < 1 ||
+      cout > cwb::CONV_MAX_N)
+    return fail(CWB_ERR_ARG, "conv: positive sizes, an even cin, at most 32 output channels");
+  s.batch = batch;
+  s.h = height;
+  s.w = width;
+  s.cin = cin;
+  s.cout = cout;
+  s.kpad = (25 * cin + 15) / 16 * 16;
+  return CWB_OK;
+}
+}  // namespace
+
+int cwb_conv_bf16_fwd(const void *x, const void *w, const float *bias, const void *mask,
+                      void *y_bf16, float *y_f32, const int32_t batch, const int32_t height,
+                      const int32_t width, const int32_t cin, const int32_t cout,
+                      const int32_t relu, void *stream) {
+  cwb::ConvShape s;
+  int rc;
+  if ((rc = conv_shape(batch, height, width, cin, cout, s)))
+    return rc;
+  if (!x || !w || (!y_bf16 && !y_f32))
+    return fail(CWB_ERR_ARG, "conv: null input, weights or output");
+  CWB_CUDA(cwb::conv_forward(x, w, bias, mask, y_bf16, y_f32, s, relu,
+                             static_cast<cudaStream_t>(stream)));
+  ++g_launches;
+  return CWB_OK;
+}
+
+int cwb_conv_bf16_bwd(const void *dy, const void *x, float *dw, float *db, const int32_t batch,
+                      const int32_t height, const int32_t width, const int32_t cin,
+                      const int32_t cout, void *stream) {
+  cwb::ConvShape s;
+  int rc;
+  if ((rc = conv_shape(batch, height, width, cin, cout, s)))
+    return rc;
+  if (!dy || !x || !dw)
+    return fail(CWB_ERR_ARG, "conv: null gradient, input or weight gradient");
+  CWB_CUDA(cwb::conv_weight_grad(dy, x, dw, db, s, static_cast<cudaStream_t>(stream)));
+  g_launches += db ? 2 : 1;
+  return CWB_OK;
+}
 
 const char *cwb_last_error(void) { return g_error.c_str(); }
 

@@ -232,6 +232,26 @@ int cwb_batch_march(cwb_batch *batch, int32_t t0, int32_t steps, int32_t graph, 
 int64_t cwb_batch_threads(const cwb_batch *batch);
 int cwb_batch_destroy(cwb_batch *batch);
 
+/* ---------------------------------------------------------------- corrector
+ * The 5x5 convolutions (stride 1, zero padding 2) of the learned dispersion corrector,
+ * on the tensor cores: BF16 operands, FP32 accumulation. Activations are channels-last
+ * BF16 (batch, height, width, channels); a layer's weights are (cout, kpad) BF16 with
+ * k = (5 ky + kx) cin + ci and kpad = 25 cin rounded up to 16 (the padding zero). cin is
+ * even (pad a channel), cout at most 32. No counterpart in the reference. */
+
+/* y = conv(x, w) + bias (optional), ReLU when `relu`; zeroed where `mask` (BF16, the
+ * shape of y, optional) is not positive; written to y_bf16 and/or y_f32 (either may be
+ * NULL). The data gradient of a layer is this call on dy with the weights flipped and
+ * transposed (wt[ci][(5 ky + kx) cout + co] = w[co][(5 (4 - ky) + 4 - kx) cin + ci]) and
+ * the layer input's activation as the mask. */
+int cwb_conv_bf16_fwd(const void *x, const void *w, const float *bias, const void *mask,
+                      void *y_bf16, float *y_f32, int32_t batch, int32_t height, int32_t width,
+                      int32_t cin, int32_t cout, int32_t relu, void *stream);
+/* dw += the weight gradient sum over pixels of dy[p][co] im2col(x)[p][k] (FP32,
+ * (cout, kpad)), db += sum over pixels of dy (optional). */
+int cwb_conv_bf16_bwd(const void *dy, const void *x, float *dw, float *db, int32_t batch,
+                      int32_t height, int32_t width, int32_t cin, int32_t cout, void *stream);
+
 /* Elements per row of the pml memory of axis d (0 for an unlined axis); a forward
  * memory holds 3 such rows, an adjoint one 5. */
 int64_t cwb_pml_row(const cwb_plan *plan, int32_t d);
