@@ -340,6 +340,113 @@ def two_d_kernels(peak: float, steps: int = 200) -> dict:
     return out
 
 
+def batch_problems(count: int, steps: int, seed: int = 3):
+    """Config 3b's population: `count` 2D designs, sides U{256..1536}, space orders
+    {4..12}, two-phase speeds {1.0, 0.3} from a thresholded smooth random field, a
+    Ricker source at the centre and 64 receivers on a row; `steps` steps each."""
+    import torch
+    import torch.nn.functional as F
+
+    from cuwave_b200 import AcousticWave, Source, ricker, stable_dt
+
+    rng = np.random.default_rng(seed)
+    problems = []
+    for _ in range(count):
+        side = int(rng.integers(256, 1537))
+        order = int(rng.choice([4, 6, 8, 10, 12]))
+        noise = torch.as_tensor(rng.standard_normal((1, 1, side, side)), dtype=torch.float32)
+        smooth = F.avg_pool2d(noise, 15, stride=1, padding=7)[0, 0].numpy()
+        c = np.where(smooth > 0.0, 1.0, 0.3)
+        dx = (1.0, 1.0)
+        dt = 0.5 * stable_dt(dx, 1.0, order)
+        sim = AcousticWave(Nx=(side, side), dx=dx, N=steps, dt=dt, space_order=order,
+                           rho1=1.0, rho2=1.0, kappa1=1.0, kappa2=0.09)
+        full = np.ones(sim.Nx_padded)
+        full[:side, :side] = c
+        ind = AcousticWave.indicator_for_speed(full, 0.09).astype(np.float32)
+        t = np.arange(steps) * dt
+        src = Source(np.array([[side // 2], [side // 2]], np.int32), ricker(t, 1.0, 0.03)[:, None])
+        sens = np.stack([np.full(64, side // 4), np.linspace(2, side - 3, 64).astype(int)]).astype(np.int32)
+        problems.append((sim, src, ind, sens))
+    return problems
+
+
+def batch_measure(count: int = 64, steps: int = 300) -> dict:
+    """simulate_batch over config 3b's population against the same simulate calls in turn
+    (device time, CUDA events; the second of two runs, the first tunes and loads)."""
+    import torch
+
+    from cuwave_b200 import simulate
+    from cuwave_b200.batch import simulate_batch
+
+    problems = batch_problems(count, steps)
+    updates = sum((p[0].Nx[0] - 2) * (p[0].Nx[1] - 2) * p[0].N for p in problems)
+    sims, srcs, inds, sens = (list(x) for x in zip(*problems))
+    out = {}
+    for rep in range(2):
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        e0.record()
+        simulate_batch(sims, srcs, [i.copy() for i in inds], sens)
+        e1.record()
+        for sim, src, ind, s in problems:
+            simulate(sim, src, ind.copy(), s)
+        e2.record()
+        torch.cuda.synchronize()
+        out = {"problems": count, "steps": steps, "updates": updates,
+               "batch_s": e0.elapsed_time(e1) / 1e3, "in_turn_s": e1.elapsed_time(e2) / 1e3}
+    out["batch_gpts"] = updates / out["batch_s"] / 1e9
+    out["in_turn_gpts"] = updates / out["in_turn_s"] / 1e9
+    return out
+
+
+def learned_measure(coarse_nodes: int = 256, coarse_steps: int = 600) -> dict:
+    """Config 4 at a reduced size: the corrector trained on pairs the plain solver makes,
+    then on held-out speed models the fine solve, the plain coarse solve and the corrected
+    coarse solve timed (CUDA events) and their receiver traces compared with the fine
+    ones (relative L2)."""
+    import torch
+
+    from cuwave_b200 import corrector as cr
+
+    pair = cr.grid_pair(coarse_nodes, 1.0, 2.0, coarse_steps)
+    rng = np.random.default_rng(0)
+    inputs, targets = cr.training_pairs(pair, rng, shots=12, windows=12)
+    net = cr.Corrector(seed=1)
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record()
+    losses = cr.train(net, inputs, targets, steps=800, batch=8, lr=5e-4)
+    t1.record()
+    torch.cuda.synchronize()
+    held = np.random.default_rng(99)
+    rows = []
+    Nc = coarse_nodes
+    for _ in range(3):
+        c = cr.speed_field(held, Nc)
+        pos = held.integers(Nc // 4, 3 * Nc // 4, size=2)
+        fsrc, csrc = cr.shot_sources(pair, pos)
+        cs = np.stack([np.full(16, Nc // 5), np.linspace(3, Nc - 4, 16).astype(int)]).astype(np.int32)
+        fs = (2 * cs - 1).astype(np.int32)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        ev[0].record()
+        fine = cr.fine_traces(pair, c, fsrc, fs)
+        ev[1].record()
+        plain, _ = cr.corrected_traces(pair, None, c, csrc, cs)
+        ev[2].record()
+        corr, est = cr.corrected_traces(pair, net, c, csrc, cs)
+        ev[3].record()
+        torch.cuda.synchronize()
+        n = min(fine.shape[0], plain.shape[0])
+        err = lambda a: float((a[:n] - fine[:n]).norm() / fine[:n].norm())  # noqa: E731
+        rows.append({"fine_ms": ev[0].elapsed_time(ev[1]), "coarse_ms": ev[1].elapsed_time(ev[2]),
+                     "corrected_ms": ev[2].elapsed_time(ev[3]), "coarse_error": err(plain),
+                     "corrected_error": err(corr), "estimate": est})
+    return {"coarse_grid": [Nc, Nc], "fine_grid": list(pair.fine.Nx), "coarse_steps": coarse_steps,
+            "fine_steps": pair.fine.N, "train_s": t0.elapsed_time(t1) / 1e3,
+            "train_loss_first": float(np.mean(losses[:5])), "train_loss_last": float(np.mean(losses[-50:])),
+            "held_out": rows}
+
+
 def run_ours(args) -> int:
     import torch
     import torch.distributed as dist
@@ -429,6 +536,8 @@ def run_ours(args) -> int:
     peak, peak_kind = hbm_peak()
     traffic = profile_traffic(w)
     kernels_2d = two_d_kernels(peak) if args.size == 512 and not args.no_2d and world == 1 else None
+    batch = batch_measure() if args.size == 512 and not args.no_batch and world == 1 else None
+    learned = learned_measure() if args.size == 512 and not args.no_learned and world == 1 else None
 
     if world > 1:
         dist.barrier()
@@ -452,6 +561,8 @@ def run_ours(args) -> int:
         "clocks": clock,
         "kernel_updates_per_s": interior_updates(w) / (kernel_ms / 1e3) / 1e9,
         "kernels_2d": kernels_2d,
+        "batch_2d": batch,
+        "learned": learned,
     }
     print(json.dumps(line))
     return 0
@@ -506,6 +617,8 @@ def main(argv=None) -> int:
     parser.add_argument("--ref-sample", type=int, default=3, help="time steps per reference bench step")
     parser.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     parser.add_argument("--no-2d", action="store_true", help="skip the 2D kernel measurements")
+    parser.add_argument("--no-batch", action="store_true", help="skip the batched 2D march")
+    parser.add_argument("--no-learned", action="store_true", help="skip the learned corrector")
     args = parser.parse_args(argv)
     if args.impl == "reference":
         return run_reference(args)

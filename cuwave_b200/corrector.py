@@ -14,8 +14,9 @@ FP32 master weights. `corrected_traces` runs the corrected coarse solve, and
 
 Layout: activations channels-last (batch, height, width, channels) over the coarse grid's
 logical nodes; layers 4 -> 32 -> 32 -> 2 channels of 5x5 convolutions, ReLU between, the
-input's fourth channel and the output's second held at zero (the kernels take an even
-channel count). The coarse node i sits on the fine node 2 i - 1 (both grids put node 1
+input's fourth channel held at zero (the kernels take an even channel count). The two
+outputs correct the coarse field's two levels, so the leapfrog's velocity is corrected
+with its displacement. The coarse node i sits on the fine node 2 i - 1 (both grids put node 1
 at the origin).
 """
 
@@ -79,14 +80,12 @@ class Corrector:
         return self.w + self.b
 
     def _hold(self) -> None:
-        """The padding channels stay zero: input channel 3, output channel 1."""
+        """The padding input channel stays zero."""
         self.w[0][:, 3] = 0.0
-        self.w[-1][1] = 0.0
-        self.b[-1][1] = 0.0
 
     # -------------------------------------------------------------------- passes
     def forward(self, x: torch.Tensor) -> torch.Tensor:
-        """x (B, H, W, 4) BF16 -> the (B, H, W) FP32 output; keeps what backward needs."""
+        """x (B, H, W, 4) BF16 -> the (B, H, W, 2) FP32 output; keeps what backward needs."""
         B, H, W, _ = x.shape
         self._x = x
         self._packed = [pack(w) for w in self.w]
@@ -98,13 +97,12 @@ class Corrector:
         out = torch.empty((B, H, W, CHANNELS[-1]), dtype=torch.float32, device=x.device)
         nat.conv_fwd(acts[-1], self._packed[-1], self.b[-1], y32=out)
         self._acts = acts
-        return out[..., 0]
+        return out
 
     def backward(self, dout: torch.Tensor) -> list[torch.Tensor]:
-        """dL/d(output) (B, H, W) FP32 -> dL/d(params) in the order of `params`."""
-        B, H, W = dout.shape
-        dy = torch.zeros((B, H, W, CHANNELS[-1]), dtype=torch.bfloat16, device=dout.device)
-        dy[..., 0] = dout.to(torch.bfloat16)
+        """dL/d(output) (B, H, W, 2) FP32 -> dL/d(params) in the order of `params`."""
+        B, H, W, _ = dout.shape
+        dy = dout.to(torch.bfloat16).contiguous()
         gw, gb = [None] * len(self.w), [None] * len(self.w)
         for layer in range(len(self.w) - 1, -1, -1):
             x = self._acts[layer]
@@ -118,8 +116,6 @@ class Corrector:
                 nat.conv_fwd(dy, pack_transposed(self.w[layer]), None, y16=dx, mask=x)
                 dy = dx
         gw[0][:, 3] = 0.0
-        gw[-1][1] = 0.0
-        gb[-1][1] = 0.0
         return gw + gb
 
     def adam(self, grads: list[torch.Tensor], lr: float, beta1=0.9, beta2=0.999, eps=1e-8) -> None:
@@ -247,15 +243,16 @@ def features(newest: torch.Tensor, before: torch.Tensor, c: torch.Tensor):
 
 
 def pulse(pair: GridPair, sim) -> np.ndarray:
-    """A Gaussian pulse sampled at `sim`'s steps, about 12 coarse cells a wavelength."""
-    freq = 1.0 / (12 * pair.coarse.dx[0])
+    """A Gaussian pulse sampled at `sim`'s steps, about 8 coarse cells a wavelength at
+    the slowest speed."""
+    freq = 1.0 / (8 * pair.coarse.dx[0])
     t = np.arange(sim.N) * sim.dt
     return np.exp(-(((t - 1.2 / freq) * freq * math.pi) ** 2))
 
 
 def pulse_end(pair: GridPair) -> int:
     """The coarse step after which the pulse has died out."""
-    freq = 1.0 / (12 * pair.coarse.dx[0])
+    freq = 1.0 / (8 * pair.coarse.dx[0])
     return int(math.ceil(2.6 / freq / pair.coarse.dt))
 
 
@@ -270,8 +267,9 @@ def shot_sources(pair: GridPair, pos) -> tuple[Source, Source]:
 
 
 def training_pairs(pair: GridPair, rng: np.random.Generator, shots: int, windows: int):
-    """(inputs (P, H, W, 4) BF16, targets (P, H, W) FP32 in field scale): fine runs
-    restricted to the coarse grid against coarse runs of EVERY steps from them."""
+    """(inputs (P, H, W, 4) BF16, targets (P, H, W, 2) FP32 in field scale): fine runs
+    restricted to the coarse grid against coarse runs of EVERY steps from them, for both
+    levels the coarse run ends on."""
     Nc = pair.coarse.Nx[0]
     inputs, targets = [], []
     for _ in range(shots):
@@ -285,15 +283,17 @@ def training_pairs(pair: GridPair, rng: np.random.Generator, shots: int, windows
         cdev = torch.as_tensor(c, dtype=torch.float32, device=device())
         # windows after the pulse, which the coarse windows do not inject
         first = pulse_end(pair) + 1
-        starts = sorted(rng.choice(np.arange(first, pair.coarse.N - EVERY - 2), windows,
-                                   replace=False))
+        slots = np.arange(first, pair.coarse.N - EVERY - 2, EVERY + 1)  # windows apart
+        starts = sorted(rng.choice(slots, min(windows, len(slots)), replace=False))
         for n in starts:
             # fine levels after n - 1 and n coarse steps, then after n + EVERY
             fine.march(pair.ratio * (n - 1) - fine.t)
             before = restrict(fine.levels()[0][: pair.fine.Nx[0], : pair.fine.Nx[1]], Nc)
             fine.march(pair.ratio)
             newest = restrict(fine.levels()[0][: pair.fine.Nx[0], : pair.fine.Nx[1]], Nc)
-            fine.march(pair.ratio * EVERY)
+            fine.march(pair.ratio * (EVERY - 1))
+            truth_old = restrict(fine.levels()[0][: pair.fine.Nx[0], : pair.fine.Nx[1]], Nc)
+            fine.march(pair.ratio)
             truth = restrict(fine.levels()[0][: pair.fine.Nx[0], : pair.fine.Nx[1]], Nc)
             coarse.set_levels(newest, before)
             coarse.march(EVERY)
@@ -301,7 +301,8 @@ def training_pairs(pair: GridPair, rng: np.random.Generator, shots: int, windows
             c_new, c_old = c_new[:Nc, :Nc], c_old[:Nc, :Nc]
             x, scale = features(c_new, c_old, cdev)
             inputs.append(x)
-            targets.append(((truth - c_new) / scale).float())
+            targets.append(torch.stack([(truth - c_new) / scale, (truth_old - c_old) / scale],
+                                       dim=-1).float())
     return torch.stack(inputs), torch.stack(targets)
 
 
@@ -328,15 +329,18 @@ def corrected_traces(pair: GridPair, net: Corrector | None, c: np.ndarray, sourc
     run = Stepper(pair.coarse, design_for(pair.coarse, c), source, sensors)
     cdev = torch.as_tensor(c, dtype=torch.float32, device=device())
     estimate = 0.0
+    quiet = pulse_end(pair)  # the corrector was trained on source-free windows
     while run.t < pair.coarse.N:
         run.march(EVERY)
-        if net is None or run.t >= pair.coarse.N:
+        if net is None or run.t >= pair.coarse.N or run.t < quiet:
             continue
         newest, before = run.levels()
         x, scale = features(newest[:Nc, :Nc], before[:Nc, :Nc], cdev)
         delta = net.forward(x[None])[0] * scale
-        estimate = max(estimate, float(delta.norm() / newest[:Nc, :Nc].norm().clamp(min=1e-30)))
-        newest[:Nc, :Nc] += delta
+        estimate = max(estimate,
+                       float(delta[..., 0].norm() / newest[:Nc, :Nc].norm().clamp(min=1e-30)))
+        newest[:Nc, :Nc] += delta[..., 0]
+        before[:Nc, :Nc] += delta[..., 1]
     return run.traces, estimate
 
 

@@ -1244,6 +1244,10 @@ struct cwb_batch {
   int *owner = nullptr, *col = nullptr;
   int nsens = 0;
   int max_steps = 0;
+  // the radius groups of a step run side by side, each on a stream of its own
+  static constexpr int SIDES = CWB_MAX_RADIUS;
+  cudaStream_t side[SIDES] = {};
+  cudaEvent_t step_fork = nullptr, side_done[SIDES] = {};
 };
 
 namespace {
@@ -1359,6 +1363,29 @@ std::vector<Launch> batch_launches(cwb_batch *b, const bool records) {
   return out;
 }
 
+// one step: with several radius groups and the receivers' launch last, the groups run
+// side by side on their own streams, joined before the receivers' launch (which ends the
+// step); otherwise in order
+int batch_step(cwb_batch *b, const std::vector<Launch> &launches, cudaStream_t s) {
+  const int groups = (int)b->groups.size();
+  if (groups < 2 || (int)launches.size() != groups + 1 || groups > cwb_batch::SIDES)
+    return enqueue_step(launches, s);
+  CWB_CUDA(cudaEventRecord(b->step_fork, s));
+  for (int i = 0; i < groups; ++i) {
+    CWB_CUDA(cudaStreamWaitEvent(b->side[i], b->step_fork, 0));
+    const cudaError_t e = launches[i](b->side[i], false);
+    if (e != cudaSuccess)
+      return fail(CWB_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
+    CWB_CUDA(cudaEventRecord(b->side_done[i], b->side[i]));
+    CWB_CUDA(cudaStreamWaitEvent(s, b->side_done[i], 0));
+  }
+  const cudaError_t e = launches.back()(s, true);
+  if (e != cudaSuccess)
+    return fail(CWB_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
+  g_launches += (long long)launches.size();
+  return CWB_OK;
+}
+
 int batch_run(cwb_batch *b, const std::vector<Launch> &launches, const int t0, const int steps,
               const bool graph, cudaStream_t s) {
   CWB_CUDA(cwb::launch_set_counter(b->ctr, t0, s));
@@ -1370,7 +1397,7 @@ int batch_run(cwb_batch *b, const std::vector<Launch> &launches, const int t0, c
     CWB_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     int rc = CWB_OK;
     for (int k = 0; k < GRAPH_STEPS && !rc; ++k)
-      rc = enqueue_step(launches, s);
+      rc = batch_step(b, launches, s);
     const cudaError_t ce = cudaStreamEndCapture(s, &g);
     if (rc)
       return rc;
@@ -1390,7 +1417,7 @@ int batch_run(cwb_batch *b, const std::vector<Launch> &launches, const int t0, c
     cudaGraphExecDestroy(exec);
   }
   for (; done < steps; ++done) {
-    const int rc = enqueue_step(launches, s);
+    const int rc = batch_step(b, launches, s);
     if (rc)
       return rc;
   }
@@ -1432,6 +1459,14 @@ int cwb_batch_destroy(cwb_batch *b) {
   for (cudaEvent_t e : events)
     if (e)
       cudaEventDestroy(e);
+  if (b->step_fork)
+    cudaEventDestroy(b->step_fork);
+  for (int i = 0; i < cwb_batch::SIDES; ++i) {
+    if (b->side_done[i])
+      cudaEventDestroy(b->side_done[i]);
+    if (b->side[i])
+      cudaStreamDestroy(b->side[i]);
+  }
   if (b->lane)
     cudaStreamDestroy(b->lane);
   delete b;
@@ -1481,10 +1516,17 @@ int cwb_batch_create(const cwb_batch_item *items, const int32_t n, cwb_batch **o
       cudaStreamCreateWithFlags(&b->lane, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&b->join, cudaEventDisableTiming) != cudaSuccess ||
-      cudaEventCreate(&b->t_begin) != cudaSuccess || cudaEventCreate(&b->t_end) != cudaSuccess) {
+      cudaEventCreate(&b->t_begin) != cudaSuccess || cudaEventCreate(&b->t_end) != cudaSuccess ||
+      cudaEventCreateWithFlags(&b->step_fork, cudaEventDisableTiming) != cudaSuccess) {
     cwb_batch_destroy(b);
     return fail(CWB_ERR_ALLOC, "batch resources");
   }
+  for (int i = 0; i < cwb_batch::SIDES; ++i)
+    if (cudaStreamCreateWithFlags(&b->side[i], cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->side_done[i], cudaEventDisableTiming) != cudaSuccess) {
+      cwb_batch_destroy(b);
+      return fail(CWB_ERR_ALLOC, "batch streams");
+    }
   cudaMemset(b->ctr, 0, 2 * sizeof(int));
   // the receivers: one table entry per item, one (owner, column) pair per sensor
   std::vector<cwb::BatchRecord<float>> recs(n);
