@@ -537,7 +537,7 @@ def run_ours(args) -> int:
     traffic = profile_traffic(w)
     kernels_2d = two_d_kernels(peak) if args.size == 512 and not args.no_2d and world == 1 else None
     batch = batch_measure() if args.size == 512 and not args.no_batch and world == 1 else None
-    learned = learned_measure() if args.size == 512 and not args.no_learned and world == 1 else None
+    learned = learned_measure() if args.size == 512 and args.learned and world == 1 else None
 
     if world > 1:
         dist.barrier()
@@ -618,7 +618,8 @@ def main(argv=None) -> int:
     parser.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     parser.add_argument("--no-2d", action="store_true", help="skip the 2D kernel measurements")
     parser.add_argument("--no-batch", action="store_true", help="skip the batched 2D march")
-    parser.add_argument("--no-learned", action="store_true", help="skip the learned corrector")
+    parser.add_argument("--learned", action="store_true",
+                        help="also train and time the learned corrector (not yet a gain)")
     args = parser.parse_args(argv)
     if args.impl == "reference":
         return run_reference(args)

@@ -222,14 +222,14 @@ class Stepper:
         """(u^(t-1), u^(t-2)): the newest level and the one before."""
         return self.U[(self.t - 1) % 2], self.U[self.t % 2]
 
-    def set_levels(self, newest: torch.Tensor, before: torch.Tensor) -> None:
-        """Start the march from two given levels at t = 0."""
-        self.t = 0
+    def set_levels(self, newest: torch.Tensor, before: torch.Tensor, t: int = 0) -> None:
+        """Continue the march from two given levels as if `t` steps had been taken."""
+        self.t = t
         n0, n1 = newest.shape
         self.U.zero_()
-        # step 0 reads U[0] as u^(-2) and U[1] as u^(-1)
-        self.U[1, :n0, :n1] = newest
-        self.U[0, :n0, :n1] = before
+        # step t reads U[t % 2] as u^(t-2) and U[(t + 1) % 2] as u^(t-1)
+        self.U[(t + 1) % 2, :n0, :n1] = newest
+        self.U[t % 2, :n0, :n1] = before
 
 
 def features(newest: torch.Tensor, before: torch.Tensor, c: torch.Tensor):
@@ -248,12 +248,6 @@ def pulse(pair: GridPair, sim) -> np.ndarray:
     freq = 1.0 / (8 * pair.coarse.dx[0])
     t = np.arange(sim.N) * sim.dt
     return np.exp(-(((t - 1.2 / freq) * freq * math.pi) ** 2))
-
-
-def pulse_end(pair: GridPair) -> int:
-    """The coarse step after which the pulse has died out."""
-    freq = 1.0 / (8 * pair.coarse.dx[0])
-    return int(math.ceil(2.6 / freq / pair.coarse.dt))
 
 
 def shot_sources(pair: GridPair, pos) -> tuple[Source, Source]:
@@ -277,13 +271,12 @@ def training_pairs(pair: GridPair, rng: np.random.Generator, shots: int, windows
         cf = np.kron(c, np.ones((2, 2)))[: pair.fine.Nx[0], : pair.fine.Nx[1]]
         fine_ind, coarse_ind = design_for(pair.fine, cf), design_for(pair.coarse, c)
         pos = rng.integers(Nc // 4, 3 * Nc // 4, size=2)
-        fine_src, _ = shot_sources(pair, pos)
+        fine_src, coarse_src = shot_sources(pair, pos)
         fine = Stepper(pair.fine, fine_ind, fine_src)
-        coarse = Stepper(pair.coarse, coarse_ind)
+        coarse = Stepper(pair.coarse, coarse_ind, coarse_src)
         cdev = torch.as_tensor(c, dtype=torch.float32, device=device())
-        # windows after the pulse, which the coarse windows do not inject
-        first = pulse_end(pair) + 1
-        slots = np.arange(first, pair.coarse.N - EVERY - 2, EVERY + 1)  # windows apart
+        # windows over the whole run, the source's own injection in the coarse ones
+        slots = np.arange(EVERY, pair.coarse.N - EVERY - 2, EVERY + 1)  # windows apart
         starts = sorted(rng.choice(slots, min(windows, len(slots)), replace=False))
         for n in starts:
             # fine levels after n - 1 and n coarse steps, then after n + EVERY
@@ -295,7 +288,7 @@ def training_pairs(pair: GridPair, rng: np.random.Generator, shots: int, windows
             truth_old = restrict(fine.levels()[0][: pair.fine.Nx[0], : pair.fine.Nx[1]], Nc)
             fine.march(pair.ratio)
             truth = restrict(fine.levels()[0][: pair.fine.Nx[0], : pair.fine.Nx[1]], Nc)
-            coarse.set_levels(newest, before)
+            coarse.set_levels(newest, before, n)
             coarse.march(EVERY)
             c_new, c_old = coarse.levels()
             c_new, c_old = c_new[:Nc, :Nc], c_old[:Nc, :Nc]
@@ -329,10 +322,9 @@ def corrected_traces(pair: GridPair, net: Corrector | None, c: np.ndarray, sourc
     run = Stepper(pair.coarse, design_for(pair.coarse, c), source, sensors)
     cdev = torch.as_tensor(c, dtype=torch.float32, device=device())
     estimate = 0.0
-    quiet = pulse_end(pair)  # the corrector was trained on source-free windows
     while run.t < pair.coarse.N:
         run.march(EVERY)
-        if net is None or run.t >= pair.coarse.N or run.t < quiet:
+        if net is None or run.t >= pair.coarse.N:
             continue
         newest, before = run.levels()
         x, scale = features(newest[:Nc, :Nc], before[:Nc, :Nc], cdev)
