@@ -1,9 +1,10 @@
 // The 2D transposed step of a uniform stiffness, with or without the gradient densities:
 // quads of four fast-axis nodes marching rows, like step2d.cuh.
 //
-// MODE_STEP       lambda^n = 2 lambda^(n+1) - lambda^(n+2) + dt^2/m (W^-1 A^T W lambda^(n+1)),
-//                 the pml transpose gathered in (cuwave adjoint_kernel + pml_adjoint_kernel,
-//                 scalar_sensitivity.cu:388-441, 545-597);
+// MODE_STEP       lambda^n = 2 lambda^(n+1) - lambda^(n+2) + dt^2/m (W^-1 A^T W lambda^(n+1))
+//                 (cuwave adjoint_kernel, scalar_sensitivity.cu:388-441), the pml transpose
+//                 (pml_adjoint_kernel, 545-597) gathered after it by adjoint2d_pml_kernel
+//                 over the nodes within R of a slab;
 // MODE_STEP_GRAD  the same, accumulating g_mass and g_stiff against u^n
 //                 (adjoint_gradient_kernel, scalar_sensitivity.cu:444-515).
 //
@@ -121,14 +122,6 @@ __global__ void __launch_bounds__(A2_THREADS, 4) adjoint2d_kernel(const AdjointP
         xheld |= 1 << i;
     }
     const T mi_derived = (flags & K_DERIVE) ? (T)1 / p.sconst : (T)0;
-    // whether a node of the quad is within R of an axis-1 pml slab (fixed for the thread)
-    const auto reach = [&](const int a, const int N, const int lo_d, const int hi_d) {
-      return (lo_d && a >= 1 && a <= lo_d + R) || (hi_d && a <= N - 2 && a >= N - 1 - (hi_d + R));
-    };
-    bool xreach = false;
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-      xreach |= ((inner >> i) & 1) && reach(xq + i, NF, g.lo[1], g.hi[1]);
     // a field over the quad at row b through the node image along axis 0
     const auto row4 = [&](const T *f, const int b, T *dst) {
       int sg = 1;
@@ -185,7 +178,6 @@ __global__ void __launch_bounds__(A2_THREADS, 4) adjoint2d_kernel(const AdjointP
         tap4(u1, z + R, qu[2 * R - 1]);
       const long long row = (long long)z * s0 + xq;
       const bool zheld = held_row(z);
-      const bool zreach = reach(z, N0, g.lo[0], g.hi[0]);
       const auto ltap = [&](const int j, const int i) -> T { return ql[R + j][i]; };
       const auto utap = [&](const int j, const int i) -> T { return qu[R - 1 + j][i]; };
       // the row's own lambda and u: the queue's centre, or memory on a held wall row
@@ -305,65 +297,6 @@ __global__ void __launch_bounds__(A2_THREADS, 4) adjoint2d_kernel(const AdjointP
           gs4[i] = gs4[i] - p.mf * gsum;
         }
       }
-      if ((flags & K_PML) && (zreach || xreach)) {
-        // the pml transpose gathered from the memories' c+ and c- rows (pml_adjoint_kernel
-        // and pml_tap, scalar_sensitivity.cu:545-597, 237-251), node by node where a
-        // node is within R of a lined axis' slab
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          if (!((inner >> i) & 1))
-            continue;
-          const int A[2] = {z, xq + i};
-          T wcell = (T)1;
-#pragma unroll
-          for (int e = 0; e < 2; ++e)
-            if (A[e] == 1 || A[e] == g.n[e] - 2)
-              wcell *= (T)0.5;
-#pragma unroll 1
-          for (int d = 0; d < 2; ++d) {
-            const int lo_d = g.lo[d], hi_d = g.hi[d];
-            if (!(lo_d + hi_d))
-              continue;
-            const int a = A[d], N = g.n[d];
-            const bool reached = (lo_d && a >= 1 && a <= lo_d + R) ||
-                                 (hi_d && a <= N - 2 && a >= N - 1 - (hi_d + R));
-            if (!reached)
-              continue;
-            const T *mem = p.mem[d];
-            const long long sz = p.memrow[d];
-            const int rows = lo_d + hi_d;
-            const auto tap = [&](const int ai, const int q) -> T {
-              const int r = slab_row(ai, N, lo_d, hi_d);
-              const long long si = d == 0 ? (long long)r * ext + A[1] : (long long)A[0] * rows + r;
-              return mem[3 * sz + si] * plus_tap<T, R>(p.w, q) + mem[4 * sz + si] * minus_tap<T, R>(p.w, q);
-            };
-            T sum = (T)0;
-#pragma unroll 1
-            for (int m = -R; m <= R; ++m)
-              if (slab_row(a + m, N, lo_d, hi_d) >= 0)
-                sum += tap(a + m, -m);
-#pragma unroll 1
-            for (int high = 0; high < 2; ++high) {
-              // the reads past the wall that land on a, folded back, odd on a Dirichlet face
-              const int ghost = high ? 2 * (N - 2) - a : 2 - a;
-              if (high ? ghost < N - 1 : ghost > 0)
-                continue;
-              T fold = (T)0;
-#pragma unroll 1
-              for (int kk = 1; kk <= R; ++kk) {
-                const int ai = high ? N - 1 - kk : kk;
-                if (slab_row(ai, N, lo_d, hi_d) >= 0 && ghost - ai >= -R && ghost - ai <= R)
-                  fold += tap(ai, ghost - ai);
-              }
-              sum += ((g.dir >> (2 * d + high)) & 1) ? -fold : fold;
-            }
-            const T delta = miv[i] * sum / wcell;
-            ln[i] += delta;
-            if constexpr (GR)
-              gm[i] -= p.mf * uc[i] * delta;
-          }
-        }
-      }
       if (inner == 15) {
         store4(l0 + row, ln);
         if constexpr (GR) {
@@ -394,6 +327,110 @@ __global__ void __launch_bounds__(A2_THREADS, 4) adjoint2d_kernel(const AdjointP
             qu[j][i] = qu[j + 1][i];
       }
     }
+  }
+  finish_step(p.ctr, p.flags & K_ADV);
+}
+
+// The nodes the 2D pml transpose reaches: those within R of a lined axis' slab. Rows
+// 1 .. za_lo and za_hi .. N0 - 2 (axis 0) are gathered whole; the rows between them over
+// columns 1 .. xb_lo and xb_hi .. NF - 2 (axis 1). The host merges ranges that meet.
+struct Adj2Reach {
+  int za_lo, za_hi;
+  int xb_lo, xb_hi;
+};
+
+constexpr int A2P_THREADS = 256;
+
+// The pml transpose of the 2D adjoint step, after adjoint2d_kernel has written lambda^n
+// (and g_mass): node by node over the reached nodes, each lined axis in turn, the taps of
+// the memories' c+ and c- rows around the node summed in stencil order, then the reads
+// past the walls that land on it folded back (odd on a Dirichlet face), scaled by 1/m and
+// the wall cells' half weights; lambda^n takes the sum, g_mass its share against u^n
+// (pml_adjoint_kernel and pml_tap, scalar_sensitivity.cu:545-597, 237-251; the order of
+// adjoint_gradient_kernel's update and then pml_adjoint_kernel's, as cuwave launches
+// them).
+template <typename T, int R, int MODE>
+__global__ void __launch_bounds__(A2P_THREADS) adjoint2d_pml_kernel(const AdjointParams<T> p,
+                                                                    const Adj2Reach reach) {
+  constexpr bool GR = MODE == MODE_STEP_GRAD;
+  const Geometry &g = p.g;
+  const int t = step_index(p.ctr);
+  const int N0 = g.n[0], NF = g.n[1], ext = g.ext[1];
+  const int nzlo = reach.za_lo, nzhi = N0 - 1 - reach.za_hi;
+  const long long nA = (long long)(nzlo + nzhi) * (NF - 2);
+  const int nxlo = reach.xb_lo, nxhi = NF - 1 - reach.xb_hi, nx = nxlo + nxhi;
+  const long long nB = (long long)(reach.za_hi - 1 - reach.za_lo) * nx;
+  const long long k = (long long)blockIdx.x * A2P_THREADS + threadIdx.x;
+  int z = -1, x = -1;
+  if (k < nA) {
+    const int r = (int)(k / (NF - 2));
+    z = r < nzlo ? 1 + r : reach.za_hi + (r - nzlo);
+    x = 1 + (int)(k % (NF - 2));
+  } else if (k - nA < nB) {
+    const long long kb = k - nA;
+    z = reach.za_lo + 1 + (int)(kb / nx);
+    const int c = (int)(kb % nx);
+    x = c < nxlo ? 1 + c : reach.xb_hi + (c - nxlo);
+  }
+  if (z >= 0) {
+    T *l0 = level<T>(p.l0, t);
+    const long long row = (long long)z * g.s[0] + x;
+    const T mi = (p.flags & K_DERIVE) ? (T)1 / p.sconst : p.minv[row];
+    const int A[2] = {z, x};
+    T wcell = (T)1;
+#pragma unroll
+    for (int e = 0; e < 2; ++e)
+      if (A[e] == 1 || A[e] == g.n[e] - 2)
+        wcell *= (T)0.5;
+    T ln = l0[row];
+    T gm = GR ? p.g_mass[row] : (T)0;
+    const T uc = GR ? level<T>(p.u1, t)[row] : (T)0;
+#pragma unroll 1
+    for (int d = 0; d < 2; ++d) {
+      const int lo_d = g.lo[d], hi_d = g.hi[d];
+      if (!(lo_d + hi_d))
+        continue;
+      const int a = A[d], N = g.n[d];
+      const bool reached = (lo_d && a >= 1 && a <= lo_d + R) ||
+                           (hi_d && a <= N - 2 && a >= N - 1 - (hi_d + R));
+      if (!reached)
+        continue;
+      const T *mem = p.mem[d];
+      const long long sz = p.memrow[d];
+      const int rows = lo_d + hi_d;
+      const auto tap = [&](const int ai, const int q) -> T {
+        const int r = slab_row(ai, N, lo_d, hi_d);
+        const long long si = d == 0 ? (long long)r * ext + A[1] : (long long)A[0] * rows + r;
+        return mem[3 * sz + si] * plus_tap<T, R>(p.w, q) + mem[4 * sz + si] * minus_tap<T, R>(p.w, q);
+      };
+      T sum = (T)0;
+#pragma unroll
+      for (int m = -R; m <= R; ++m)
+        if (slab_row(a + m, N, lo_d, hi_d) >= 0)
+          sum += tap(a + m, -m);
+#pragma unroll
+      for (int high = 0; high < 2; ++high) {
+        // the reads past the wall that land on a, folded back, odd on a Dirichlet face
+        const int ghost = high ? 2 * (N - 2) - a : 2 - a;
+        if (high ? ghost < N - 1 : ghost > 0)
+          continue;
+        T fold = (T)0;
+#pragma unroll
+        for (int kk = 1; kk <= R; ++kk) {
+          const int ai = high ? N - 1 - kk : kk;
+          if (slab_row(ai, N, lo_d, hi_d) >= 0 && ghost - ai >= -R && ghost - ai <= R)
+            fold += tap(ai, ghost - ai);
+        }
+        sum += ((g.dir >> (2 * d + high)) & 1) ? -fold : fold;
+      }
+      const T delta = mi * sum / wcell;
+      ln += delta;
+      if constexpr (GR)
+        gm -= p.mf * uc * delta;
+    }
+    l0[row] = ln;
+    if constexpr (GR)
+      p.g_mass[row] = gm;
   }
   finish_step(p.ctr, p.flags & K_ADV);
 }

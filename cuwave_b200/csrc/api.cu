@@ -447,6 +447,18 @@ cudaError_t step2d_r(const cwb::StepParams<T> &p, const int R, const bool u, con
 }
 
 template <typename T>
+cudaError_t adjoint2d_pml_r(const cwb::AdjointParams<T> &p, const cwb::Adj2Reach &reach,
+                            const int R, const int mode, const dim3 grid, cudaStream_t s) {
+  switch (R) {
+  case 1: return cwb::adjoint2d_pml_unit<T, 1>(p, reach, mode, grid, s);
+  case 2: return cwb::adjoint2d_pml_unit<T, 2>(p, reach, mode, grid, s);
+  case 3: return cwb::adjoint2d_pml_unit<T, 3>(p, reach, mode, grid, s);
+  case 4: return cwb::adjoint2d_pml_unit<T, 4>(p, reach, mode, grid, s);
+  }
+  return cudaErrorInvalidValue;
+}
+
+template <typename T>
 cudaError_t adjoint2d_r(const cwb::AdjointParams<T> &p, const int R, const int mode,
                         const dim3 grid, cudaStream_t s) {
   switch (R) {
@@ -870,6 +882,30 @@ int translate(cwb_plan *p, const cwb_op &op, const size_t slot, cudaStream_t str
           q.flags |= cwb::K_ADV;
         return adjoint2d_r<T>(q, R, mode, grid, s);
       });
+      if (flags & cwb::K_PML) {
+        // the pml transpose over the nodes within R of a slab: the rows that axis 0's
+        // slabs reach, whole, then the other rows' columns that axis 1's reach
+        const int N0 = g.n[0], NF = g.n[1];
+        cwb::Adj2Reach reach;
+        reach.za_lo = g.lo[0] ? std::min(g.lo[0] + R, N0 - 2) : 0;
+        reach.za_hi = g.hi[0] ? std::max(N0 - 1 - (g.hi[0] + R), 1) : N0 - 1;
+        if (reach.za_lo >= reach.za_hi)
+          reach.za_lo = N0 - 2, reach.za_hi = N0 - 1;
+        reach.xb_lo = g.lo[1] ? std::min(g.lo[1] + R, NF - 2) : 0;
+        reach.xb_hi = g.hi[1] ? std::max(NF - 1 - (g.hi[1] + R), 1) : NF - 1;
+        if (reach.xb_lo >= reach.xb_hi)
+          reach.xb_lo = NF - 2, reach.xb_hi = NF - 1;
+        const long long nodes =
+            (long long)(reach.za_lo + N0 - 1 - reach.za_hi) * (NF - 2) +
+            (long long)(reach.za_hi - 1 - reach.za_lo) * (reach.xb_lo + NF - 1 - reach.xb_hi);
+        const dim3 pgrid((unsigned)std::max<long long>(1, (nodes + cwb::A2P_THREADS - 1) / cwb::A2P_THREADS));
+        out.push_back([ap, reach, R, mode, pgrid](cudaStream_t s, bool adv) {
+          cwb::AdjointParams<T> q = ap;
+          if (adv)
+            q.flags |= cwb::K_ADV;
+          return adjoint2d_pml_r<T>(q, reach, R, mode, pgrid, s);
+        });
+      }
       return CWB_OK;
     }
     dim3 grid;

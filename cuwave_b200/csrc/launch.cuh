@@ -49,6 +49,11 @@ bool step2d_built();
 // MODE_STEP_GRAD, 128 threads a block
 template <typename T, int R>
 cudaError_t adjoint2d_unit(const AdjointParams<T> &p, int mode, dim3 grid, cudaStream_t stream);
+struct Adj2Reach;
+// its pml transpose, a launch after it over the nodes within R of a slab
+template <typename T, int R>
+cudaError_t adjoint2d_pml_unit(const AdjointParams<T> &p, const Adj2Reach &reach, int mode,
+                               dim3 grid, cudaStream_t stream);
 
 template <typename T>
 struct March2Params;

@@ -176,6 +176,22 @@ cudaError_t adjoint2d_unit(const AdjointParams<T> &p, const int mode, const dim3
     return cudaGetLastError();
   }
 }
+
+template <typename T, int R>
+cudaError_t adjoint2d_pml_unit(const AdjointParams<T> &p, const Adj2Reach &reach, const int mode,
+                               const dim3 grid, cudaStream_t s) {
+  if constexpr (!Adj2Shape<T, R>::SUPPORTED) {
+    return cudaErrorInvalidValue;
+  } else {
+    if (mode == MODE_STEP_GRAD)
+      adjoint2d_pml_kernel<T, R, MODE_STEP_GRAD><<<grid, A2P_THREADS, 0, s>>>(p, reach);
+    else if (mode == MODE_STEP)
+      adjoint2d_pml_kernel<T, R, MODE_STEP><<<grid, A2P_THREADS, 0, s>>>(p, reach);
+    else
+      return cudaErrorInvalidValue;
+    return cudaGetLastError();
+  }
+}
 #endif
 
 #if CWB_NDIM == 3
@@ -226,6 +242,9 @@ template cudaError_t march2d_unit<CWB_REAL, CWB_RADIUS>(const March2Params<CWB_R
                                                          cudaStream_t);
 template cudaError_t adjoint2d_unit<CWB_REAL, CWB_RADIUS>(const AdjointParams<CWB_REAL> &, int,
                                                           dim3, cudaStream_t);
+template cudaError_t adjoint2d_pml_unit<CWB_REAL, CWB_RADIUS>(const AdjointParams<CWB_REAL> &,
+                                                              const Adj2Reach &, int, dim3,
+                                                              cudaStream_t);
 #endif
 #if CWB_NDIM == 3
 template cudaError_t step3d_unit<CWB_REAL, CWB_RADIUS>(const Step3Params<CWB_REAL> &, bool, dim3,
