@@ -8,9 +8,11 @@
 // MODE_STEP_GRAD  the same, accumulating g_mass and g_stiff against u^n
 //                 (adjoint_gradient_kernel, scalar_sensitivity.cu:444-515).
 //
-// A thread owns a quad and marches a chunk of rows, keeping lambda^(n+1) over rows
-// z-R .. z+R and u^n over rows z-R+1 .. z+R in register queues (the axis-0 taps) and
-// reading the quad's axis-1 runs of 4 + 2H values as 16-byte rows. The taps read through
+// A thread owns a quad and marches a chunk of rows, reading the axis-0 taps (lambda^(n+1)
+// over rows z-R .. z+R, u^n over rows z-R+1 .. z+R) row by row as 16-byte rows of its
+// column, which the rows before brought into L1 (register queues of them measured
+// slower: their 68 registers and shifts cost more than the L1 reads), and the quad's
+// axis-1 runs of 4 + 2H values. The taps read through
 // the node image (a stored ghost is never read; lambda and u odd across a Dirichlet face)
 // and read zero on a held wall node, as cuwave's `reflected` does
 // (scalar_sensitivity.cu:177-184). Along axis 1 the quad shares its runs' first
@@ -27,6 +29,7 @@
 namespace cwb {
 
 constexpr int A2_THREADS = 128;
+constexpr int A2_MIN_BLOCKS = 4;  // blocks an SM (128 registers a thread)
 
 template <typename T, int R>
 struct Adj2Shape {
@@ -90,7 +93,7 @@ __device__ __forceinline__ void image_run(T *xr, const T *row, const int xq, con
 }
 
 template <typename T, int R, int MODE>
-__global__ void __launch_bounds__(A2_THREADS, 4) adjoint2d_kernel(const AdjointParams<T> p) {
+__global__ void __launch_bounds__(A2_THREADS, A2_MIN_BLOCKS) adjoint2d_kernel(const AdjointParams<T> p) {
   using S = Adj2Shape<T, R>;
   static_assert(S::SUPPORTED && MODE != MODE_GRAD, "the 2D quad adjoint: float, radius <= 4");
   constexpr bool GR = MODE == MODE_STEP_GRAD;
@@ -146,52 +149,83 @@ __global__ void __launch_bounds__(A2_THREADS, 4) adjoint2d_kernel(const AdjointP
           dst[i] = (T)0;
       }
     };
-    // queues: lambda rows z-R .. z+R, u rows z-R+1 .. z+R; the plain D+ of u at the row
-    // before (this row's D-), which reads u row c0 - R once
-    T ql[2 * R + 1][4], qu[2 * R][4], dmz[4];
-#pragma unroll
-    for (int j = 0; j < 2 * R; ++j)
-      tap4(l1, c0 - R + j, ql[j]);
+    // The axis-0 taps are read row by row as the march needs them (the thread read the
+    // same rows of its column in the rows before, so they come from L1): lambda rows
+    // z-R .. z+R and u rows z-R+1 .. z+R. dmz carries the plain D+ of u at the row before
+    // (this row's D-); the first row's reads u row c0 - R once.
+    T dmz[4];
     if constexpr (GR) {
-      T first[4];
-      tap4(u1, c0 - R, first);
-#pragma unroll
-      for (int j = 0; j < 2 * R - 1; ++j)
-        tap4(u1, c0 - R + 1 + j, qu[j]);
-      const auto utap = [&](const int j, const int i) -> T {
-        return j == -R + 1 ? first[i] : qu[R - 2 + j][i];
-      };
+      T uc[4], a[4], b[4];
+      tap4(u1, c0 - 1, uc);
+      tap4(u1, c0, a);
       // (u on a held wall row is zero, so its tap is its centre)
 #pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        const T uc = utap(0, i);
-        T d = p.w[0] * (utap(1, i) - uc);
+      for (int i = 0; i < 4; ++i)
+        dmz[i] = p.w[0] * (a[i] - uc[i]);
 #pragma unroll
-        for (int kk = 2; kk <= R; ++kk)
-          d += p.w[kk - 1] * (utap(kk, i) - utap(1 - kk, i));
-        dmz[i] = d;
+      for (int kk = 2; kk <= R; ++kk) {
+        tap4(u1, c0 - 1 + kk, a);
+        tap4(u1, c0 - kk, b);
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+          dmz[i] += p.w[kk - 1] * (a[i] - b[i]);
       }
     }
     for (int z = c0; z < c1; ++z) {
-      tap4(l1, z + R, ql[2 * R]);
-      if constexpr (GR)
-        tap4(u1, z + R, qu[2 * R - 1]);
       const long long row = (long long)z * s0 + xq;
       const bool zheld = held_row(z);
-      const auto ltap = [&](const int j, const int i) -> T { return ql[R + j][i]; };
-      const auto utap = [&](const int j, const int i) -> T { return qu[R - 1 + j][i]; };
-      // the row's own lambda and u: the queue's centre, or memory on a held wall row
+      // the row's own lambda and u, as stored (a held wall row's own value is not the
+      // zero its taps read)
       T lcz[4], ucz[4];
-      if (!zheld) {
+      row4(l1, z, lcz);
+      if constexpr (GR)
+        row4(u1, z, ucz);
+      // axis 0: the per-node differences of lambda, rows z +- 1 .. z +- R in turn; the
+      // first rows on either side kept for the stiffness densities
+      T div0[4], lp1[4], lm1[4];
+      {
+        T lh[4], ll[4];
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
-          lcz[i] = ql[R][i];
-          ucz[i] = GR ? qu[R - 1][i] : (T)0;
+          div0[i] = (T)0;
+          lh[i] = ll[i] = lcz[i];
         }
-      } else {
-        row4(l1, z, lcz);
-        if constexpr (GR)
-          row4(u1, z, ucz);
+#pragma unroll
+        for (int j = 1; j <= R; ++j) {
+          T hi[4], lo[4];
+          tap4(l1, z + j, hi);
+          tap4(l1, z - j, lo);
+          if (j == 1) {
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+              lp1[i] = hi[i];
+              lm1[i] = lo[i];
+            }
+          }
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            div0[i] += p.w[j - 1] * (gg * (hi[i] - lh[i]) - gg * (ll[i] - lo[i]));
+            lh[i] = hi[i];
+            ll[i] = lo[i];
+          }
+        }
+      }
+      // the plain D+ of u along axis 0 at this row
+      T dpz[4];
+      if constexpr (GR) {
+        T a[4], b[4];
+        tap4(u1, z + 1, a);
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+          dpz[i] = p.w[0] * (a[i] - ucz[i]);
+#pragma unroll
+        for (int kk = 2; kk <= R; ++kk) {
+          tap4(u1, z + kk, a);
+          tap4(u1, z + 1 - kk, b);
+#pragma unroll
+          for (int i = 0; i < 4; ++i)
+            dpz[i] += p.w[kk - 1] * (a[i] - b[i]);
+        }
       }
       // the axis-1 runs through the node image, zero on a held wall node
       T lr[XR], ur[XR];
@@ -235,18 +269,6 @@ __global__ void __launch_bounds__(A2_THREADS, 4) adjoint2d_kernel(const AdjointP
         uc[i] = GR ? ucz[i] : (T)0;
         const bool held = zheld || ((xheld >> i) & 1);
         const T lw = held ? (T)0 : lc[i];
-        // axis 0: the per-node form
-        T div0 = (T)0;
-        {
-          T lh = lc[i], ll = lc[i];
-#pragma unroll
-          for (int j = 1; j <= R; ++j) {
-            const T lh1 = ltap(j, i), ll1 = ltap(-j, i);
-            div0 += p.w[j - 1] * (gg * (lh1 - lh) - gg * (ll - ll1));
-            lh = lh1;
-            ll = ll1;
-          }
-        }
         // axis 1: shared differences, or the per-node form on a held wall node
         const int c = H + i;
         T div1 = (T)0;
@@ -265,17 +287,13 @@ __global__ void __launch_bounds__(A2_THREADS, 4) adjoint2d_kernel(const AdjointP
           }
         }
         T div_l = (T)0;
-        div_l += p.f[0] * div0;
+        div_l += p.f[0] * div0[i];
         div_l += p.f[1] * div1;
         T gsum = (T)0;
         if constexpr (GR) {
           // the stiffness densities (stiffness_gradient_taps), axis 0 then axis 1
-          T dpz = p.w[0] * (utap(1, i) - uc[i]);
-#pragma unroll
-          for (int kk = 2; kk <= R; ++kk)
-            dpz += p.w[kk - 1] * (utap(kk, i) - utap(1 - kk, i));
-          const T sd0 = p.f[0] * (dg * dpz * (ltap(1, i) - lw) + dg * dmz[i] * (lw - ltap(-1, i)));
-          dmz[i] = dpz;
+          const T sd0 = p.f[0] * (dg * dpz[i] * (lp1[i] - lw) + dg * dmz[i] * (lw - lm1[i]));
+          dmz[i] = dpz[i];
           const T sd1 = p.f[1] * (dg * dpx[i + 1] * (lr[c + 1] - lw) + dg * dpx[i] * (lw - lr[c - 1]));
           gsum += sd0;
           gsum += sd1;
@@ -313,18 +331,6 @@ __global__ void __launch_bounds__(A2_THREADS, 4) adjoint2d_kernel(const AdjointP
               p.g_stiff[row + i] = gs4[i];
             }
           }
-      }
-#pragma unroll
-      for (int j = 0; j < 2 * R; ++j)
-#pragma unroll
-        for (int i = 0; i < 4; ++i)
-          ql[j][i] = ql[j + 1][i];
-      if constexpr (GR) {
-#pragma unroll
-        for (int j = 0; j < 2 * R - 1; ++j)
-#pragma unroll
-          for (int i = 0; i < 4; ++i)
-            qu[j][i] = qu[j + 1][i];
       }
     }
   }

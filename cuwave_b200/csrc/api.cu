@@ -868,12 +868,12 @@ int translate(cwb_plan *p, const cwb_op &op, const size_t slot, cudaStream_t str
         (mode != cwb::MODE_STEP_GRAD ||
          (aligned16(op.c.base, op.c.stride) && aligned16(op.g_mass, 0) && aligned16(op.g_stiff, 0))) &&
         ((flags & cwb::K_DERIVE) || aligned16(ap.minv, 0)) && g.n[0] >= 3 * R && g.n[1] >= 3 * R) {
-      // short chunks: the adjoint's rows are long dependent chains, so about six blocks
-      // an SM of short marches keep more of them in flight than long ones (measured on
-      // 2048^2 with the pml gathered apart: 9 rows 116 us a step, 2 rows 124 us)
+      // the shortest chunks that fit the grid in one wave of resident blocks: a partial
+      // second wave idles most SMs for its length (measured on 2048^2 with the pml
+      // gathered apart: 14 rows, one wave, 97 us a step; 9 rows, 1.5 waves, 110 us)
       const long long rows = g.n[0] - 2, quads = (g.n[1] - 2) / 4 + 1;
-      const long long want = (long long)p->sms * 6 * cwb::A2_THREADS;
-      const int chunk = (int)std::max<long long>(1, std::min<long long>(rows, rows * quads / want));
+      const long long wave = (long long)p->sms * cwb::A2_MIN_BLOCKS * cwb::A2_THREADS;
+      const int chunk = (int)std::min<long long>(rows, (rows * quads + wave - 1) / wave);
       ap.chunk = p->chunk_override > 0 ? p->chunk_override : std::max(2, chunk);
       const long long threads = quads * ((rows + ap.chunk - 1) / ap.chunk);
       const dim3 grid((unsigned)((threads + cwb::A2_THREADS - 1) / cwb::A2_THREADS));
