@@ -406,6 +406,45 @@ def batch_measure(count: int = 64, steps: int = 300) -> dict:
     return out
 
 
+def shots_measure(count: int = 96, steps: int = 2000, n: int = 1024) -> dict:
+    """Config 3a: `count` shots on a shared n^2 grid (config 0's blob speeds, radius 4),
+    sources evenly spaced along the top, 256 receivers 50 cells down, `steps` steps;
+    the summed misfit gradient (a forward with its history and an adjoint per shot, in
+    turn) timed with CUDA events after one warm-up shot. Observed data are zero, so the
+    misfit is the traces' energy."""
+    import torch
+
+    from cuwave_b200 import AcousticWave, ricker
+    from cuwave_b200.stencils import stable_dt
+    from cuwave_b200.utils import Sensors, misfit_gradient, shots
+
+    c = blob_speed(n)
+    kappa2 = 0.25
+    dt = 0.5 * stable_dt((1.0, 1.0), float(c.max()), 8, "optimized")
+    sim = AcousticWave(Nx=(n, n), dx=(1.0, 1.0), N=steps, dt=dt, precision="float32",
+                       space_order=8, rho1=1.0, rho2=1.0, kappa1=1.0, kappa2=kappa2)
+    ind = np.zeros(sim.Nx_padded, np.float32)
+    ind[:n, :n] = (1.0 / c**2 - 1.0) / (1.0 / kappa2 - 1.0)
+    # about 20 points a wavelength at the peak frequency
+    signal = ricker(np.arange(steps) * dt, 1.0, float(c.min()) / 20.0)
+    coords = np.stack([np.full(count, 10.0), np.linspace(20.0, n - 21.0, count)], axis=1)
+    sources = shots(sim, coords, signal)
+    sensors = Sensors(sim, np.stack([np.full(256, 50.0), np.linspace(20.0, n - 21.0, 256)], axis=1))
+    observed = [torch.zeros((steps, 256), dtype=torch.float32, device="cuda")] * count
+    misfit_gradient(sim, sources[:1], ind, sensors, observed[:1])
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    cost, gradient = misfit_gradient(sim, sources, ind, sensors, observed)
+    e1.record()
+    torch.cuda.synchronize()
+    seconds = e0.elapsed_time(e1) / 1e3
+    updates = 2 * count * steps * (n - 2) ** 2  # forward and adjoint
+    return {"shots": count, "steps": steps, "grid": [n, n], "space_order": 8,
+            "receivers": 256, "in_turn_s": seconds, "shots_per_s": count / seconds,
+            "gpts": updates / seconds / 1e9, "finite": bool(np.isfinite(cost))}
+
+
 def learned_measure(coarse_nodes: int = 256, coarse_steps: int = 600) -> dict:
     """Config 4 at a reduced size: the corrector trained on pairs the plain solver makes,
     then on held-out speed models the fine solve, the plain coarse solve and the corrected
@@ -544,6 +583,7 @@ def run_ours(args) -> int:
     traffic = profile_traffic(w)
     kernels_2d = two_d_kernels(peak) if args.size == 512 and not args.no_2d and world == 1 else None
     batch = batch_measure() if args.size == 512 and not args.no_batch and world == 1 else None
+    shots_2d = shots_measure() if args.size == 512 and not args.no_batch and world == 1 else None
     learned = learned_measure() if args.size == 512 and args.learned and world == 1 else None
 
     if world > 1:
@@ -569,6 +609,7 @@ def run_ours(args) -> int:
         "kernel_updates_per_s": interior_updates(w) / (kernel_ms / 1e3) / 1e9,
         "kernels_2d": kernels_2d,
         "batch_2d": batch,
+        "shots_2d": shots_2d,
         "learned": learned,
     }
     print(json.dumps(line))
