@@ -218,6 +218,10 @@ def test_quad_2d_step_by_step_on_a_large_grid():
     (2, 3, 0b1001, 4, False, (67, 91)), (2, 4, 0b0110, 5, False, (75, 139)),
     (2, 4, 0b0000, 0, True, (67, 91)), (2, 4, 0b1111, 0, False, (59, 101)),
     (3, 2, 0b100110, 3, False, (23, 21, 27)),
+    # the narrowest grids a pml allows (its width + R on both sides leaves one interior
+    # node): the transpose's gathered rows and columns leave one row or a few columns
+    (2, 4, 0b0110, 6, False, (11, 13)), (2, 3, 0b1001, 5, False, (9, 61)),
+    (2, 2, 0b0101, 4, False, (53, 7)), (2, 1, 0b0000, 3, False, (41, 37)),
 ])
 def test_uniform_sensitivity_matches_oracle(ndim, R, dirichlet, pml, damping, Nx):
     """sensitivity of a uniform stiffness (the quad adjoint in 2D) on grids of many row
