@@ -391,7 +391,7 @@ __global__ void __launch_bounds__(A2P_THREADS) adjoint2d_pml_kernel(const Adjoin
     T ln = l0[row];
     T gm = GR ? p.g_mass[row] : (T)0;
     const T uc = GR ? level<T>(p.u1, t)[row] : (T)0;
-#pragma unroll 1
+#pragma unroll
     for (int d = 0; d < 2; ++d) {
       const int lo_d = g.lo[d], hi_d = g.hi[d];
       if (!(lo_d + hi_d))
@@ -416,7 +416,11 @@ __global__ void __launch_bounds__(A2P_THREADS) adjoint2d_pml_kernel(const Adjoin
           sum += tap(a + m, -m);
 #pragma unroll
       for (int high = 0; high < 2; ++high) {
-        // the reads past the wall that land on a, folded back, odd on a Dirichlet face
+        // the reads past the wall that land on a, folded back, odd on a Dirichlet face;
+        // none reaches a node more than R + 1 from the wall (skipping its zero fold
+        // leaves the sum's bits as they are: it starts at +0 and cannot turn -0)
+        if (high ? a < N - 2 - R : a > R + 1)
+          continue;
         const int ghost = high ? 2 * (N - 2) - a : 2 - a;
         if (high ? ghost < N - 1 : ghost > 0)
           continue;
