@@ -23,6 +23,8 @@
 // (scalar_sensitivity.cu:119-154).
 #pragma once
 
+#include <type_traits>
+
 #include "adjoint.cuh"
 #include "step.cuh"
 
@@ -171,168 +173,190 @@ __global__ void __launch_bounds__(A2_THREADS, A2_MIN_BLOCKS) adjoint2d_kernel(co
           dmz[i] += p.w[kk - 1] * (a[i] - b[i]);
       }
     }
-    for (int z = c0; z < c1; ++z) {
-      const long long row = (long long)z * s0 + xq;
-      const bool zheld = held_row(z);
-      // the row's own lambda and u, as stored (a held wall row's own value is not the
-      // zero its taps read)
-      T lcz[4], ucz[4];
-      row4(l1, z, lcz);
-      if constexpr (GR)
-        row4(u1, z, ucz);
-      // axis 0: the per-node differences of lambda, rows z +- 1 .. z +- R in turn; the
-      // first rows on either side kept for the stiffness densities
-      T div0[4], lp1[4], lm1[4];
-      {
-        T lh[4], ll[4];
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          div0[i] = (T)0;
-          lh[i] = ll[i] = lcz[i];
-        }
-#pragma unroll
-        for (int j = 1; j <= R; ++j) {
-          T hi[4], lo[4];
-          tap4(l1, z + j, hi);
-          tap4(l1, z - j, lo);
-          if (j == 1) {
-#pragma unroll
-            for (int i = 0; i < 4; ++i) {
-              lp1[i] = hi[i];
-              lm1[i] = lo[i];
-            }
-          }
-#pragma unroll
+    // Rows two or more from either wall read their taps as stored: a chunk whose taps
+    // all lie there marches without the wall logic (the same values, fewer instructions)
+    const bool plain = c0 - R >= 2 && c1 - 1 + R <= N0 - 3;
+    const auto march = [&](auto plain_tag) {
+      constexpr bool PLAIN = decltype(plain_tag)::value;
+      const auto tapz = [&](const T *f, const int b, T *dst) {
+        if constexpr (PLAIN)
+          load4(dst, f + (long long)b * s0 + xq);
+        else
+          tap4(f, b, dst);
+      };
+      const auto rowz = [&](const T *f, const int b, T *dst) {
+        if constexpr (PLAIN)
+          load4(dst, f + (long long)b * s0 + xq);
+        else
+          row4(f, b, dst);
+      };
+      for (int z = c0; z < c1; ++z) {
+        const long long row = (long long)z * s0 + xq;
+        const bool zheld = held_row(z);
+        // the row's own lambda and u, as stored (a held wall row's own value is not the
+        // zero its taps read)
+        T lcz[4], ucz[4];
+        rowz(l1, z, lcz);
+        if constexpr (GR)
+          rowz(u1, z, ucz);
+        // axis 0: the per-node differences of lambda, rows z +- 1 .. z +- R in turn; the
+        // first rows on either side kept for the stiffness densities
+        T div0[4], lp1[4], lm1[4];
+        {
+          T lh[4], ll[4];
+  #pragma unroll
           for (int i = 0; i < 4; ++i) {
-            div0[i] += p.w[j - 1] * (gg * (hi[i] - lh[i]) - gg * (ll[i] - lo[i]));
-            lh[i] = hi[i];
-            ll[i] = lo[i];
+            div0[i] = (T)0;
+            lh[i] = ll[i] = lcz[i];
           }
-        }
-      }
-      // the plain D+ of u along axis 0 at this row
-      T dpz[4];
-      if constexpr (GR) {
-        T a[4], b[4];
-        tap4(u1, z + 1, a);
-#pragma unroll
-        for (int i = 0; i < 4; ++i)
-          dpz[i] = p.w[0] * (a[i] - ucz[i]);
-#pragma unroll
-        for (int kk = 2; kk <= R; ++kk) {
-          tap4(u1, z + kk, a);
-          tap4(u1, z + 1 - kk, b);
-#pragma unroll
-          for (int i = 0; i < 4; ++i)
-            dpz[i] += p.w[kk - 1] * (a[i] - b[i]);
-        }
-      }
-      // the axis-1 runs through the node image, zero on a held wall node
-      T lr[XR], ur[XR];
-      image_run<T, XR, H>(lr, l1 + row, xq, NF, ext, dirF);
-      if constexpr (GR)
-        image_run<T, XR, H>(ur, u1 + row, xq, NF, ext, dirF);
-      // shared along axis 1: g times the first differences of lambda, the plain D+ of u
-      T ge[XR];
-#pragma unroll
-      for (int c = H - R + 1; c <= H + 3 + R; ++c)
-        ge[c] = gg * (lr[c] - lr[c - 1]);
-      T dpx[5];
-      if constexpr (GR) {
-#pragma unroll
-        for (int j = 0; j < 5; ++j) {
-          const int c = H - 1 + j;
-          T d = p.w[0] * (ur[c + 1] - ur[c]);
-#pragma unroll
-          for (int kk = 2; kk <= R; ++kk)
-            d += p.w[kk - 1] * (ur[c + kk] - ur[c + 1 - kk]);
-          dpx[j] = d;
-        }
-      }
-      T ln[4], gm[4], gs4[4];
-      T lov[4], miv[4], uc[4], lc[4];
-      load4(lov, l0 + row);
-      if (flags & K_DERIVE) {
-#pragma unroll
-        for (int i = 0; i < 4; ++i)
-          miv[i] = mi_derived;
-      } else {
-        load4(miv, p.minv + row);
-      }
-      if constexpr (GR) {
-        load4(gm, p.g_mass + row);
-        load4(gs4, p.g_stiff + row);
-      }
-#pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        lc[i] = lcz[i];
-        uc[i] = GR ? ucz[i] : (T)0;
-        const bool held = zheld || ((xheld >> i) & 1);
-        const T lw = held ? (T)0 : lc[i];
-        // axis 1: shared differences, or the per-node form on a held wall node
-        const int c = H + i;
-        T div1 = (T)0;
-        if (!((xheld >> i) & 1)) {
-#pragma unroll
-          for (int j = 1; j <= R; ++j)
-            div1 += p.w[j - 1] * (ge[c + j] - ge[c - j + 1]);
-        } else {
-          T lh = lc[i], ll = lc[i];
-#pragma unroll
+  #pragma unroll
           for (int j = 1; j <= R; ++j) {
-            const T lh1 = lr[c + j], ll1 = lr[c - j];
-            div1 += p.w[j - 1] * (gg * (lh1 - lh) - gg * (ll - ll1));
-            lh = lh1;
-            ll = ll1;
-          }
-        }
-        T div_l = (T)0;
-        div_l += p.f[0] * div0[i];
-        div_l += p.f[1] * div1;
-        T gsum = (T)0;
-        if constexpr (GR) {
-          // the stiffness densities (stiffness_gradient_taps), axis 0 then axis 1
-          const T sd0 = p.f[0] * (dg * dpz[i] * (lp1[i] - lw) + dg * dmz[i] * (lw - lm1[i]));
-          dmz[i] = dpz[i];
-          const T sd1 = p.f[1] * (dg * dpx[i + 1] * (lr[c + 1] - lw) + dg * dpx[i] * (lw - lr[c - 1]));
-          gsum += sd0;
-          gsum += sd1;
-        }
-        const T lo = lov[i], mi = miv[i];
-        T v;
-        if (flags & K_DAMP) {
-          const T dmp = ((inner >> i) & 1) ? p.damping[row + i] : (T)0;
-          const T beta = (T)0.5 * mi * dmp * p.dt;
-          v = ((T)2 * lc[i] - lo * ((T)1 - beta) + mi * div_l) / ((T)1 + beta);
-        } else {
-          v = -lo + (T)2 * lc[i] + mi * div_l;
-        }
-        if (held)
-          v = (T)0;
-        ln[i] = v;
-        if constexpr (GR) {
-          gm[i] = gm[i] - p.mf * uc[i] * (v - (T)2 * lc[i] + lo);
-          gs4[i] = gs4[i] - p.mf * gsum;
-        }
-      }
-      if (inner == 15) {
-        store4(l0 + row, ln);
-        if constexpr (GR) {
-          store4(p.g_mass + row, gm);
-          store4(p.g_stiff + row, gs4);
-        }
-      } else {
-#pragma unroll
-        for (int i = 0; i < 4; ++i)
-          if ((inner >> i) & 1) {
-            l0[row + i] = ln[i];
-            if constexpr (GR) {
-              p.g_mass[row + i] = gm[i];
-              p.g_stiff[row + i] = gs4[i];
+            T hi[4], lo[4];
+            tapz(l1, z + j, hi);
+            tapz(l1, z - j, lo);
+            if (j == 1) {
+  #pragma unroll
+              for (int i = 0; i < 4; ++i) {
+                lp1[i] = hi[i];
+                lm1[i] = lo[i];
+              }
+            }
+  #pragma unroll
+            for (int i = 0; i < 4; ++i) {
+              div0[i] += p.w[j - 1] * (gg * (hi[i] - lh[i]) - gg * (ll[i] - lo[i]));
+              lh[i] = hi[i];
+              ll[i] = lo[i];
             }
           }
+        }
+        // the plain D+ of u along axis 0 at this row
+        T dpz[4];
+        if constexpr (GR) {
+          T a[4], b[4];
+          tapz(u1, z + 1, a);
+  #pragma unroll
+          for (int i = 0; i < 4; ++i)
+            dpz[i] = p.w[0] * (a[i] - ucz[i]);
+  #pragma unroll
+          for (int kk = 2; kk <= R; ++kk) {
+            tapz(u1, z + kk, a);
+            tapz(u1, z + 1 - kk, b);
+  #pragma unroll
+            for (int i = 0; i < 4; ++i)
+              dpz[i] += p.w[kk - 1] * (a[i] - b[i]);
+          }
+        }
+        // the axis-1 runs through the node image, zero on a held wall node
+        T lr[XR], ur[XR];
+        image_run<T, XR, H>(lr, l1 + row, xq, NF, ext, dirF);
+        if constexpr (GR)
+          image_run<T, XR, H>(ur, u1 + row, xq, NF, ext, dirF);
+        // shared along axis 1: g times the first differences of lambda, the plain D+ of u
+        T ge[XR];
+  #pragma unroll
+        for (int c = H - R + 1; c <= H + 3 + R; ++c)
+          ge[c] = gg * (lr[c] - lr[c - 1]);
+        T dpx[5];
+        if constexpr (GR) {
+  #pragma unroll
+          for (int j = 0; j < 5; ++j) {
+            const int c = H - 1 + j;
+            T d = p.w[0] * (ur[c + 1] - ur[c]);
+  #pragma unroll
+            for (int kk = 2; kk <= R; ++kk)
+              d += p.w[kk - 1] * (ur[c + kk] - ur[c + 1 - kk]);
+            dpx[j] = d;
+          }
+        }
+        T ln[4], gm[4], gs4[4];
+        T lov[4], miv[4], uc[4], lc[4];
+        load4(lov, l0 + row);
+        if (flags & K_DERIVE) {
+  #pragma unroll
+          for (int i = 0; i < 4; ++i)
+            miv[i] = mi_derived;
+        } else {
+          load4(miv, p.minv + row);
+        }
+        if constexpr (GR) {
+          load4(gm, p.g_mass + row);
+          load4(gs4, p.g_stiff + row);
+        }
+  #pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          lc[i] = lcz[i];
+          uc[i] = GR ? ucz[i] : (T)0;
+          const bool held = zheld || ((xheld >> i) & 1);
+          const T lw = held ? (T)0 : lc[i];
+          // axis 1: shared differences, or the per-node form on a held wall node
+          const int c = H + i;
+          T div1 = (T)0;
+          if (!((xheld >> i) & 1)) {
+  #pragma unroll
+            for (int j = 1; j <= R; ++j)
+              div1 += p.w[j - 1] * (ge[c + j] - ge[c - j + 1]);
+          } else {
+            T lh = lc[i], ll = lc[i];
+  #pragma unroll
+            for (int j = 1; j <= R; ++j) {
+              const T lh1 = lr[c + j], ll1 = lr[c - j];
+              div1 += p.w[j - 1] * (gg * (lh1 - lh) - gg * (ll - ll1));
+              lh = lh1;
+              ll = ll1;
+            }
+          }
+          T div_l = (T)0;
+          div_l += p.f[0] * div0[i];
+          div_l += p.f[1] * div1;
+          T gsum = (T)0;
+          if constexpr (GR) {
+            // the stiffness densities (stiffness_gradient_taps), axis 0 then axis 1
+            const T sd0 = p.f[0] * (dg * dpz[i] * (lp1[i] - lw) + dg * dmz[i] * (lw - lm1[i]));
+            dmz[i] = dpz[i];
+            const T sd1 = p.f[1] * (dg * dpx[i + 1] * (lr[c + 1] - lw) + dg * dpx[i] * (lw - lr[c - 1]));
+            gsum += sd0;
+            gsum += sd1;
+          }
+          const T lo = lov[i], mi = miv[i];
+          T v;
+          if (flags & K_DAMP) {
+            const T dmp = ((inner >> i) & 1) ? p.damping[row + i] : (T)0;
+            const T beta = (T)0.5 * mi * dmp * p.dt;
+            v = ((T)2 * lc[i] - lo * ((T)1 - beta) + mi * div_l) / ((T)1 + beta);
+          } else {
+            v = -lo + (T)2 * lc[i] + mi * div_l;
+          }
+          if (held)
+            v = (T)0;
+          ln[i] = v;
+          if constexpr (GR) {
+            gm[i] = gm[i] - p.mf * uc[i] * (v - (T)2 * lc[i] + lo);
+            gs4[i] = gs4[i] - p.mf * gsum;
+          }
+        }
+        if (inner == 15) {
+          store4(l0 + row, ln);
+          if constexpr (GR) {
+            store4(p.g_mass + row, gm);
+            store4(p.g_stiff + row, gs4);
+          }
+        } else {
+  #pragma unroll
+          for (int i = 0; i < 4; ++i)
+            if ((inner >> i) & 1) {
+              l0[row + i] = ln[i];
+              if constexpr (GR) {
+                p.g_mass[row + i] = gm[i];
+                p.g_stiff[row + i] = gs4[i];
+              }
+            }
+        }
       }
-    }
+    };
+    if (plain)
+      march(std::true_type{});
+    else
+      march(std::false_type{});
   }
   finish_step(p.ctr, p.flags & K_ADV);
 }
