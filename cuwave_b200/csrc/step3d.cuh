@@ -81,7 +81,9 @@ __device__ __forceinline__ void st4(T *dst, const T *v) {
   *reinterpret_cast<float4 *>(dst) = make_float4(v[0], v[1], v[2], v[3]);
 }
 
-template <typename T, int R, bool UNIF>
+// HOLD: the grid has a Dirichlet face, whose wall nodes the step holds at zero (without
+// one, no node is held and the step carries no wall test)
+template <typename T, int R, bool UNIF, bool HOLD = true>
 __global__ void __launch_bounds__(S3_THREADS, 2)
     step3d_kernel(const __grid_constant__ Step3Params<T> P) {
   using S = Step3Shape<T, R>;
@@ -292,7 +294,7 @@ __global__ void __launch_bounds__(S3_THREADS, 2)
     if (!own)
       continue;
 
-    const int held = (yheld || held_wall(z, N0, dir0)) ? inner : xheld;
+    const int held = !HOLD ? 0 : (yheld || held_wall(z, N0, dir0)) ? inner : xheld;
     const int zrow = (flags & K_PML) ? slab_row(z, N0, g.lo[0], g.hi[0]) : -1;
 
     const T *cb = box(z);

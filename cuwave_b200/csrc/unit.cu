@@ -89,7 +89,7 @@ cudaError_t step3d_one(const Step3Params<T> &p, const dim3 grid, cudaStream_t s)
     return cudaErrorInvalidValue;
   } else {
     const size_t smem = Step3Shape<T, R>::SMEM;
-    const auto k = step3d_kernel<T, R, U>;
+    const auto k = p.s.g.dir ? step3d_kernel<T, R, U, true> : step3d_kernel<T, R, U, false>;
     cudaError_t e = allow_smem(k, smem);
     if (e != cudaSuccess)
       return e;
