@@ -94,7 +94,9 @@ __device__ __forceinline__ void image_run(T *xr, const T *row, const int xq, con
     zero_at<T, XR>(xr, N - 2 - (xq - H));
 }
 
-template <typename T, int R, int MODE>
+// HOLD: the grid has a Dirichlet face (without one, the faces' masks are zero at compile
+// time and every wall test folds away)
+template <typename T, int R, int MODE, bool HOLD = true>
 __global__ void __launch_bounds__(A2_THREADS, A2_MIN_BLOCKS) adjoint2d_kernel(const AdjointParams<T> p) {
   using S = Adj2Shape<T, R>;
   static_assert(S::SUPPORTED && MODE != MODE_GRAD, "the 2D quad adjoint: float, radius <= 4");
@@ -112,7 +114,7 @@ __global__ void __launch_bounds__(A2_THREADS, A2_MIN_BLOCKS) adjoint2d_kernel(co
     T *l0 = level<T>(p.l0, t);
     const T *__restrict__ l1 = level<T>(p.l1, t);
     const T *__restrict__ u1 = GR ? level<T>(p.u1, t) : nullptr;
-    const int dir0 = g.dir & 3, dirF = (g.dir >> 2) & 3;
+    const int dir0 = HOLD ? g.dir & 3 : 0, dirF = HOLD ? (g.dir >> 2) & 3 : 0;
     const int s0 = g.s[0];
     const int flags = p.flags;
     const T gg = p.gconst, dg = p.dgconst;

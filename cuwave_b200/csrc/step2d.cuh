@@ -49,8 +49,9 @@ struct Fold2 {
   int refill;           // faces whose ghosts are written
 };
 
-// unit k (a quad and a chunk of rows) of the step at t
-template <typename T, int R>
+// unit k (a quad and a chunk of rows) of the step at t; HOLD: the grid has a Dirichlet
+// face (without one, the faces' masks are zero at compile time and the wall tests fold)
+template <typename T, int R, bool HOLD = true>
 __device__ __forceinline__ void step2d_rows(const StepParams<T> &p, const int t, const long long k,
                                             const Fold2<T> &fold) {
   using S = Step2Shape<T, R>;
@@ -68,7 +69,7 @@ __device__ __forceinline__ void step2d_rows(const StepParams<T> &p, const int t,
     const T *__restrict__ u1 = level<T>(p.u1, t);
     T *u2 = level<T>(p.u2, t);
     const T *__restrict__ minv = p.minv;
-    const int dir0 = g.dir & 3, dirF = (g.dir >> 2) & 3;
+    const int dir0 = HOLD ? g.dir & 3 : 0, dirF = HOLD ? (g.dir >> 2) & 3 : 0;
     const int s0 = g.s[0];
     const int flags = p.flags;
     const T gg = p.gconst;
@@ -294,13 +295,14 @@ __device__ __forceinline__ void step2d_rows(const StepParams<T> &p, const int t,
   }
 }
 
-template <typename T, int R, bool UNIF>
+template <typename T, int R, bool UNIF, bool HOLD = true>
 __global__ void __launch_bounds__(S2_THREADS, Step2Shape<T, R>::MIN_BLOCKS)
     step2d_kernel(const StepParams<T> p) {
   static_assert(Step2Shape<T, R>::SUPPORTED && UNIF,
                 "the 2D quad step is built for float and a uniform stiffness");
   const Fold2<T> none{};
-  step2d_rows<T, R>(p, step_index(p.ctr), (long long)blockIdx.x * S2_THREADS + threadIdx.x, none);
+  step2d_rows<T, R, HOLD>(p, step_index(p.ctr), (long long)blockIdx.x * S2_THREADS + threadIdx.x,
+                          none);
   finish_step(p.ctr, p.flags & K_ADV);
 }
 

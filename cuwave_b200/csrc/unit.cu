@@ -120,7 +120,10 @@ cudaError_t step2d_unit(const StepParams<T> &p, const bool uniform, const dim3 g
   } else {
     if (!uniform)
       return cudaErrorInvalidValue;
-    step2d_kernel<T, R, true><<<grid, S2_THREADS, 0, s>>>(p);
+    if (p.g.dir)
+      step2d_kernel<T, R, true, true><<<grid, S2_THREADS, 0, s>>>(p);
+    else
+      step2d_kernel<T, R, true, false><<<grid, S2_THREADS, 0, s>>>(p);
     return cudaGetLastError();
   }
 }
@@ -167,10 +170,15 @@ cudaError_t adjoint2d_unit(const AdjointParams<T> &p, const int mode, const dim3
   if constexpr (!Adj2Shape<T, R>::SUPPORTED) {
     return cudaErrorInvalidValue;
   } else {
-    if (mode == MODE_STEP_GRAD)
-      adjoint2d_kernel<T, R, MODE_STEP_GRAD><<<grid, A2_THREADS, 0, s>>>(p);
+    const bool hold = p.g.dir != 0;
+    if (mode == MODE_STEP_GRAD && hold)
+      adjoint2d_kernel<T, R, MODE_STEP_GRAD, true><<<grid, A2_THREADS, 0, s>>>(p);
+    else if (mode == MODE_STEP_GRAD)
+      adjoint2d_kernel<T, R, MODE_STEP_GRAD, false><<<grid, A2_THREADS, 0, s>>>(p);
+    else if (mode == MODE_STEP && hold)
+      adjoint2d_kernel<T, R, MODE_STEP, true><<<grid, A2_THREADS, 0, s>>>(p);
     else if (mode == MODE_STEP)
-      adjoint2d_kernel<T, R, MODE_STEP><<<grid, A2_THREADS, 0, s>>>(p);
+      adjoint2d_kernel<T, R, MODE_STEP, false><<<grid, A2_THREADS, 0, s>>>(p);
     else
       return cudaErrorInvalidValue;
     return cudaGetLastError();
