@@ -323,7 +323,7 @@ struct March2Params {
   long long units;  // quads x row chunks
 };
 
-template <typename T, int R>
+template <typename T, int R, bool HOLD = true>
 __global__ void __launch_bounds__(S2_THREADS, Step2Shape<T, R>::MIN_BLOCKS)
     march2d_kernel(const __grid_constant__ March2Params<T> mp) {
   static_assert(Step2Shape<T, R>::SUPPORTED, "the 2D quad step is built for float");
@@ -334,7 +334,7 @@ __global__ void __launch_bounds__(S2_THREADS, Step2Shape<T, R>::MIN_BLOCKS)
   for (int s = 0; s < mp.steps; ++s) {
     const int t = mp.t0 + s;
     for (long long k = gtid; k < mp.units; k += gsize)
-      step2d_rows<T, R>(mp.s, t, k, mp.fold);
+      step2d_rows<T, R, HOLD>(mp.s, t, k, mp.fold);
     grid.sync();  // the step's nodes and ghosts are all written
     for (int r = 0; r < mp.nrec; ++r) {
       const TransferParams<T> &rp = mp.rec[r];

@@ -148,7 +148,7 @@ cudaError_t march2d_unit(const March2Params<T> &mp, const int sms, cudaStream_t 
   if constexpr (!Step2Shape<T, R>::SUPPORTED) {
     return cudaErrorInvalidValue;
   } else {
-    const auto k = march2d_kernel<T, R>;
+    const auto k = mp.s.g.dir ? march2d_kernel<T, R, true> : march2d_kernel<T, R, false>;
     int per = 0;
     cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, S2_THREADS, 0);
     if (e != cudaSuccess)
