@@ -258,7 +258,7 @@ def step_kernel_ms(sim, mat_inputs, steps: int) -> float:
 
 
 def blob_speed(n: int, seed: int = 0) -> np.ndarray:
-    """Config 0's speed: 1 plus 8 seeded Gaussian blobs (A in [-0.3, 0.3], sigma in
+    """The blob speed model: 1 plus 8 seeded Gaussian blobs (A in [-0.3, 0.3], sigma in
     [10, 40] cells at 512, scaled with the grid)."""
     rng = np.random.default_rng(seed)
     y, x = np.meshgrid(np.arange(n), np.arange(n), indexing="ij")
@@ -293,10 +293,10 @@ def march_ms(plan, ops, t0: int, steps: int, base: int = 64) -> float:
 
 
 def two_d_kernels(peak: float, steps: int = 200) -> dict:
-    """The 2D kernels at the shapes of configs 0 and 2 (512^2 Neumann; 2048^2 with a
-    20-cell PML): the forward step and the fused adjoint step (adjoint + gradients + pml
-    transpose + adjoint load), each as Gpt-updates/s and its algorithmic HBM bytes over its
-    CUDA-event time."""
+    """The 2D kernels at the 2D forward and sensitivity shapes (512^2 Neumann; 2048^2 with a
+    20-cell PML): the forward step and the adjoint step (pml memory, the transposed update
+    with the gradients, the pml gather, the adjoint load), each as Gpt-updates/s and its
+    algorithmic HBM bytes over its CUDA-event time."""
     import torch
 
     from cuwave_b200 import AcousticWave, Pml, _native as nat
@@ -348,7 +348,7 @@ def two_d_kernels(peak: float, steps: int = 200) -> dict:
 
 
 def batch_problems(count: int, steps: int, seed: int = 3):
-    """Config 3b's population: `count` 2D designs, sides U{256..1536}, space orders
+    """A topology-optimisation population: `count` 2D designs, sides U{256..1536}, space orders
     {4..12}, two-phase speeds {1.0, 0.3} from a thresholded smooth random field, a
     Ricker source at the centre and 64 receivers on a row; `steps` steps each."""
     import torch
@@ -379,7 +379,7 @@ def batch_problems(count: int, steps: int, seed: int = 3):
 
 
 def batch_measure(count: int = 64, steps: int = 300) -> dict:
-    """simulate_batch over config 3b's population against the same simulate calls in turn
+    """simulate_batch over the design population (batch_problems) against the same simulate calls in turn
     (device time, CUDA events; the second of two runs, the first tunes and loads)."""
     import torch
 
@@ -407,7 +407,7 @@ def batch_measure(count: int = 64, steps: int = 300) -> dict:
 
 
 def shots_measure(count: int = 96, steps: int = 2000, n: int = 1024) -> dict:
-    """Config 3a: `count` shots on a shared n^2 grid (config 0's blob speeds, radius 4),
+    """A multi-shot gradient: `count` shots on a shared n^2 grid (blob speeds, radius 4),
     sources evenly spaced along the top, 256 receivers 50 cells down, `steps` steps;
     the summed misfit gradient (a forward with its history and an adjoint per shot, in
     turn) timed with CUDA events after one warm-up shot. Observed data are zero, so the
@@ -446,7 +446,7 @@ def shots_measure(count: int = 96, steps: int = 2000, n: int = 1024) -> dict:
 
 
 def learned_measure(coarse_nodes: int = 256, coarse_steps: int = 600) -> dict:
-    """Config 4 at a reduced size: the corrector trained on pairs the plain solver makes,
+    """The learned coarse-grid form at a reduced size: the corrector trained on pairs the plain solver makes,
     then on held-out speed models the fine solve, the plain coarse solve and the corrected
     coarse solve timed (CUDA events) and their receiver traces compared with the fine
     ones (relative L2)."""
