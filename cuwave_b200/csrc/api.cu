@@ -1275,6 +1275,7 @@ struct cwb_batch {
     void *items = nullptr;  // device Batch2Item<float>[count]
     int count = 0;
     long long total = 0;
+    bool hold = true;  // an item of the group has a Dirichlet face
   };
   std::vector<Group> groups;
   void *recs = nullptr;  // device BatchRecord<float>[items]
@@ -1356,6 +1357,9 @@ int batch_layout(cwb_batch *b, const long long want) {
     grp.R = R;
     grp.count = (int)host.size();
     grp.total = first;
+    grp.hold = false;
+    for (const auto &it : host)
+      grp.hold = grp.hold || it.s.g.dir != 0;
     CWB_CUDA(cudaMalloc(&grp.items, sizeof(cwb::Batch2Item<T>) * host.size()));
     b->groups.push_back(grp);
     CWB_CUDA(cudaMemcpy(grp.items, host.data(), sizeof(cwb::Batch2Item<T>) * host.size(),
@@ -1374,6 +1378,7 @@ std::vector<Launch> batch_launches(cwb_batch *b, const bool records) {
     bp.items = static_cast<const cwb::Batch2Item<T> *>(g.items);
     bp.count = g.count;
     bp.total = g.total;
+    bp.hold = g.hold ? 1 : 0;
     bp.ctr = b->ctr;
     const dim3 grid((unsigned)((g.total + cwb::S2_THREADS - 1) / cwb::S2_THREADS));
     const int R = g.R;

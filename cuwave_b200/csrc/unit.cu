@@ -138,7 +138,10 @@ cudaError_t batch2d_unit(const Batch2Params<T> &p, const dim3 grid, cudaStream_t
   if constexpr (!Step2Shape<T, R>::SUPPORTED) {
     return cudaErrorInvalidValue;
   } else {
-    batch2d_kernel<T, R><<<grid, S2_THREADS, 0, s>>>(p);
+    if (p.hold)
+      batch2d_kernel<T, R, true><<<grid, S2_THREADS, 0, s>>>(p);
+    else
+      batch2d_kernel<T, R, false><<<grid, S2_THREADS, 0, s>>>(p);
     return cudaGetLastError();
   }
 }
