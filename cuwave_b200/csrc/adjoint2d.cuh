@@ -12,10 +12,9 @@
 // over rows z-R .. z+R, u^n over rows z-R+1 .. z+R) row by row as 16-byte rows of its
 // column, which the rows before brought into L1 (register queues of them measured
 // slower: their 68 registers and shifts cost more than the L1 reads), and the quad's
-// axis-1 runs of 4 + 2H values. The taps read through
-// the node image (a stored ghost is never read; lambda and u odd across a Dirichlet face)
-// and read zero on a held wall node, as cuwave's `reflected` does
-// (scalar_sensitivity.cu:177-184). Along axis 1 the quad shares its runs' first
+// axis-1 runs of 4 + 2H values. The taps read through the node image (a stored ghost is
+// never read; lambda and u odd across a Dirichlet face) and read zero on a held wall
+// node, as cuwave's `reflected` does (scalar_sensitivity.cu:177-184). Along axis 1 the quad shares its runs' first
 // differences and the plain D+ of u between neighbouring nodes: the same subtractions and
 // products of the same values the per-node form performs, so the sums are bit-identical;
 // a node on a held wall keeps the per-node form (its own value is not its taps' zero).
@@ -156,7 +155,7 @@ __global__ void __launch_bounds__(A2_THREADS, A2_MIN_BLOCKS) adjoint2d_kernel(co
     // The axis-0 taps are read row by row as the march needs them (the thread read the
     // same rows of its column in the rows before, so they come from L1): lambda rows
     // z-R .. z+R and u rows z-R+1 .. z+R. dmz carries the plain D+ of u at the row before
-    // (this row's D-); the first row's reads u row c0 - R once.
+    // (this row's D-); for the chunk's first row it reads u rows c0 - R .. c0 + R - 1.
     T dmz[4];
     if constexpr (GR) {
       T uc[4], a[4], b[4];
