@@ -140,44 +140,139 @@ def dist_setup():
     return rank, world, local
 
 
-def cpu_baseline(w: dict, sample_steps: int, cores: int | None = None) -> dict:
+def cpu_baseline(w: dict, sample_steps: int, cores: int | None = None):
     """The reference's own kernels (oracle/_ref, built from its sources) on the host cores,
-    a bounded sample of `sample_steps` steps of the same job."""
+    a bounded sample of `sample_steps` steps of the same job. Returns the baseline entry
+    and the sample's final field and traces (None when the build is missing)."""
     from oracle import oracle as o
 
-    path = o.ref_library(3, 4, "optimized", "float32")
+    path, level = o.ref_library(3, 4, "optimized", "float32")
     if not path.exists():
         return {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
-                "sample": f"unavailable: {path.name} not built (oracle/ref_build.py)"}
+                "sample": f"unavailable: {path.name} not built (oracle/ref_build.py)"}, None, None
     cores = cores or os.cpu_count() or 1
     case = reference_case(w)
-    o.ref_simulate_3d(case, 1, threads=cores)  # page in, spawn the OpenMP team
+    o.ref_simulate(case, 1, threads=cores)  # page in, spawn the OpenMP team
     t0 = time.perf_counter()
-    o.ref_simulate_3d(case, sample_steps, threads=cores)
+    field, traces = o.ref_simulate(case, sample_steps, threads=cores)
     elapsed = time.perf_counter() - t0
     value = interior_updates(w) * sample_steps / elapsed / 1e9
     return {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
             "sample": f"{sample_steps} of {w['steps']} steps of the full {w['Nx'][0]}^3 job "
-                      f"({elapsed:.1f} s), reference kernels via oracle/_ref, OpenMP"}
+                      f"({elapsed:.1f} s), reference kernels via oracle/_ref built with g++ -O3 "
+                      f"-fopenmp -ffp-contract=off -march={REF_MARCH[level]}, OpenMP"}, field, traces
 
 
-def reference_case(w: dict):
-    """The job as an oracle case: the same materials, tables and source weights."""
+# the -march of each instruction-set level oracle/ref_build.py builds (the reference's own
+# host build uses -march=native, cuwave/cpu.py:22)
+REF_MARCH = {"v4": "x86-64-v4 (AVX-512)", "v3": "x86-64-v3 (AVX2)", "v1": "x86-64"}
+
+
+def sample_parity(sim, w: dict, steps: int, ref_field, ref_traces) -> dict:
+    """The repo's march over the first `steps` steps of the job (the public `simulate`,
+    the same inputs) against the reference kernels' sample: field and traces compared
+    to the bit."""
+    from dataclasses import replace
+
+    import torch
+
+    from cuwave_b200 import Source, simulate
+
+    dev = torch.device("cuda")
+    short = replace(sim, N=steps)
+    field, traces = simulate(short, Source(torch.as_tensor(w["source"], device=dev),
+                                           torch.as_tensor(w["signal"], device=dev)),
+                             torch.as_tensor(w["indicator"], device=dev), torch.as_tensor(w["sensors"], device=dev))
+    field = field.cpu().numpy()
+    traces = traces.cpu().numpy()
+    ref = ref_field[tuple(slice(0, n) for n in w["Nx"])]
+    diff = np.abs(field.astype(np.float64) - ref)
+    scale = float(np.linalg.norm(ref.astype(np.float64)))
+    return {"steps": steps, "field_max_abs": float(diff.max()),
+            "field_rel_l2": float(np.linalg.norm(diff) / scale) if scale else float(np.linalg.norm(diff)),
+            "traces_max_abs": float(np.abs(traces.astype(np.float64) - ref_traces).max()),
+            "bitwise": bool(np.array_equal(field, ref) and np.array_equal(traces, ref_traces)),
+            "against": "the cpu_baseline sample (reference kernels via oracle/_ref)"}
+
+
+def reference_case(w: dict, dtype=np.float32):
+    """A 2D or 3D job as an oracle case: the same materials, tables and source weights,
+    in `dtype` (the float64 case is the same scheme on the same inputs)."""
     from oracle import oracle as o
 
-    Nx = w["Nx"]
-    stiff, minv = o.acoustic_materials(Nx, w["indicator"], 1.0, 1.0, 1.0, w["kappa2"], np.float32)
-    widths = tuple((w["width"], w["width"]) for _ in range(3)) if w["width"] else None
-    profiles = o.pml_profiles(Nx, (1.0,) * 3, w["dt"], widths, w["width"], w["c_max"], 1e-6, 0.0,
-                              np.float32) if w["width"] else None
-    flat = lambda p: (p[0].astype(np.int64) * Nx[1] * ((Nx[2] + 31) // 32 * 32)  # noqa: E731
-                      + p[1].astype(np.int64) * ((Nx[2] + 31) // 32 * 32) + p[2]).astype(np.int32)
-    case = o.Case(Nx=Nx, R=4, coeffs=o.cell_coefficients(4, "optimized"),
-                  factors=[np.float32(2.0 * w["dt"] ** 2)] * 3, dt=w["dt"], stiff=stiff, minv=minv,
-                  widths=widths, profiles=profiles, source_lin=flat(w["source"]),
-                  signal=w["signal"], sensor_lin=flat(w["sensors"]))
+    Nx = tuple(w["Nx"])
+    ndim = len(Nx)
+    R = w.get("radius", 4)
+    stiff, minv = o.acoustic_materials(Nx, w["indicator"], 1.0, 1.0, 1.0, w["kappa2"], dtype)
+    widths = tuple((w["width"], w["width"]) for _ in range(ndim)) if w["width"] else None
+    profiles = o.pml_profiles(Nx, (1.0,) * ndim, w["dt"], widths, w["width"], w["c_max"], 1e-6, 0.0,
+                              dtype) if w["width"] else None
+    shape = (*Nx[:-1], (Nx[-1] + 31) // 32 * 32)
+    strides = [int(np.prod(shape[d + 1:])) for d in range(ndim)]
+
+    def flat(p):
+        return sum(p[d].astype(np.int64) * strides[d] for d in range(ndim)).astype(np.int32)
+
+    case = o.Case(Nx=Nx, R=R, coeffs=o.cell_coefficients(R, "optimized"),
+                  factors=[dtype(2.0 * w["dt"] ** 2)] * ndim, dt=w["dt"], stiff=stiff, minv=minv,
+                  dtype=dtype, widths=widths, profiles=profiles, source_lin=flat(w["source"]),
+                  signal=w["signal"].astype(dtype), sensor_lin=flat(w["sensors"]))
     case.source_weight = case.excitation_weights(case.source_lin)
     return case
+
+
+def blob_workload(n: int, steps: int, width: int = 0, seed: int = 0) -> dict:
+    """The 2D blob job: AcousticWave on an n x n grid (ghosts included), radius 4, speed 1
+    plus 8 seeded Gaussian blobs (blob_speed), dt at CFL 0.5 of the fastest speed, a Ricker
+    source at the centre with about 20 points a wavelength at the slowest speed, 64
+    receivers on row 51 at columns linspace(1, n - 2, 64) rounded, an optional pml."""
+    from cuwave_b200.signals import ricker
+    from cuwave_b200.stencils import stable_dt
+
+    c = blob_speed(n, seed)
+    kappa2 = 0.25
+    shape = (n, (n + 31) // 32 * 32)
+    indicator = np.zeros(shape, np.float32)
+    indicator[:, :n] = ((1.0 / c**2 - 1.0) / (1.0 / kappa2 - 1.0)).astype(np.float32)
+    c_max = float(c.max())
+    dt = 0.5 * stable_dt((1.0, 1.0), c_max, 8, "optimized")
+    signal = ricker(np.arange(steps) * dt, 1.0, float(c.min()) / 20.0)[:, None].astype(np.float32)
+    source = np.array([[n // 2], [n // 2]], np.int32)
+    cols = np.round(np.linspace(1, n - 2, 64)).astype(np.int32)
+    sensors = np.stack([np.full(64, 51, np.int32), cols]).astype(np.int32)
+    return dict(Nx=(n, n), steps=steps, width=width, dt=dt, c_max=c_max, kappa2=kappa2,
+                indicator=indicator, signal=signal, source=source, sensors=sensors, speed=c)
+
+
+def sensitivity_workload(n: int = 2048, steps: int = 300, width: int = 20, seed: int = 0) -> dict:
+    """The 2D gradient job: the blob job on an n x n grid with a `width`-cell pml, one
+    source 20 rows inside the pml's inner edge and 256 receivers 40 rows below it
+    (columns spread over the interior), and observed traces made with the speed
+    perturbed by 5% seeded blobs (c_obs = c (1 + 0.05 b), b a second blob field scaled to
+    [-1, 1]), so the misfit is not small. `steps` is short of a full run, so the
+    source and the receivers sit close enough for the wave to reach them."""
+    w = blob_workload(n, steps, width, seed)
+    R = 4
+    w["source"] = np.array([[width + 20], [n // 2]], np.int32)
+    cols = np.round(np.linspace(width + R + 2, n - width - R - 3, 256)).astype(np.int32)
+    w["sensors"] = np.stack([np.full(256, width + 60, np.int32), cols]).astype(np.int32)
+    b = (blob_speed(n, seed + 1) - 1.0) / 0.3
+    c_obs = w["speed"] * (1.0 + 0.05 * b)
+    ind = np.zeros_like(w["indicator"])
+    ind[:, :n] = ((1.0 / c_obs**2 - 1.0) / (1.0 / w["kappa2"] - 1.0)).astype(np.float32)
+    w["indicator_obs"] = ind
+    return w
+
+
+def make_sim_2d(w: dict, precision: str = "float32", steps: int | None = None):
+    from cuwave_b200 import AcousticWave, Pml
+
+    return AcousticWave(
+        Nx=w["Nx"], dx=(1.0, 1.0), N=steps or w["steps"], dt=w["dt"], precision=precision,
+        space_order=8, stencil="optimized",
+        pml=Pml(width=w["width"], wavespeed=w["c_max"]) if w["width"] else None,
+        rho1=1.0, rho2=1.0, kappa1=1.0, kappa2=w["kappa2"],
+    )
 
 
 def run_reference(args) -> int:
@@ -189,7 +284,7 @@ def run_reference(args) -> int:
     times = []
     from oracle import oracle as o
 
-    path = o.ref_library(3, 4, "optimized", "float32")
+    path, level = o.ref_library(3, 4, "optimized", "float32")
     if not path.exists():
         print(json.dumps({"impl": "reference", "unavailable": f"{path.name} was not built"}))
         return 0
@@ -197,7 +292,7 @@ def run_reference(args) -> int:
     cores = os.cpu_count() or 1
     for i in range(args.warmup + args.steps):
         t0 = time.perf_counter()
-        o.ref_simulate_3d(case, sample, threads=cores)
+        o.ref_simulate(case, sample, threads=cores)
         if i >= args.warmup:
             times.append(time.perf_counter() - t0)
     per = sum(times) / len(times)
@@ -209,7 +304,9 @@ def run_reference(args) -> int:
         "data": "synthetic (seeded layered model)",
         "config": config_line(w, args),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
-                         "sample": f"{sample} of {w['steps']} steps of the full job per bench step"},
+                         "sample": f"{sample} of {w['steps']} steps of the full job per bench step, "
+                                   f"reference kernels via oracle/_ref built with g++ -O3 -fopenmp "
+                                   f"-ffp-contract=off -march={REF_MARCH[level]}"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -345,6 +442,65 @@ def two_d_kernels(peak: float, steps: int = 200) -> dict:
             del V, P
         out[name] = entry
     return out
+
+
+def three_d_kernels(peak: float, n: int = 256, steps: int = 100) -> dict:
+    """The 3D steps beside the bench job's radius: the forward step for radius 1..8 on an
+    n^3 grid with Neumann faces (radius 1..4 on the register-blocked kernel, 5..8 on the
+    row kernel), and the fused adjoint step (transposed update with the gradients, the
+    pml transpose, the adjoint load) at radius 4 with a 10-cell pml, each as
+    Gpt-updates/s and the fraction of the measured HBM peak its algorithmic bytes give."""
+    import torch
+
+    from cuwave_b200 import AcousticWave, Pml, _native as nat
+    from cuwave_b200.sensitivity import _adjoint_ops
+    from cuwave_b200.stencils import stable_dt
+    from cuwave_b200.wave import flatten_indices, forward_ops, pml_memory, prepare_shot
+
+    dev = torch.device("cuda")
+    rng = np.random.default_rng(5)
+    c = 1.0 + 0.5 * rng.random((n, n, n))
+    kappa2 = 0.25
+    interior = (n - 2) ** 3
+    out = {}
+    N = steps + 64 + 8
+    for R in range(1, 9):
+        width = 10 if R == 4 else 0
+        dt = 0.5 * stable_dt((1.0,) * 3, float(c.max()), 2 * R, "optimized")
+        sim = AcousticWave(Nx=(n, n, n), dx=(1.0,) * 3, N=N, dt=dt, precision="float32",
+                           space_order=2 * R, pml=Pml(width=width, wavespeed=float(c.max())) if width else None,
+                           rho1=1.0, rho2=1.0, kappa1=1.0, kappa2=kappa2)
+        ind = torch.zeros(sim.Nx_padded, dtype=torch.float32, device=dev)
+        ind[..., :n] = torch.as_tensor((1.0 / c**2 - 1.0) / (1.0 / kappa2 - 1.0), device=dev)
+        mat = sim.build_materials(ind)
+        shot = prepare_shot(sim, mat, torch.tensor([[n // 2]] * 3, device=dev),
+                            torch.zeros((N, 1), dtype=torch.float32, device=dev))
+        U = torch.zeros((2, *sim.Nx_padded), dtype=torch.float32, device=dev)
+        ops = forward_ops(sim, mat, nat.level(U, add=0, period=2), nat.level(U, add=1, period=2),
+                          nat.level(U, add=0, period=2), shot, pml_memory(sim, 3, dev))
+        plan = sim.plan()
+        ms = march_ms(plan, ops, 0, steps)
+        slab = sum(2 * width * (n - 2) ** 2 for _ in range(3))
+        fwd_bytes = 16 * interior + 24 * slab
+        entry = {"pml": width, "forward_gpts": interior / (ms / 1e3) / 1e9, "forward_ms_per_step": ms,
+                 "forward_roofline_frac": fwd_bytes / (ms / 1e3) / 1e9 / peak}
+        if R == 4:
+            V = torch.zeros((N + 2, *sim.Nx_padded), dtype=torch.float32, device=dev)
+            P = torch.zeros((2, *sim.Nx_padded), dtype=torch.float32, device=dev)
+            sensors = torch.tensor([[20] * 64, list(range(20, 20 + 64 * 3, 3)), [n // 2] * 64],
+                                   dtype=torch.int32, device=dev)
+            lin = flatten_indices(sim, sensors)
+            adj_signal = torch.zeros((N, 64), dtype=torch.float32, device=dev)
+            aops = _adjoint_ops(sim, mat, P, pml_memory(sim, 5, dev), u_level=nat.level(V, mul=-1, add=N + 1),
+                                grads=sim.gradient_fields(mat), load=(lin, adj_signal, sim.excitation_weights(mat, lin)))
+            ams = march_ms(plan, aops, 0, steps)
+            adj_bytes = 32 * interior + 44 * slab
+            entry.update({"adjoint_gpts": interior / (ams / 1e3) / 1e9, "adjoint_ms_per_step": ams,
+                          "adjoint_roofline_frac": adj_bytes / (ams / 1e3) / 1e9 / peak})
+            del V, P
+        out[f"r{R}"] = entry
+        del U
+    return {"grid": [n, n, n], "kernels": out}
 
 
 def batch_problems(count: int, steps: int, seed: int = 3):
@@ -565,7 +721,7 @@ def run_ours(args) -> int:
 
     e2e_job()
     barrier()
-    e2e_steps = max(1, min(args.steps, 3))
+    e2e_steps = max(1, min(args.steps, 10))
     e0.record(stream)
     for _ in range(e2e_steps):
         e2e_job()
@@ -582,6 +738,7 @@ def run_ours(args) -> int:
     peak, peak_kind = hbm_peak()
     traffic = profile_traffic(w)
     kernels_2d = two_d_kernels(peak) if args.size == 512 and not args.no_2d and world == 1 else None
+    kernels_3d = three_d_kernels(peak) if args.size == 512 and not args.no_2d and world == 1 else None
     batch = batch_measure() if args.size == 512 and not args.no_batch and world == 1 else None
     shots_2d = shots_measure() if args.size == 512 and not args.no_batch and world == 1 else None
     learned = learned_measure() if args.size == 512 and args.learned and world == 1 else None
@@ -591,7 +748,11 @@ def run_ours(args) -> int:
         dist.destroy_process_group()
     if rank != 0:
         return 0
-    baseline = cpu_baseline(w, args.cpu_sample) if not args.no_cpu else None
+    baseline, parity = None, None
+    if not args.no_cpu:
+        baseline, ref_field, ref_traces = cpu_baseline(w, args.cpu_sample)
+        if ref_field is not None:
+            parity = sample_parity(sim, w, args.cpu_sample, ref_field, ref_traces)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
@@ -602,12 +763,14 @@ def run_ours(args) -> int:
                      "kernel": step_kernel_name(),
                      "kernel_ms": kernel_ms, "algorithmic_bytes_per_launch": bytes_per_launch},
         "cpu_baseline": baseline,
+        "parity": parity,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms},
         "gpu_launches": launches,
         "clocks": clock,
         "kernel_updates_per_s": interior_updates(w) / (kernel_ms / 1e3) / 1e9,
         "kernels_2d": kernels_2d,
+        "kernels_3d": kernels_3d,
         "batch_2d": batch,
         "shots_2d": shots_2d,
         "learned": learned,

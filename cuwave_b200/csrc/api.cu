@@ -1244,6 +1244,64 @@ int march(cwb_plan *p, const cwb_op *ops, const int nops, const int t0, const in
   return CWB_OK;
 }
 
+// A plan's geometry from its grid, validated: the stencil and precision built here,
+// the padded extents and strides, the pml slabs and their memory rows, the device's SM
+// count and the environment's overrides. cwb_plan_create and cwb_march_static both
+// start from it, so the two step the same geometry.
+int plan_geometry(const cwb_grid &G, cwb_plan &p) {
+  if (G.ndim != 2 && G.ndim != 3)
+    return fail(CWB_ERR_UNSUPPORTED, "the steps are 2D and 3D");
+  if (G.radius < 1 || G.radius > CWB_MAX_RADIUS)
+    return fail(CWB_ERR_UNSUPPORTED, "radius runs 1 .. 8");
+  if (G.precision != 4 && G.precision != 8)
+    return fail(CWB_ERR_UNSUPPORTED, "precision is 4 or 8 bytes");
+  if ((G.dirichlet & G.neumann) != 0)
+    return fail(CWB_ERR_ARG, "a face is either Neumann or Dirichlet");
+  cwb::Geometry &geo = p.geo;
+  std::memset(&geo, 0, sizeof geo);
+  geo.ndim = G.ndim;
+  long long total = 1;
+  for (int d = 0; d < G.ndim; ++d) {
+    if (G.nx[d] < G.radius + 3)
+      return fail(CWB_ERR_ARG, "every axis needs at least radius + 3 nodes");
+    geo.n[d] = G.nx[d];
+    geo.ext[d] = d == G.ndim - 1 ? (G.nx[d] + 31) / 32 * 32 : G.nx[d];
+    total *= geo.ext[d];
+  }
+  if (total >= (1LL << 31))
+    return fail(CWB_ERR_ARG, "the padded grid overflows int32 flat indices");
+  geo.s[G.ndim - 1] = 1;
+  for (int d = G.ndim - 2; d >= 0; --d)
+    geo.s[d] = geo.s[d + 1] * geo.ext[d + 1];
+  geo.dir = G.dirichlet;
+  for (int d = 0; d < G.ndim; ++d) {
+    geo.lo[d] = G.pml_lo[d];
+    geo.hi[d] = G.pml_hi[d];
+    if (geo.lo[d] < 0 || geo.hi[d] < 0 ||
+        (geo.lo[d] + geo.hi[d] > 0 &&
+         (geo.lo[d] ? geo.lo[d] + G.radius : 0) + (geo.hi[d] ? geo.hi[d] + G.radius : 0) >=
+             G.nx[d] - 2))
+      return fail(CWB_ERR_ARG, "the pml layers and their reach leave no interior");
+    if (geo.lo[d] + geo.hi[d] == 0)
+      continue;
+    long long row = 1;
+    for (int e = 0; e < G.ndim; ++e)
+      row *= e == d ? geo.lo[d] + geo.hi[d] : geo.ext[e];
+    p.pml_row[d] = row;
+  }
+  p.grid = G;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&p.sms, cudaDevAttrMultiProcessorCount, dev);
+  if (const char *env = std::getenv("CWB_CHUNK"))
+    p.chunk_override = std::atoi(env);
+  if (const char *env = std::getenv("CWB_NO_TMA"))
+    p.tma = std::atoi(env) == 0;
+  if (const char *env = std::getenv("CWB_STEP3D"))
+    p.blocked3 = std::atoi(env) != 0;
+  return CWB_OK;
+}
+
 // ------------------------------------------------------------------------------ batches
 template <typename T>
 cudaError_t batch2d_r(const cwb::Batch2Params<T> &p, const int R, const dim3 grid,
@@ -1723,61 +1781,11 @@ int cwb_plan_create(const cwb_grid *grid, cwb_plan **out) {
   if (!grid || !out)
     return fail(CWB_ERR_ARG, "null argument");
   *out = nullptr;
-  const cwb_grid &G = *grid;
-  if (G.ndim != 2 && G.ndim != 3)
-    return fail(CWB_ERR_UNSUPPORTED, "the steps are 2D and 3D");
-  if (G.radius < 1 || G.radius > CWB_MAX_RADIUS)
-    return fail(CWB_ERR_UNSUPPORTED, "radius runs 1 .. 8");
-  if (G.precision != 4 && G.precision != 8)
-    return fail(CWB_ERR_UNSUPPORTED, "precision is 4 or 8 bytes");
-  cwb::Geometry geo;
-  std::memset(&geo, 0, sizeof geo);
-  geo.ndim = G.ndim;
-  long long total = 1;
-  for (int d = 0; d < G.ndim; ++d) {
-    if (G.nx[d] < G.radius + 3)
-      return fail(CWB_ERR_ARG, "every axis needs at least radius + 3 nodes");
-    geo.n[d] = G.nx[d];
-    geo.ext[d] = d == G.ndim - 1 ? (G.nx[d] + 31) / 32 * 32 : G.nx[d];
-    total *= geo.ext[d];
-  }
-  if (total >= (1LL << 31))
-    return fail(CWB_ERR_ARG, "the padded grid overflows int32 flat indices");
-  geo.s[G.ndim - 1] = 1;
-  for (int d = G.ndim - 2; d >= 0; --d)
-    geo.s[d] = geo.s[d + 1] * geo.ext[d + 1];
-  geo.dir = G.dirichlet;
-  if ((G.dirichlet & G.neumann) != 0)
-    return fail(CWB_ERR_ARG, "a face is either Neumann or Dirichlet");
-  for (int d = 0; d < G.ndim; ++d) {
-    geo.lo[d] = G.pml_lo[d];
-    geo.hi[d] = G.pml_hi[d];
-    if (geo.lo[d] < 0 || geo.hi[d] < 0 ||
-        (geo.lo[d] + geo.hi[d] > 0 &&
-         (geo.lo[d] ? geo.lo[d] + G.radius : 0) + (geo.hi[d] ? geo.hi[d] + G.radius : 0) >=
-             G.nx[d] - 2))
-      return fail(CWB_ERR_ARG, "the pml layers and their reach leave no interior");
-  }
   cwb_plan *p = new cwb_plan();
-  p->grid = G;
-  p->geo = geo;
-  for (int d = 0; d < G.ndim; ++d) {
-    if (geo.lo[d] + geo.hi[d] == 0)
-      continue;
-    long long row = 1;
-    for (int e = 0; e < G.ndim; ++e)
-      row *= e == d ? geo.lo[d] + geo.hi[d] : geo.ext[e];
-    p->pml_row[d] = row;
+  if (const int rc = plan_geometry(*grid, *p)) {
+    delete p;
+    return rc;
   }
-  int dev = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&p->sms, cudaDevAttrMultiProcessorCount, dev);
-  if (const char *env = std::getenv("CWB_CHUNK"))
-    p->chunk_override = std::atoi(env);
-  if (const char *env = std::getenv("CWB_NO_TMA"))
-    p->tma = std::atoi(env) == 0;
-  if (const char *env = std::getenv("CWB_STEP3D"))
-    p->blocked3 = std::atoi(env) != 0;
   if (cudaMalloc(&p->ctr, 2 * sizeof(int)) != cudaSuccess ||
       cudaMalloc(&p->err, sizeof(int)) != cudaSuccess ||
       cudaStreamCreateWithFlags(&p->lane, cudaStreamNonBlocking) != cudaSuccess ||
@@ -1848,81 +1856,18 @@ namespace {
 // 16 bytes of counter and flag, the rest for folded-source lists
 __device__ __align__(256) unsigned char g_static_scratch[CWB_STATIC_SCRATCH_BYTES];
 
-constexpr int MAX_DEVICES = 64;
-void *g_static_ptr[MAX_DEVICES] = {};
-
 // The device address of g_static_scratch on the current device. In host code the
-// symbol's name is only a host-side stand-in, so the address is asked from the runtime
-// once per device, with that device current, and cached.
+// symbol's name is only a host-side stand-in, so the address is asked from the runtime,
+// with the device current, on every call: a cached address could outlive the module it
+// points into (a device reset, or a primary context torn down and made again, loads the
+// module anew), and one lookup costs nothing next to a march.
 int static_scratch(void **out) {
-  int dev = 0;
-  CWB_CUDA(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= MAX_DEVICES)
-    return fail(CWB_ERR_UNSUPPORTED, "device ordinal past the static scratch table");
-  if (!g_static_ptr[dev]) {
-    void *ptr = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&ptr, g_static_scratch);
-    if (e != cudaSuccess)
-      return fail(CWB_ERR_CUDA,
-                  std::string("cudaGetSymbolAddress(g_static_scratch): ") + cudaGetErrorString(e));
-    g_static_ptr[dev] = ptr;
-  }
-  *out = g_static_ptr[dev];
-  return CWB_OK;
-}
-
-// the plan fields a march reads, validated as cwb_plan_create validates them
-int static_geometry(const cwb_grid &G, cwb_plan &p) {
-  if (G.ndim != 2 && G.ndim != 3)
-    return fail(CWB_ERR_UNSUPPORTED, "the steps are 2D and 3D");
-  if (G.radius < 1 || G.radius > CWB_MAX_RADIUS)
-    return fail(CWB_ERR_UNSUPPORTED, "radius runs 1 .. 8");
-  if (G.precision != 4 && G.precision != 8)
-    return fail(CWB_ERR_UNSUPPORTED, "precision is 4 or 8 bytes");
-  if ((G.dirichlet & G.neumann) != 0)
-    return fail(CWB_ERR_ARG, "a face is either Neumann or Dirichlet");
-  cwb::Geometry &geo = p.geo;
-  std::memset(&geo, 0, sizeof geo);
-  geo.ndim = G.ndim;
-  long long total = 1;
-  for (int d = 0; d < G.ndim; ++d) {
-    if (G.nx[d] < G.radius + 3)
-      return fail(CWB_ERR_ARG, "every axis needs at least radius + 3 nodes");
-    geo.n[d] = G.nx[d];
-    geo.ext[d] = d == G.ndim - 1 ? (G.nx[d] + 31) / 32 * 32 : G.nx[d];
-    total *= geo.ext[d];
-  }
-  if (total >= (1LL << 31))
-    return fail(CWB_ERR_ARG, "the padded grid overflows int32 flat indices");
-  geo.s[G.ndim - 1] = 1;
-  for (int d = G.ndim - 2; d >= 0; --d)
-    geo.s[d] = geo.s[d + 1] * geo.ext[d + 1];
-  geo.dir = G.dirichlet;
-  for (int d = 0; d < G.ndim; ++d) {
-    geo.lo[d] = G.pml_lo[d];
-    geo.hi[d] = G.pml_hi[d];
-    if (geo.lo[d] < 0 || geo.hi[d] < 0 ||
-        (geo.lo[d] + geo.hi[d] > 0 &&
-         (geo.lo[d] ? geo.lo[d] + G.radius : 0) + (geo.hi[d] ? geo.hi[d] + G.radius : 0) >=
-             G.nx[d] - 2))
-      return fail(CWB_ERR_ARG, "the pml layers and their reach leave no interior");
-    if (geo.lo[d] + geo.hi[d] == 0)
-      continue;
-    long long row = 1;
-    for (int e = 0; e < G.ndim; ++e)
-      row *= e == d ? geo.lo[d] + geo.hi[d] : geo.ext[e];
-    p.pml_row[d] = row;
-  }
-  p.grid = G;
-  int dev = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&p.sms, cudaDevAttrMultiProcessorCount, dev);
-  if (const char *env = std::getenv("CWB_CHUNK"))
-    p.chunk_override = std::atoi(env);
-  if (const char *env = std::getenv("CWB_NO_TMA"))
-    p.tma = std::atoi(env) == 0;
-  if (const char *env = std::getenv("CWB_STEP3D"))
-    p.blocked3 = std::atoi(env) != 0;
+  void *ptr = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&ptr, g_static_scratch);
+  if (e != cudaSuccess)
+    return fail(CWB_ERR_CUDA,
+                std::string("cudaGetSymbolAddress(g_static_scratch): ") + cudaGetErrorString(e));
+  *out = ptr;
   return CWB_OK;
 }
 
@@ -1965,7 +1910,7 @@ extern "C" int cwb_march_static(const cwb_grid *grid, const cwb_op *ops, const i
   if (rc)
     return rc;
   cwb_plan p;  // on the stack: no stream, event or device memory of its own
-  if ((rc = static_geometry(*grid, p)))
+  if ((rc = plan_geometry(*grid, p)))
     return rc;
   unsigned char *bytes = static_cast<unsigned char *>(base);
   p.ctr = reinterpret_cast<int *>(bytes);      // step counter and blocks done

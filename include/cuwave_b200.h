@@ -11,6 +11,8 @@
  * is sum_d i_d * stride_d over that grid, int32. Every call returns CWB_OK (0) or a
  * negative CWB_ERR_* code, and cwb_last_error() then holds one line of text. Nothing is
  * allocated outside a plan: a plan owns its scratch (counters, source lists, graphs).
+ * The one entry point that runs without a plan, cwb_march_static, allocates nothing at
+ * all: its scratch is a fixed static device array.
  *
  * The reference (cmpmech/cuwave) launches one CUDA C kernel per operation from Python;
  * on its host fallback each kernel is bound through the C ABI
@@ -192,8 +194,9 @@ int cwb_march(cwb_plan *plan, const cwb_op *ops, int32_t nops, int32_t t0,
  * directly on `stream`, without a plan: it allocates nothing, captures no graph, and
  * keeps its step counter, error flag and folded-source lists (16 bytes per source plus
  * 4 bytes per block of the step's grid) in one static device array of
- * CWB_STATIC_SCRATCH_BYTES, whose device address it asks the runtime for on its first
- * call on each device (make that first call before any stream capture). A march whose
+ * CWB_STATIC_SCRATCH_BYTES. It asks the runtime for the array's device address on
+ * every call, with the caller's device current (the first call on a device may load the
+ * library's device code: make it before any stream capture). A march whose
  * lists do not fit is refused with CWB_ERR_ARG. Every call shares the array: calls that
  * overlap on the GPU (two streams, two host threads) race and must not be issued. The
  * call returns after the march has finished on the GPU. */

@@ -702,40 +702,56 @@ def l2(observed):
 REF_DIR = HERE / "_ref"
 
 
-def ref_library(ndim=3, radius=4, stencil="optimized", precision="float32") -> Path:
-    tag = "f32" if precision == "float32" else "f64"
-    return REF_DIR / f"libref{ndim}d_r{radius}_{stencil}_{tag}.so"
+def ref_library(ndim=3, radius=4, stencil="optimized", precision="float32") -> tuple[Path, str]:
+    """(path, instruction-set level) of the reference's kernels built for this host by
+    ref_build.py: the highest level the host's CPU supports."""
+    import importlib.util
+    import sys
+
+    spec = importlib.util.spec_from_file_location("_oracle_ref_build", HERE / "ref_build.py")
+    module = sys.modules.get(spec.name)
+    if module is None:
+        module = importlib.util.module_from_spec(spec)
+        sys.modules[spec.name] = module
+        spec.loader.exec_module(module)
+    return module.library(ndim, radius, stencil, precision)
 
 
-def ref_simulate_3d(case: "Case", N: int, threads: int | None = None):
+def ref_simulate(case: "Case", N: int, threads: int | None = None, library: Path | None = None):
     """The reference's own fd/pml/excitation/refill/record kernels (built by ref_build.py
-    from its sources) stepped N times on a 3D Neumann case; returns (field, traces)."""
-    path = ref_library(3, case.R, "optimized", "float32" if case.dtype == np.float32 else "float64")
+    from its sources) stepped N times on a 2D or 3D Neumann case; returns (field, traces),
+    the field over the padded grid. `library` names a build; by default the one for this
+    host's instruction set."""
+    ndim = len(case.Nx)
+    path = library or ref_library(ndim, case.R, "optimized",
+                                  "float32" if case.dtype == np.float32 else "float64")[0]
     if not path.exists():
         raise FileNotFoundError(f"{path.name} is not built: run oracle/ref_build.py")
     if threads is not None:
         os.environ["OMP_NUM_THREADS"] = str(threads)
     lib = ctypes.CDLL(str(path))
-    n0, n1, n2 = case.Nx
     U = np.zeros((2, *case.shape), case.dtype)
     lo = hi = 0
     aux_parts, prof_parts = [], []
     if case.widths is not None:
         lo, hi = case.widths[0]
-        for d in range(3):
-            plane = int(np.prod([case.shape[e] for e in range(3) if e != d]))
+        for d in range(ndim):
+            plane = int(np.prod([case.shape[e] for e in range(ndim) if e != d]))
             aux_parts.append(np.zeros(3 * (lo + hi) * plane, case.dtype))
             prof_parts.append(case.profiles[d].ravel())
     aux = np.concatenate(aux_parts) if aux_parts else np.zeros(1, case.dtype)
     prof = np.concatenate(prof_parts) if prof_parts else np.zeros(1, case.dtype)
     um = np.zeros((N, case.sensor_lin.size), case.dtype)
-    f = np.ascontiguousarray(case.f[:3])
+    f = np.zeros(3, case.dtype)
+    f[:ndim] = case.f[:ndim]
     signal = np.ascontiguousarray(case.signal[:N], case.dtype)
-    rc = lib.ref_simulate_3d(
-        n0, n1, n2, case.shape[2], _p(U), _p(case.stiff), _p(case.minv), int(case.derive), _p(f),
+    n = np.zeros(3, np.int32)
+    n[:ndim] = case.Nx
+    rc = lib.ref_simulate(
+        _p(n), int(case.shape[-1]), _p(U), _p(case.stiff), _p(case.minv), int(case.derive), _p(f),
         lo, hi, _p(aux), _p(prof), _p(case.source_lin), _p(case.source_weight), _p(signal),
         int(case.source_lin.size), _p(case.sensor_lin), _p(um), int(case.sensor_lin.size), N,
     )
     if rc:
-        raise RuntimeError("ref_simulate_3d refused the case")
+        raise RuntimeError("ref_simulate refused the case")
     return U[(N - 1) % 2], um

@@ -313,3 +313,50 @@ def test_sponge_matches_reference(name):
     sim, design = cases.product_sim(fx)
     field = sponge(sim, design.copy(), width=4, beta=0.3)
     np.testing.assert_array_equal(field, fx["damping_field"])
+
+
+@pytest.mark.parametrize("name", ["grad2d_r4_pml", "grad3d_r2_pml", "grad2d_r4_damped"])
+@pytest.mark.parametrize("precision,stored,tolerance", [("float64", "float32", 1e-6),
+                                                        ("float64", "bfloat16", 1e-2),
+                                                        ("float32", "bfloat16", 1e-2)])
+def test_narrower_strip_trades_exactness_for_memory(name, precision, stored, tolerance):
+    """A strip stored narrower than the field (bfloat16 bits, or float32 under float64)
+    rebuilds the forward field from rounded values: the gradient stays within the
+    reference's own bounds of the stored-history one where the strip shields it
+    (cuwave sensitivity_test.py:1015-1035: 1e-6 for float32 under float64, 1e-2 for
+    bfloat16), on the mass-and-stiffness combination the design sees."""
+    from cuwave_b200 import Source
+    from cuwave_b200.sensitivity import (l2_misfit, reconstruction_nodes, reconstruction_sensitivity,
+                                         sensitivity)
+
+    fx = dict(cases.load(name))
+    fx["precision"] = np.array(precision)
+    sim, design = cases.product_sim(fx)
+    src = Source(fx["source"], fx["signal"].astype(cases.dtype_of(fx)))
+    objective = l2_misfit(fx["observed"].astype(cases.dtype_of(fx)))
+    _, ref, _, _ = sensitivity(sim, src, design.copy(), fx["sensors"], objective)
+    _, got, _, info = reconstruction_sensitivity(sim, src, design.copy(), fx["sensors"], objective,
+                                                 strip_dtype=stored)
+    _, valid = reconstruction_nodes(sim, design.copy())
+    d_mass, d_stiff = sim.parametrization_jacobian(None)
+
+    def combine(g):
+        return (d_mass * g["mass"] + d_stiff * g["stiff"])[valid].double().cpu().numpy()
+
+    a, b = combine(got), combine(ref)
+    rel = float(np.linalg.norm(a - b) / np.linalg.norm(b))
+    assert rel < tolerance, rel
+    if stored == "bfloat16":
+        assert rel > 0, "a bfloat16 strip rounds what it stores"
+
+
+def test_strip_no_narrower_is_refused():
+    from cuwave_b200 import Source
+    from cuwave_b200.sensitivity import l2_misfit, reconstruction_sensitivity
+
+    fx = cases.load("grad2d_r4_pml")
+    sim, design = cases.product_sim(fx)
+    src = Source(fx["source"], fx["signal"])
+    with pytest.raises(ValueError):
+        reconstruction_sensitivity(sim, src, design.copy(), fx["sensors"], l2_misfit(fx["observed"]),
+                                   strip_dtype="float32")

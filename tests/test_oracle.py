@@ -75,6 +75,41 @@ def test_float32_error_against_float64(name):
     assert 0 < err < 1e-5 and 0 < terr < 1e-5, (err, terr)
 
 
+REF_CASES = ["fwd2d_r4", "fwd2d_r4_f64", "fwd2d_r4_pml", "fwd3d_r4_pml"]
+
+
+@pytest.mark.parametrize("level", ["v1", "v3", "v4"])
+@pytest.mark.parametrize("name", REF_CASES)
+def test_reference_build_matches_reference(name, level):
+    """oracle/_ref (the reference's own kernels, compiled by oracle/ref_build.py at each
+    instruction-set level) against the fixtures the reference's Python produced: bit for
+    bit, forward field and traces, so the CPU baseline and the large-grid parity checks
+    that use it run the reference's arithmetic."""
+    import importlib.util
+    import os
+
+    spec = importlib.util.spec_from_file_location("_rb", cases.ROOT / "oracle" / "ref_build.py")
+    rb = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(rb)
+    fx = cases.load(name)
+    tag = "f32" if str(fx["precision"]) == "float32" else "f64"
+    ndim = int(fx["ndim"])
+    path = rb.library_name(ndim, 4, "optimized", str(fx["precision"]), level)
+    if not path.exists():
+        pytest.skip(f"{path.name} not built (oracle/ref_build.py needs the reference tree)")
+    need = dict((t, f) for t, _, f in rb.LEVELS)[level]
+    if not all(f in rb.host_flags() for f in need):
+        pytest.skip(f"this host cannot run {level} code")
+    case = cases.oracle_case(fx)
+    lib = o.ctypes.CDLL(str(path))
+    assert lib.ref_ndim() == ndim and tag in path.name
+    field, traces = o.ref_simulate(case, int(fx["N"]), threads=min(4, os.cpu_count() or 1),
+                                   library=path)
+    Nx = tuple(int(n) for n in fx["Nx"])
+    np.testing.assert_array_equal(field[tuple(slice(0, n) for n in Nx)], fx["field"])
+    np.testing.assert_array_equal(traces, fx["traces"])
+
+
 SUPERPOSITION = sorted(p.stem for p in cases.GOLDEN.glob("sup*.npz"))
 
 

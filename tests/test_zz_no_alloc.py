@@ -79,6 +79,72 @@ def test_static_march_matches_plan_march(name):
         np.testing.assert_array_equal(traces, ref_traces)
 
 
+def test_static_march_builds_its_source_lists_in_the_array():
+    """A heterogeneous stiffness (a ScalarWave design) steps on the row kernel, which folds
+    the sources into the step through per-block lists; with two shots in one op list both
+    lists land in the static array one after the other. Each shot must equal what the
+    plan-based march gives and what the reference gives, on two calls in a row."""
+    from cuwave_b200 import _native as nat
+    from cuwave_b200.wave import flatten_indices, forward_ops, pml_memory, prepare_shot
+
+    lib = nat.library()
+    lib.cwb_march_static.restype = ctypes.c_int
+    fx = cases.load("fwd2d_scalar_r2")
+    sim, design = cases.product_sim(fx)
+    N = int(fx["N"])
+    mat = sim.build_materials(design.copy())
+    assert not mat["uniform"], "the case must have a heterogeneous stiffness"
+    signal = fx["signal"].astype(np.float32)
+    # the fixture's shot, and a second one of two sources elsewhere with its own signal
+    second = np.array([[5, int(fx["Nx"][0]) - 6], [int(fx["Nx"][1]) - 5, 4]], np.int32)
+    signal2 = np.ascontiguousarray(np.stack([signal[:, 0], -0.5 * signal[:, 0]], axis=1))
+    shots = [prepare_shot(sim, mat, fx["source"], signal), prepare_shot(sim, mat, second, signal2)]
+    assert all(s.foldable for s in shots)
+    sensor_lin = flatten_indices(sim, fx["sensors"])
+    dev = torch.device("cuda")
+
+    def marched(run):
+        fields = []
+        ops = []
+        for shot in shots:
+            U = torch.zeros((2, *sim.Nx_padded), dtype=sim.dtype, device=dev)
+            um = torch.zeros((N, sensor_lin.numel()), dtype=sim.dtype, device=dev)
+            ops += forward_ops(sim, mat, nat.level(U, add=0, period=2), nat.level(U, add=1, period=2),
+                               nat.level(U, add=0, period=2), shot, pml_memory(sim, 3, dev),
+                               records=[(sensor_lin, um, 1, 0, nat.STORE_NATIVE)])
+            fields.append((U, um))
+        assert sum(1 for op in ops if op.flags & nat.FOLD_SOURCES) == 2
+        run(ops)
+        torch.cuda.synchronize()
+        return [(U[(N - 1) % 2].cpu().numpy(), um.cpu().numpy()) for U, um in fields]
+
+    ref = marched(lambda ops: sim.plan().march(ops, 0, N))
+    grid = sim.plan().grid
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+    def static(ops):
+        array = (nat.Op * len(ops))(*ops)
+        rc = lib.cwb_march_static(ctypes.byref(grid), array, len(ops), 0, N, stream)
+        assert rc == 0, lib.cwb_last_error().decode()
+
+    logical = tuple(slice(0, int(n)) for n in fx["Nx"])
+    # the second shot through the oracle, the fixture holding only the first
+    case = cases.oracle_case(fx)
+    case.source_lin = cases.flat(fx, second)
+    case.signal = signal2
+    case.source_weight = case.excitation_weights(case.source_lin)
+    oracle_field, oracle_traces = case.forward(N)
+    for call in range(2):
+        got = marched(static)
+        for (field, traces), (rf, rt) in zip(got, ref):
+            np.testing.assert_array_equal(field, rf)
+            np.testing.assert_array_equal(traces, rt)
+        np.testing.assert_array_equal(got[0][0][logical], fx["field"])
+        np.testing.assert_array_equal(got[0][1], fx["traces"])
+        np.testing.assert_array_equal(got[1][0][logical], oracle_field[logical])
+        np.testing.assert_array_equal(got[1][1], oracle_traces)
+
+
 def test_static_march_refuses_lists_past_its_array():
     """A march whose source lists cannot fit the static array is refused, not truncated.
     (A heterogeneous stiffness: its step folds the sources through per-block lists,
