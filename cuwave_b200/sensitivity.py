@@ -12,6 +12,7 @@ the gather inside the step) and the adjoint load (CWB_OP_LOAD).
 
 from __future__ import annotations
 
+import itertools
 import math
 import warnings
 from collections.abc import Callable
@@ -624,36 +625,49 @@ def reconstruction_nodes(sim: Simulation, indicator, span: int | None = None):
 
 
 def segment_split(lo: int, hi: int, free: int) -> int:
-    """Where to snapshot segments lo .. hi with `free` slots: the binomial treeverse split
-    of Griewank & Walther (2000) (cuwave sensitivity.py:229-240)."""
-    r = 0
-    while math.comb(free + r, free) < hi - lo:
-        r += 1
-    return max(lo + 1, hi - math.comb(free - 1 + r, free - 1))
+    """The segment treeverse snapshots next when it must reverse segments lo .. hi - 1
+    with `free` snapshot slots: binomial checkpointing (Griewank & Walther 2000,
+    https://doi.org/10.1145/347837.347846; cuwave sensitivity.py:229-240). With s slots
+    and r replays at most C(s + r, s) segments can be reversed; with the fewest replays
+    r that cover hi - lo segments, the part past the snapshot is what s - 1 slots and r
+    replays cover, C(s - 1 + r, s - 1) segments, so the snapshot sits that far before hi
+    (and at least one segment past lo)."""
+    need = hi - lo
+    replays = next(r for r in itertools.count() if math.comb(free + r, free) >= need)
+    return max(lo + 1, hi - math.comb(free - 1 + replays, free - 1))
 
 
 def checkpoint_schedule(segments: int, slots: int) -> list[tuple]:
-    """Treeverse over `segments` with `slots` snapshots past the initial state (cuwave sensitivity.py:243-269).
+    """The treeverse schedule that reverses `segments` with `slots` snapshots beyond the
+    initial state (the action sequence of cuwave sensitivity.py:243-269).
 
-    Actions in order: ("restore", k), ("store", k), ("drop", k), ("advance", a, b) and
-    ("leaf", k), which replays segment k forwards and reverses it.
+    Actions, in order: ("restore", k) and ("store", k) move segment k's start state
+    between a snapshot and the working slots, ("drop", k) frees it, ("advance", a, b)
+    marches from segment a's start to segment b's, and ("leaf", k) replays segment k
+    forwards and then reverses it.
+
+    Built with an explicit work stack. Reversing lo .. hi - 1 with free slots is: one
+    segment, a leaf; no free slot, every segment from the last down re-marched from lo;
+    otherwise march to the split, snapshot it, reverse the part past it with a slot
+    fewer, drop the snapshot and reverse the part before it with the same slots.
     """
-    actions = []
-
-    def reverse(lo, hi, free):
-        while hi - lo > 1:
-            if free == 0:
-                for k in range(hi - 1, lo, -1):
-                    actions.extend((("restore", lo), ("advance", lo, k), ("leaf", k)))
-                break
+    actions: list[tuple] = []
+    work: list[tuple] = [("reverse", 0, segments, slots)]
+    while work:
+        item = work.pop()
+        if item[0] != "reverse":
+            actions.append(item)
+            continue
+        _, lo, hi, free = item
+        if hi - lo > 1 and free > 0:
             mid = segment_split(lo, hi, free)
-            actions.extend((("restore", lo), ("advance", lo, mid), ("store", mid)))
-            reverse(mid, hi, free - 1)
-            actions.append(("drop", mid))
-            hi = mid
-        actions.extend((("restore", lo), ("leaf", lo)))
-
-    reverse(0, segments, slots)
+            actions += [("restore", lo), ("advance", lo, mid), ("store", mid)]
+            # popped last-in first: the part past the snapshot, its drop, the part before
+            work += [("reverse", lo, mid, free), ("drop", mid), ("reverse", mid, hi, free - 1)]
+            continue
+        for k in range(hi - 1, lo, -1):
+            actions += [("restore", lo), ("advance", lo, k), ("leaf", k)]
+        actions += [("restore", lo), ("leaf", lo)]
     return actions
 
 

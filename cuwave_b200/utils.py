@@ -97,49 +97,53 @@ def interior_slice(sim: Simulation) -> tuple[slice, ...]:
 
 
 def threshold(field, eta: float = 0.5, low: float = 0.0, high: float = 1.0, dtype=None):
-    """`low` below `eta`, `high` from it on, in the field's float dtype (cuwave utils.py:81-96)."""
+    """A grey design snapped to two phases: `low` where it lies below `eta`, `high`
+    everywhere else (a NaN included), as cuwave's utils.threshold (utils.py:81-96).
+
+    The result keeps the field's floating dtype (a float32 design stays float32, the
+    precision the kernels read it in); a non-float field takes the dtype of the two
+    phase values. numpy arrays and torch tensors come back as what they were.
+    """
     if isinstance(field, torch.Tensor):
-        if dtype is None:
-            dtype = field.dtype if field.is_floating_point() else torch.float64
-        return torch.where(field < eta, low, high).to(dtype)
-    field = np.asarray(field)
-    snapped = np.where(field < eta, low, high)
-    if dtype is None:
-        dtype = field.dtype if field.dtype.kind == "f" else snapped.dtype
-    return snapped.astype(dtype)
+        kind = dtype or (field.dtype if field.is_floating_point() else torch.float64)
+        snapped = torch.full(field.shape, high, dtype=kind, device=field.device)
+        snapped[field < eta] = low
+        return snapped
+    values = np.asarray(field)
+    kind = dtype or (values.dtype if values.dtype.kind == "f" else np.result_type(low, high))
+    snapped = np.full(values.shape, high, dtype=kind)
+    snapped[values < eta] = low
+    return snapped
 
 
 def resample(signal, dt: float, dt_new: float, N_new: int | None = None):
-    """Linear resampling from step `dt` to `dt_new`, zero past the end (cuwave utils.py:99-134).
+    """Linear interpolation of a sampled signal (time along axis 0) from step `dt` onto
+    step `dt_new`, zero past its last sample (cuwave utils.py:99-134).
 
-    Works on numpy arrays and torch tensors alike, returning the kind it was given.
+    Output row k sits at input position k * (dt_new / dt), the ratio and the positions
+    in the signal's floating precision (float64 for an integer signal); it blends the
+    two input rows around that position. Without `N_new` the output spans the input.
+    numpy arrays and torch tensors come back as what they were.
     """
-    is_torch = isinstance(signal, torch.Tensor)
-    values = signal if is_torch else np.asarray(signal)
-    steps = values.shape[0]
-    if steps < 2:
-        raise ValueError(f"resampling needs at least two samples, got {steps}")
+    given_torch = isinstance(signal, torch.Tensor)
+    x = signal if given_torch else torch.from_numpy(np.ascontiguousarray(signal))
+    count = x.shape[0]
+    if count < 2:
+        raise ValueError(f"resampling needs at least two samples, got {count}")
     if N_new is None:
-        span = (steps - 1) * dt / dt_new
+        span = (count - 1) * dt / dt_new
         N_new = int(span + 1e-9 * max(1.0, span)) + 1
-    if is_torch:
-        dtype = values.dtype if values.is_floating_point() else torch.float64
-        ratio = torch.tensor(dt_new / dt, dtype=dtype).item()
-        t = torch.arange(N_new, dtype=dtype, device=values.device) * ratio
-        left = torch.clamp(torch.floor(t), 0, steps - 2)
-        index = left.to(torch.int64)
-        vals = values.to(dtype)
-    else:
-        dtype = np.dtype(values.dtype if values.dtype.kind == "f" else np.float64)
-        t = np.arange(N_new, dtype=dtype) * dtype.type(dt_new / dt)
-        left = np.clip(np.floor(t), 0, steps - 2)
-        index = left.astype(np.int32)
-        vals = values
-    weight = t - left
-    if values.ndim > 1:
-        weight = weight.reshape(N_new, *(1,) * (values.ndim - 1))
-    interpolated = (1 - weight) * vals[index] + weight * vals[index + 1]
-    return interpolated * (t.reshape(weight.shape) <= steps - 1)
+    real = x.dtype if x.is_floating_point() else torch.float64
+    ratio = torch.tensor(dt_new / dt, dtype=real)
+    position = torch.arange(N_new, dtype=real, device=x.device) * ratio.to(x.device)
+    base = torch.floor(position).clamp(0, count - 2)
+    frac = (position - base).reshape(N_new, *(1,) * (x.dim() - 1))
+    i = base.to(torch.int64)
+    x = x.to(real) if given_torch else x
+    blended = (1 - frac) * x[i] + frac * x[i + 1]
+    inside = (position <= count - 1).reshape(frac.shape)
+    out = blended * inside
+    return out if given_torch else out.numpy()
 
 
 def line(start, stop, count: int) -> np.ndarray:
@@ -356,116 +360,134 @@ def misfit_gradient(sim: Simulation, sources: Sequence[Source], indicator, senso
 
 # ------------------------------------------------------------------------------ tato
 def energy(sim: Simulation) -> Callable:
-    """Objective: J = 1/2 sum over sensors and steps of p^2, times dx^ndim dt (cuwave utils.py:463-470)."""
-    scale = float(np.prod(sim.dx)) * sim.dt
+    """The objective that scores the energy reaching the sensors (cuwave utils.py:463-470):
+    J = (dx^ndim dt / 2) sum over steps and sensors of p^2, dJ/dp = dx^ndim dt p."""
+    cell_time = float(np.prod(sim.dx)) * sim.dt
 
     def objective(traces):
-        return 0.5 * scale * float(torch.sum(traces**2)), scale * traces
+        gradient = cell_time * traces
+        return 0.5 * cell_time * float(torch.sum(traces**2)), gradient
 
     return objective
 
 
 def response(sim: Simulation, source: Source, indicator, sensors, objective: Callable):
-    """(cost, final field) of one forward pass (cuwave utils.py:473-487)."""
-    wavefield, traces = simulate(sim, source, indicator, sensors=sensors)
-    return objective(traces)[0], wavefield
+    """One shot forward only: its cost and its final field over the logical grid
+    (cuwave utils.py:473-487)."""
+    field, traces = simulate(sim, source, indicator, sensors=sensors)
+    cost, _ = objective(traces)
+    return cost, field
 
 
 def response_gradient(sim: Simulation, source: Source, indicator, sensors, objective: Callable,
                       adjoint: Callable = sensitivity):
-    """Cost of one shot and its reparametrized gradient (cuwave utils.py:490-514)."""
+    """One shot's cost and its gradient on the design field, taken by `adjoint`
+    (`sensitivity`, or `reconstruction_sensitivity` where a stored history does not fit)
+    and mapped from (mass, stiffness) onto the design (cuwave utils.py:490-514)."""
     cost, grads, _, _ = adjoint(sim, source, indicator, sensors, objective)
     return cost, _reparametrize(sim, indicator, grads)
 
 
 # ------------------------------------------------------------------------------ tpto
 def intensity(sim: Simulation, frequencies, weights=None) -> Callable:
-    """Objective: J = sum w |u_hat(f)|^2 over the sensors (cuwave utils.py:518-552).
+    """The objective that scores spectral intensity at the sensors (cuwave utils.py:518-552):
+    J = sum over frequencies and sensors of w |u(f)|^2, u(f) = dt sum_t u(t) exp(-2 pi i f t dt).
 
-    u_hat(f) = dt sum_t u(t) e^{-2 pi i f t dt}, with the phase tables built in float64
-    and cast to the simulation's dtype; the derivative is the same tables read back.
+    The transform is one real matrix, its rows the cosine and the negated sine rows of
+    every frequency (phases in float64, since they reach 1e5 radians over a long run,
+    then rounded to the simulation's precision), so J's derivative is that matrix
+    transposed onto 2 w (Re, Im).
     """
     f = np.atleast_1d(np.asarray(frequencies, dtype=np.float64))
-    t = np.arange(sim.N, dtype=np.float64) * sim.dt
-    phase = 2.0 * np.pi * t[:, None] * f[None, :]
+    phase = 2.0 * np.pi * np.outer(f, np.arange(sim.N, dtype=np.float64) * sim.dt)
     dev = device()
-    cos = torch.as_tensor(np.cos(phase), device=dev).to(sim.dtype)
-    sin = torch.as_tensor(np.sin(phase), device=dev).to(sim.dtype)
-    scale = float(sim.np_dtype(sim.dt))
-    w = 1.0 if weights is None else as_device(weights, sim.dtype)
+    table = torch.as_tensor(np.concatenate([np.cos(phase), -np.sin(phase)]), device=dev).to(sim.dtype)
+    dt = float(sim.np_dtype(sim.dt))
+    count = f.size
+    w = torch.ones((), dtype=sim.dtype, device=dev) if weights is None else as_device(weights, sim.dtype)
 
     def objective(traces):
-        re = scale * (cos.T @ traces)
-        im = -scale * (sin.T @ traces)
+        spectrum = dt * (table @ traces)  # (2F, sensors): the Re rows over the Im rows
+        re, im = spectrum[:count], spectrum[count:]
         cost = float(torch.sum(w * (re * re + im * im)))
-        return cost, 2.0 * scale * (cos @ (w * re) - sin @ (w * im))
+        both = torch.broadcast_to(w, re.shape).repeat(2, 1)
+        return cost, 2.0 * dt * (table.T @ (both * spectrum))
 
     return objective
 
 
 # ------------------------------------------------------------------- time dispersion
 def _warn_low_order(sim: Simulation) -> None:
+    """At space order 2 the leapfrog time error cancels part of the spatial one, so
+    taking it out makes the solution worse: say so."""
     if sim.space_order == 2:
         warnings.warn(
-            "at space_order 2 the leapfrog time error offsets the spatial one, so removing "
-            "it makes the result less accurate; use space_order 4 or higher",
+            "removing the leapfrog time error at space_order 2 makes the result less "
+            "accurate (there it offsets the spatial error); use space_order 4 or higher",
             RuntimeWarning,
             stacklevel=3,
         )
 
 
 def _warp(sim: Simulation, values, offset: int, read: Callable):
-    """The spectrum of `values` re-read at `read(omega)`, back on the same rows (cuwave utils.py:567-590).
+    """`values` (time along axis 0, row n at time (n + offset) dt) with its spectrum moved
+    from each frequency w onto read(w) (NaN: no counterpart, dropped), back on the same
+    rows (cuwave utils.py:567-590).
 
-    A direct transform from the sample times onto the warped frequencies (tables in
-    float64), then an inverse real FFT of twice the length, so the moved samples do not
-    wrap round.
+    The moved spectrum is a non-uniform transform from the sample times onto read(w) over
+    the bins of a real FFT twice the signal's length (so a moved sample cannot wrap round
+    into the kept rows), evaluated as phase matrices in float64 a bounded number of
+    entries at a time, then inverted by that FFT.
     """
-    is_torch = isinstance(values, torch.Tensor)
-    x = values if is_torch else torch.as_tensor(np.asarray(values))
-    rows = x.reshape(x.shape[0], -1)
-    steps = rows.shape[0]
-    size = 2 * steps
-    omega = 2.0 * np.pi * np.fft.rfftfreq(size, sim.dt)
-    target = read(omega)
-    keep = np.isfinite(target)
-    cdtype = torch.complex64 if rows.dtype == torch.float32 else torch.complex128
-    times = torch.as_tensor((np.arange(steps) + offset) * sim.dt, device=rows.device)
-    freqs = torch.as_tensor(np.where(keep, target, 0.0), device=rows.device)
-    crow = rows.to(cdtype)
-    spectrum = torch.empty((omega.size, rows.shape[1]), dtype=cdtype, device=rows.device)
-    block = max(1, 2**23 // steps)
-    for k in range(0, omega.size, block):
-        table = torch.exp(-1j * torch.outer(freqs[k:k + block], times))
-        spectrum[k:k + block] = table.to(cdtype) @ crow
-    shift = torch.as_tensor(keep * np.exp(1j * omega * offset * sim.dt), device=rows.device)
-    out = torch.fft.irfft(spectrum * shift.to(cdtype)[:, None], size, dim=0)[:steps]
-    out = out.to(x.dtype).reshape(x.shape)
-    return out if is_torch else out.numpy()
+    given_torch = isinstance(values, torch.Tensor)
+    x = values if given_torch else torch.from_numpy(np.ascontiguousarray(values))
+    count = x.shape[0]
+    flat = x.reshape(count, -1)
+    length = 2 * count
+    omega = 2.0 * np.pi * np.fft.rfftfreq(length, sim.dt)
+    moved = read(omega)
+    valid = np.isfinite(moved)
+    ctype = torch.complex64 if flat.dtype == torch.float32 else torch.complex128
+    dev = flat.device
+    times = torch.as_tensor((offset + np.arange(count)) * sim.dt, device=dev)
+    targets = torch.as_tensor(np.where(valid, moved, 0.0), device=dev)
+    samples = flat.to(ctype)
+    rows_per_chunk = max(1, (1 << 23) // count)  # phase entries held at once
+    spectrum = torch.cat([
+        torch.exp(-1j * torch.outer(targets[k:k + rows_per_chunk], times)).to(ctype) @ samples
+        for k in range(0, omega.size, rows_per_chunk)
+    ])
+    back = torch.as_tensor(valid * np.exp(1j * omega * offset * sim.dt), device=dev).to(ctype)
+    out = torch.fft.irfft(spectrum * back[:, None], length, dim=0)[:count].to(x.dtype).reshape(x.shape)
+    return out if given_torch else out.numpy()
 
 
 def tdt(sim: Simulation, signal, offset: int = 0):
-    """Time-dispersion transform: the input leapfrog needs for `signal` to come out exact (cuwave utils.py:593-609)."""
+    """The time-dispersion transform (cuwave utils.py:593-609): what leapfrog must be fed
+    for `signal` to come out free of its time error, each frequency w read at the
+    leapfrog's (2 / dt) sin(w dt / 2). offset 0 for a source signal, 1 for a record."""
     _warn_low_order(sim)
-    return _warp(sim, signal, offset, lambda w: 2.0 / sim.dt * np.sin(0.5 * w * sim.dt))
+    return _warp(sim, signal, offset, lambda w: np.sin(0.5 * sim.dt * w) * (2.0 / sim.dt))
 
 
 def itdt(sim: Simulation, record, offset: int = 1):
-    """Inverse of `tdt`, zero above the highest frequency leapfrog carries (cuwave utils.py:612-634)."""
+    """The inverse of `tdt` (cuwave utils.py:612-634): each frequency w read at
+    (2 / dt) arcsin(w dt / 2), nothing where w dt / 2 passes 1 (above what leapfrog can
+    carry at this dt). offset 1 for a record of `simulate`, 0 for a source signal."""
     _warn_low_order(sim)
 
-    def read(omega):
-        half = 0.5 * omega * sim.dt
-        inverse = 2.0 / sim.dt * np.arcsin(np.minimum(half, 1.0))
-        return np.where(half <= 1.0, inverse, np.nan)
+    def read(w):
+        s = 0.5 * sim.dt * w
+        return np.where(s <= 1.0, np.arcsin(np.clip(s, None, 1.0)) * (2.0 / sim.dt), np.nan)
 
     return _warp(sim, record, offset, read)
 
 
 def leapfrog_frequency(sim: Simulation, frequency) -> np.ndarray:
-    """The leapfrog frequency that answers exactly for `frequency` (cuwave utils.py:637-643)."""
+    """The frequency whose leapfrog solution oscillates at `frequency` exactly
+    (cuwave utils.py:637-643): arcsin(pi f dt) / (pi dt), defined below 1 / (pi dt)."""
     _warn_low_order(sim)
-    phase = np.pi * np.asarray(frequency, dtype=np.float64) * sim.dt
-    if np.any(phase >= 1.0):
+    x = np.pi * sim.dt * np.asarray(frequency, dtype=np.float64)
+    if np.any(x >= 1.0):
         raise ValueError(f"{frequency} is above 1 / (pi dt) = {1 / (np.pi * sim.dt):g}")
-    return np.arcsin(phase) / (np.pi * sim.dt)
+    return np.arcsin(x) / (np.pi * sim.dt)

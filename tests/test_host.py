@@ -134,3 +134,73 @@ def test_checkpoint_schedule_reverses_every_segment():
         for slots in range(0, 4):
             leaves = [a[1] for a in checkpoint_schedule(segments, slots) if a[0] == "leaf"]
             assert leaves == list(range(segments - 1, -1, -1))
+
+
+def test_checkpoint_schedule_keeps_its_snapshot_budget():
+    """Every snapshot stored is dropped again, no more than `slots` are held at once, a
+    march starts from the state just restored, and treeverse's replay count is the
+    binomial bound's: a segment is re-marched at most r + 1 times for the fewest r with
+    C(slots + r, slots) >= segments."""
+    import math
+
+    from cuwave_b200.sensitivity import checkpoint_schedule
+
+    for segments in range(1, 60):
+        for slots in range(0, 5):
+            held, restored, marched = set(), None, [0] * segments
+            for action in checkpoint_schedule(segments, slots):
+                if action[0] == "store":
+                    held.add(action[1])
+                    assert len(held) <= slots
+                elif action[0] == "drop":
+                    held.remove(action[1])
+                elif action[0] == "restore":
+                    assert action[1] == 0 or action[1] in held
+                    restored = action[1]
+                elif action[0] == "advance":
+                    assert action[1] == restored
+                    for k in range(action[1], action[2]):
+                        marched[k] += 1
+            assert not held
+            if slots:
+                r = next(r for r in range(segments + 1) if math.comb(slots + r, slots) >= segments)
+                assert max(marched) <= r
+            else:
+                assert max(marched) == segments - 1
+
+
+def test_resample_and_threshold():
+    import torch
+
+    from cuwave_b200.utils import resample, threshold
+
+    x = np.arange(11, dtype=np.float64) * 0.5 + 1.0  # linear: interpolation is exact
+    y = resample(x, 1.0, 0.25)
+    np.testing.assert_allclose(y, 1.0 + 0.5 * 0.25 * np.arange(41), rtol=0, atol=1e-12)
+    z = resample(torch.as_tensor(x), 1.0, 0.5, N_new=30)
+    assert torch.all(z[21:] == 0) and float(z[20]) == x[-1]
+    field = np.array([0.1, 0.5, 0.7, np.nan], np.float32)
+    np.testing.assert_array_equal(threshold(field), np.array([0, 1, 1, 1], np.float32))
+    assert threshold(field).dtype == np.float32
+    assert torch.equal(threshold(torch.as_tensor(field), 0.6, 0.3, 1.0),
+                       torch.tensor([0.3, 0.3, 1.0, 1.0], dtype=torch.float32))
+
+
+def test_time_dispersion_round_trip():
+    """itdt undoes tdt on a signal whose band leapfrog carries, to the truncation of the
+    finite transforms (1e-4 of the peak)."""
+    import warnings
+
+    from cuwave_b200 import AcousticWave
+    from cuwave_b200.signals import ricker
+    from cuwave_b200.utils import itdt, leapfrog_frequency, tdt
+
+    sim = AcousticWave(Nx=(20, 20), dx=(1.0, 1.0), N=400, dt=0.2, space_order=4,
+                       rho1=1.0, rho2=1.0, kappa1=1.0, kappa2=2.0)
+    s = ricker(np.arange(400) * sim.dt, 1.0, 0.2)[:, None]
+    with warnings.catch_warnings():
+        warnings.simplefilter("error")
+        back = itdt(sim, tdt(sim, s, offset=0), offset=0)
+        np.testing.assert_allclose(back, s, rtol=0, atol=2e-4 * np.abs(s).max())
+        f = leapfrog_frequency(sim, 0.2)
+        assert f > 0.2 and np.isclose(np.sin(np.pi * f * sim.dt), np.pi * 0.2 * sim.dt)
