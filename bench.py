@@ -386,7 +386,9 @@ def march_ms(plan, ops, t0: int, steps: int, base: int = 64) -> float:
         return a.elapsed_time(b)
 
     run(base + steps)
-    return min(run(base + steps) - run(base) for _ in range(3)) / steps
+    long = min(run(base + steps) for _ in range(3))
+    short = min(run(base) for _ in range(3))
+    return (long - short) / steps
 
 
 def two_d_kernels(peak: float, steps: int = 200) -> dict:
@@ -738,7 +740,7 @@ def run_ours(args) -> int:
     peak, peak_kind = hbm_peak()
     traffic = profile_traffic(w)
     kernels_2d = two_d_kernels(peak) if args.size == 512 and not args.no_2d and world == 1 else None
-    kernels_3d = three_d_kernels(peak) if args.size == 512 and not args.no_2d and world == 1 else None
+    kernels_3d = three_d_kernels(peak) if args.size == 512 and not args.no_3d and world == 1 else None
     batch = batch_measure() if args.size == 512 and not args.no_batch and world == 1 else None
     shots_2d = shots_measure() if args.size == 512 and not args.no_batch and world == 1 else None
     learned = learned_measure() if args.size == 512 and args.learned and world == 1 else None
@@ -828,6 +830,7 @@ def main(argv=None) -> int:
     parser.add_argument("--ref-sample", type=int, default=3, help="time steps per reference bench step")
     parser.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
     parser.add_argument("--no-2d", action="store_true", help="skip the 2D kernel measurements")
+    parser.add_argument("--no-3d", action="store_true", help="skip the 3D kernel measurements beside the job's")
     parser.add_argument("--no-batch", action="store_true", help="skip the batched 2D march")
     parser.add_argument("--learned", action="store_true",
                         help="also train and time the learned corrector (not yet a gain)")

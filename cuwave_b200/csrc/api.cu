@@ -56,6 +56,7 @@ struct cwb_plan {
   int *err = nullptr;  // raised by a kernel whose bounded wait ran out
   bool tma = true;     // stage planes with tensor-map copies where the layout allows
   bool blocked3 = true;  // uniform-stiffness steps on the register-blocked kernels (CWB_STEP3D=0: off)
+  int flow3 = 1;  // the 3D blocked step without a block barrier per plane (CWB_FLOW3D=0: with; 2: deeper ring)
   cudaStream_t lane = nullptr;
   cudaEvent_t fork = nullptr, join = nullptr;
   int sms = 148;
@@ -713,6 +714,7 @@ int translate(cwb_plan *p, const cwb_op &op, const size_t slot, cudaStream_t str
         sp.ctr = p->ctr;
         s3.s = sp;
         s3.err = p->err;
+        s3.flow = p->flow3;
         out.push_back([s3, R, uniform, grid](cudaStream_t s, bool adv) {
           cwb::Step3Params<T> q = s3;
           if (adv)
@@ -1299,6 +1301,8 @@ int plan_geometry(const cwb_grid &G, cwb_plan &p) {
     p.tma = std::atoi(env) == 0;
   if (const char *env = std::getenv("CWB_STEP3D"))
     p.blocked3 = std::atoi(env) != 0;
+  if (const char *env = std::getenv("CWB_FLOW3D"))
+    p.flow3 = std::atoi(env);
   return CWB_OK;
 }
 

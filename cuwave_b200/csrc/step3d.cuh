@@ -37,13 +37,13 @@ namespace cwb {
 
 constexpr int S3_BX = 64, S3_BY = 16, S3_THREADS = 256;
 
-template <typename T, int R>
+template <typename T, int R, int PF = 3>
 struct Step3Shape {
   static constexpr int V = 16 / (int)sizeof(T);            // values per 16-byte row
   static constexpr int H = (R + V - 1) / V * V;             // axis-2 halo, whole 16-byte rows
   static constexpr int WB = S3_BX + 2 * H;                  // box width
   static constexpr int HB = S3_BY + 2 * R;                  // box height
-  static constexpr int PREFETCH = 3;                        // planes issued past the feed
+  static constexpr int PREFETCH = PF;                       // planes issued past the feed
   static constexpr int NS1 = R + 1 + PREFETCH;              // boxes of u^(t-1)
   static constexpr int NS0 = PREFETCH + 1;                  // tiles of u^(t-2) and 1/m
   static constexpr int BOX_BYTES = (WB * HB * (int)sizeof(T) + 127) / 128 * 128;
@@ -65,6 +65,7 @@ struct Step3Params {
   int level_u1[3];
   int level_u0[3];
   int *err;
+  int flow;  // 1: the barrier-free march (step3d_flow.cuh), 0: the per-plane barrier one
 };
 
 // four values from 16-byte aligned memory

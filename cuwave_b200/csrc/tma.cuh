@@ -63,6 +63,19 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, const unsigned parity) 
   }
 }
 
+// one test of phase `parity`, without the waiting loop: true if it has completed
+__device__ __forceinline__ bool mbar_try(uint64_t *bar, const unsigned parity) {
+  unsigned done;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(done)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return done;
+}
+
 // a 4D tile (x fastest) of `map` at coordinates (x, y, z, w) into shared memory, its
 // bytes completing on `bar`; x * element size must be a multiple of 16 bytes
 __device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, uint64_t *bar,

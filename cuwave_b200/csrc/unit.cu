@@ -11,6 +11,7 @@
 #include "adjoint2d.cuh"
 #include "step2d.cuh"
 #include "step3d.cuh"
+#include "step3d_flow.cuh"
 
 #if !defined(CWB_REAL) || !defined(CWB_NDIM) || !defined(CWB_RADIUS)
 #error "unit.cu is compiled with CWB_REAL, CWB_NDIM and CWB_RADIUS"
@@ -88,8 +89,20 @@ cudaError_t step3d_one(const Step3Params<T> &p, const dim3 grid, cudaStream_t s)
   if constexpr (!Step3Shape<T, R>::SUPPORTED || !U) {
     return cudaErrorInvalidValue;
   } else {
+    // p.flow: 0 the per-plane barrier march, else the barrier-free one (step3d_flow.cuh),
+    // built per (Dirichlet face, derived inertia, damping)
     const size_t smem = Step3Shape<T, R>::SMEM;
-    const auto k = p.s.g.dir ? step3d_kernel<T, R, U, true> : step3d_kernel<T, R, U, false>;
+    const bool hold = p.s.g.dir, derive = p.s.flags & K_DERIVE, damp = p.s.flags & K_DAMP;
+    using K = void (*)(const Step3Params<T>);
+    K k;
+    if (!p.flow)
+      k = hold ? step3d_kernel<T, R, U, true> : step3d_kernel<T, R, U, false>;
+    else if (hold)
+      k = derive ? (damp ? step3d_flow_kernel<T, R, true, true, true> : step3d_flow_kernel<T, R, true, true, false>)
+                 : (damp ? step3d_flow_kernel<T, R, true, false, true> : step3d_flow_kernel<T, R, true, false, false>);
+    else
+      k = derive ? (damp ? step3d_flow_kernel<T, R, false, true, true> : step3d_flow_kernel<T, R, false, true, false>)
+                 : (damp ? step3d_flow_kernel<T, R, false, false, true> : step3d_flow_kernel<T, R, false, false, false>);
     cudaError_t e = allow_smem(k, smem);
     if (e != cudaSuccess)
       return e;
