@@ -446,6 +446,49 @@ def two_d_kernels(peak: float, steps: int = 200) -> dict:
     return out
 
 
+def blocked_2d(peak: float, n: int = 8192, steps: int = 64) -> dict:
+    """The temporally blocked 2D march against the march of one launch a step, on a grid
+    whose fields stream from HBM: n x n, radius 4, Neumann faces, the blob speed model and a
+    source at the centre. Per step: its CUDA-event time, Gpt-updates/s and the fraction of
+    the measured HBM peak the single-step algorithmic bytes (16 B an update) would need at
+    that rate -- above 1 where a pass over HBM serves several steps."""
+    import os
+
+    import torch
+
+    from cuwave_b200 import AcousticWave, _native as nat
+    from cuwave_b200.stencils import stable_dt
+    from cuwave_b200.wave import forward_ops, pml_memory, prepare_shot
+
+    dev = torch.device("cuda")
+    c = blob_speed(n)
+    kappa2 = 0.25
+    dt = 0.5 * stable_dt((1.0, 1.0), float(c.max()), 8, "optimized")
+    N = 2 * (steps + 64) + 8
+    interior = (n - 2) ** 2
+    out = {"grid": [n, n], "space_order": 8}
+    for name, mode in (("single", "0"), ("blocked", "2")):
+        os.environ["CWB_TBLOCK"] = mode
+        try:
+            sim = AcousticWave(Nx=(n, n), dx=(1.0, 1.0), N=N, dt=dt, precision="float32",
+                               space_order=8, rho1=1.0, rho2=1.0, kappa1=1.0, kappa2=kappa2)
+            ind = torch.zeros(sim.Nx_padded, dtype=torch.float32, device=dev)
+            ind[:n, :n] = torch.as_tensor((1.0 / c**2 - 1.0) / (1.0 / kappa2 - 1.0), device=dev)
+            mat = sim.build_materials(ind)
+            shot = prepare_shot(sim, mat, torch.tensor([[n // 2], [n // 2]], device=dev),
+                                torch.zeros((N, 1), dtype=torch.float32, device=dev))
+            U = torch.zeros((2, *sim.Nx_padded), dtype=torch.float32, device=dev)
+            ops = forward_ops(sim, mat, nat.level(U, add=0, period=2), nat.level(U, add=1, period=2),
+                              nat.level(U, add=0, period=2), shot, pml_memory(sim, 3, dev))
+            ms = march_ms(sim.plan(), ops, 0, steps)
+        finally:
+            os.environ.pop("CWB_TBLOCK", None)
+        out[name] = {"ms_per_step": ms, "gpts": interior / (ms / 1e3) / 1e9,
+                     "roofline_frac": 16 * interior / (ms / 1e3) / 1e9 / peak}
+        del U
+    return out
+
+
 def three_d_kernels(peak: float, n: int = 256, steps: int = 100) -> dict:
     """The 3D steps beside the bench job's radius: the forward step for radius 1..8 on an
     n^3 grid with Neumann faces (radius 1..4 on the register-blocked kernel, 5..8 on the
@@ -741,6 +784,7 @@ def run_ours(args) -> int:
     traffic = profile_traffic(w)
     kernels_2d = two_d_kernels(peak) if args.size == 512 and not args.no_2d and world == 1 else None
     kernels_3d = three_d_kernels(peak) if args.size == 512 and not args.no_3d and world == 1 else None
+    blocked = blocked_2d(peak) if args.size == 512 and not args.no_2d and world == 1 else None
     batch = batch_measure() if args.size == 512 and not args.no_batch and world == 1 else None
     shots_2d = shots_measure() if args.size == 512 and not args.no_batch and world == 1 else None
     learned = learned_measure() if args.size == 512 and args.learned and world == 1 else None
@@ -773,6 +817,7 @@ def run_ours(args) -> int:
         "kernel_updates_per_s": interior_updates(w) / (kernel_ms / 1e3) / 1e9,
         "kernels_2d": kernels_2d,
         "kernels_3d": kernels_3d,
+        "blocked_2d": blocked,
         "batch_2d": batch,
         "shots_2d": shots_2d,
         "learned": learned,

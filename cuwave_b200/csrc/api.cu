@@ -20,6 +20,7 @@
 #include "step2d.cuh"
 #include "step3d.cuh"
 #include "step_tma.cuh"
+#include "tblock2d.cuh"
 
 namespace {
 
@@ -67,6 +68,12 @@ struct cwb_plan {
   // array (cwb_march_static) instead of the plan's scratch
   unsigned char *fixed = nullptr;
   size_t fixed_cap = 0, fixed_used = 0;
+  // the temporally blocked 2D march: its second pair of field slots (the passes alternate
+  // between the caller's and these) and its per-block source and receiver lists
+  int tblock = 1;  // temporal blocking on 2D grids too large for L2 (CWB_TBLOCK=0: off; 2: any size)
+  void *tb_fields = nullptr;
+  size_t tb_fields_bytes = 0;
+  Scratch tb_src, tb_rec;
 };
 
 namespace {
@@ -1087,6 +1094,18 @@ cudaError_t march2d_r(const cwb::March2Params<T> &mp, const int R, const int sms
   return cudaErrorInvalidValue;
 }
 
+template <typename T>
+cudaError_t tblock2d_r(const cwb::TBlock2Params<float> &tp, const int R, const dim3 grid,
+                       cudaStream_t s) {
+  switch (R) {
+  case 1: return cwb::tblock2d_unit<T, 1>(tp, grid, s);
+  case 2: return cwb::tblock2d_unit<T, 2>(tp, grid, s);
+  case 3: return cwb::tblock2d_unit<T, 3>(tp, grid, s);
+  case 4: return cwb::tblock2d_unit<T, 4>(tp, grid, s);
+  }
+  return cudaErrorInvalidValue;
+}
+
 // A 2D op list [step, records] of a uniform stiffness (float) runs as one
 // cooperative launch of all its steps, sources and refill folded into the step and a
 // grid-wide barrier before the records (march2d_kernel). Returns false where the list is
@@ -1181,13 +1200,252 @@ bool march2d_path(cwb_plan *p, const cwb_op *ops, const int nops, const int t0, 
   return true;
 }
 
+// per-block lists (CSR) uploaded into a plan scratch: starts[nblocks + 1], entries
+int upload_lists(Scratch &sc, const std::vector<std::vector<int4>> &per, cudaStream_t s) {
+  std::vector<int> starts(per.size() + 1, 0);
+  std::vector<int4> entries;
+  for (size_t b = 0; b < per.size(); ++b) {
+    entries.insert(entries.end(), per[b].begin(), per[b].end());
+    starts[b + 1] = (int)entries.size();
+  }
+  if (entries.empty())
+    entries.push_back(make_int4(-1, -1, 0, 0));
+  if (sc.start_cap < starts.size()) {
+    if (sc.start)
+      cudaFree(sc.start);
+    sc.start = nullptr;
+    if (cudaMalloc(&sc.start, sizeof(int) * starts.size()) != cudaSuccess)
+      return fail(CWB_ERR_ALLOC, "list allocation failed");
+    sc.start_cap = starts.size();
+  }
+  if (sc.entry_cap < entries.size()) {
+    if (sc.entry)
+      cudaFree(sc.entry);
+    sc.entry = nullptr;
+    if (cudaMalloc(&sc.entry, sizeof(int4) * entries.size()) != cudaSuccess)
+      return fail(CWB_ERR_ALLOC, "list allocation failed");
+    sc.entry_cap = entries.size();
+  }
+  CWB_CUDA(cudaMemcpyAsync(sc.start, starts.data(), sizeof(int) * starts.size(),
+                           cudaMemcpyHostToDevice, s));
+  CWB_CUDA(cudaMemcpyAsync(sc.entry, entries.data(), sizeof(int4) * entries.size(),
+                           cudaMemcpyHostToDevice, s));
+  CWB_CUDA(cudaStreamSynchronize(s));
+  return CWB_OK;
+}
+
+// A 2D op list [step (sources and refill folded), records] of a uniform stiffness
+// (float, radius <= 4, no pml, no damping) on a grid too large for L2, its levels the two
+// slots a simulation rotates (u^s in slot (s + add) mod 2), runs TB_K steps per pass over
+// HBM (tblock2d_kernel): the passes alternate between the caller's slots and the plan's
+// second pair, the last result is copied back, and the steps short of a whole pass are
+// left to the per-step march. Returns false where the list is another shape.
+bool tblock2d_path(cwb_plan *p, const cwb_op *ops, const int nops, const int t0, int &steps,
+                   cudaStream_t user, int &rc, int &done) {
+  using T = float;
+  constexpr int K = cwb::TB_K;
+  const Geometry &g = p->geo;
+  const int R = p->grid.radius;
+  done = 0;
+  if (!p->tblock || p->fixed || p->grid.precision != 4 || g.ndim != 2 || R > 4 ||
+      steps < 2 * K || nops < 1 || nops > 1 + cwb::TB_RECORDS || ops[0].kind != CWB_OP_STEP ||
+      ops[0].mat.cells || (ops[0].flags & CWB_PML) || !(ops[0].flags & CWB_FOLD_REFILL) ||
+      ((p->grid.neumann | p->grid.dirichlet) & 15) != 15 || g.n[0] < 3 * R + 2 || g.n[1] < 3 * R + 2)
+    return false;
+  const cwb_op &op = ops[0];
+  // the two slots a simulation rotates: a and c the same slot, b the other
+  const cwb_level &A = op.a, &B = op.b, &C = op.c;
+  if (A.base != B.base || A.base != C.base || A.stride != B.stride || A.stride != C.stride ||
+      A.period != 2 || B.period != 2 || C.period != 2 || A.mul != 1 || B.mul != 1 || C.mul != 1 ||
+      ((A.add - C.add) % 2) != 0 || (((B.add - C.add) % 2 + 2) % 2) != 1)
+    return false;
+  for (int i = 1; i < nops; ++i) {
+    const cwb_points &pt = ops[i].points;
+    if (ops[i].kind != CWB_OP_RECORD || pt.num <= 0 || !pt.lin || !pt.record || pt.store < 0 ||
+        pt.store > 1 || ops[i].a.base != C.base || ops[i].a.stride != C.stride ||
+        ops[i].a.period != 2 || ops[i].a.mul != 1 || ((ops[i].a.add - C.add) % 2) != 0)
+      return false;
+  }
+  cwb::TBlock2Params<T> tp;
+  std::memset(&tp, 0, sizeof tp);
+  cwb::StepParams<T> &sp = tp.s;
+  int flags = 0;
+  bool uniform = false;
+  if (step_setup<T>(p, op, sp, flags, uniform) || !uniform || (flags & (cwb::K_DAMP | cwb::K_PML)))
+    return false;
+  const auto aligned16 = [](const void *ptr, const long long stride_elems) {
+    return reinterpret_cast<uintptr_t>(ptr) % 16 == 0 && (stride_elems * (long long)sizeof(T)) % 16 == 0;
+  };
+  if (!aligned16(A.base, A.stride) || (!(flags & cwb::K_DERIVE) && !aligned16(sp.minv, 0)))
+    return false;
+  const long long rows = g.n[0] - 2, quads = (g.n[1] - 2) / 4 + 1;
+  // grids L2 holds step well one step a launch; this pays where the fields stream from HBM
+  if (p->tblock < 2 && rows * quads * 4 * (long long)sizeof(T) * 3 < 96LL * 1024 * 1024)
+    return false;
+  const int qx_step = cwb::TB_TQ - 2 * K;
+  const int gx = (int)((quads + qx_step - 1) / qx_step);
+  // rows per block: about two waves of blocks two a SM, no fewer than 64
+  const long long want_blocks = 4LL * p->sms;
+  int chunk = (int)std::max<long long>(64, (rows * gx + want_blocks - 1) / want_blocks);
+  if (p->chunk_override > 0)
+    chunk = p->chunk_override;
+  chunk = (int)std::min<long long>(chunk, rows);
+  const int gy = (int)((rows + chunk - 1) / chunk);
+  const int nblocks = gx * gy;
+  const int N0 = g.n[0];
+  sp.flags = flags;
+  sp.ctr = p->ctr;
+  tp.chunk = chunk;
+  tp.qx_step = qx_step;
+  tp.refill = p->grid.neumann | p->grid.dirichlet;
+  rc = CWB_OK;
+  // the per-block lists: sources over the rows and quads a block steps, receivers over
+  // the nodes it owns
+  const auto block_rows = [&](const int by, int &lo, int &hi, int &own_lo, int &own_hi) {
+    own_lo = 1 + by * chunk;
+    own_hi = std::min(N0 - 1, own_lo + chunk);
+    lo = std::max(1, own_lo - (K - 1) * R);
+    hi = std::min(N0 - 1, own_hi + (K - 1) * R);
+  };
+  const auto copy_lin = [&](const int *lin, const int num, std::vector<int> &out) -> int {
+    out.resize(num);
+    if (num) {
+      CWB_CUDA(cudaMemcpyAsync(out.data(), lin, sizeof(int) * num, cudaMemcpyDeviceToHost, user));
+      CWB_CUDA(cudaStreamSynchronize(user));
+    }
+    return CWB_OK;
+  };
+  const int s0 = g.s[0];
+  const cwb_points &src = op.points;
+  if ((op.flags & CWB_FOLD_SOURCES) && src.num > 0) {
+    if (!src.weight || !src.record)
+      return rc = fail(CWB_ERR_ARG, "folded sources need weights and a signal"), true;
+    std::vector<int> lin;
+    if ((rc = copy_lin(src.lin, src.num, lin)))
+      return true;
+    std::vector<std::vector<int4>> per(nblocks);
+    for (int e = 0; e < src.num; ++e) {
+      const int r = lin[e] / s0, x = lin[e] % s0;
+      if (r < 1 || r > N0 - 2 || x < 1 || x > g.n[1] - 2)
+        return rc = fail(CWB_ERR_ARG, "a folded source must sit on an interior node"), true;
+      for (int by = 0; by < gy; ++by) {
+        int lo, hi, olo, ohi;
+        block_rows(by, lo, hi, olo, ohi);
+        if (r < lo || r >= hi)
+          continue;
+        for (int bx = 0; bx < gx; ++bx) {
+          const int q0 = bx * qx_step - K, q = x / 4;
+          if (q >= q0 && q < q0 + cwb::TB_TQ)
+            per[by * gx + bx].push_back(make_int4(r, x, e, 0));
+        }
+      }
+    }
+    if ((rc = upload_lists(p->tb_src, per, user)))
+      return true;
+    tp.src_start = p->tb_src.start;
+    tp.src_entry = p->tb_src.entry;
+    tp.src_weight = static_cast<const T *>(src.weight);
+    tp.signal = static_cast<const T *>(src.record);
+    tp.nsrc = src.num;
+    tp.sig_mul = src.row_mul;
+    tp.sig_add = src.row_add;
+  }
+  tp.nrec = nops - 1;
+  if (tp.nrec) {
+    std::vector<std::vector<int4>> per(nblocks);
+    for (int i = 1; i < nops; ++i) {
+      const cwb_points &pt = ops[i].points;
+      std::vector<int> lin;
+      if ((rc = copy_lin(pt.lin, pt.num, lin)))
+        return true;
+      for (int j = 0; j < pt.num; ++j) {
+        const int r = lin[j] / s0, x = lin[j] % s0;
+        if (r < 1 || r > N0 - 2 || x < 1 || x > g.n[1] - 2)
+          return false;  // a receiver off the interior: the per-step march records it
+        const int by = (r - 1) / chunk, bx = (x / 4) / qx_step;
+        per[by * gx + bx].push_back(make_int4(r, x, j, i - 1));
+      }
+      cwb::TransferParams<T> &rp = tp.rec[i - 1];
+      rp.g = g;
+      rp.lin = pt.lin;
+      rp.record = pt.record;
+      rp.num = pt.num;
+      rp.row_mul = pt.row_mul;
+      rp.row_add = pt.row_add;
+      rp.store = pt.store;
+    }
+    for (auto &v : per)
+      std::stable_sort(v.begin(), v.end(), [](const int4 &a, const int4 &b) { return a.x < b.x; });
+    if ((rc = upload_lists(p->tb_rec, per, user)))
+      return true;
+    tp.rec_start = p->tb_rec.start;
+    tp.rec_entry = p->tb_rec.entry;
+  }
+  // the second pair of slots, a copy of the caller's so the nodes no pass writes (corner
+  // ghosts, padding) match
+  const size_t slot_bytes = (size_t)A.stride * sizeof(T);
+  if (p->tb_fields_bytes < 2 * slot_bytes) {
+    if (p->tb_fields)
+      cudaFree(p->tb_fields);
+    p->tb_fields = nullptr;
+    p->tb_fields_bytes = 0;
+    if (cudaMalloc(&p->tb_fields, 2 * slot_bytes) != cudaSuccess)
+      return rc = fail(CWB_ERR_ALLOC, "temporal blocking's second slots"), true;
+    p->tb_fields_bytes = 2 * slot_bytes;
+  }
+  T *mine[2] = {static_cast<T *>(A.base), static_cast<T *>(A.base) + A.stride};
+  T *other[2] = {static_cast<T *>(p->tb_fields), static_cast<T *>(p->tb_fields) + A.stride};
+  const auto slot_of = [&](const int m) { return ((m + C.add) % 2 + 2) % 2; };  // u^m's slot
+  const int passes = steps / K;
+  const auto run = [&]() -> int {
+    CWB_CUDA(cudaEventRecord(p->fork, user));
+    CWB_CUDA(cudaStreamWaitEvent(p->lane, p->fork, 0));
+    cudaStream_t s = p->lane;
+    CWB_CUDA(cudaMemcpyAsync(other[0], mine[0], 2 * slot_bytes, cudaMemcpyDeviceToDevice, s));
+    for (int k = 0; k < passes; ++k) {
+      const int t = t0 + k * K;
+      T **from = k % 2 ? other : mine, **to = k % 2 ? mine : other;
+      tp.t = t;
+      tp.A = from[slot_of(t - 2)];
+      tp.B = from[slot_of(t - 1)];
+      tp.outA = to[slot_of(t + K - 2)];
+      tp.outB = to[slot_of(t + K - 1)];
+      CWB_CUDA(tblock2d_r<T>(tp, R, dim3(gx, gy), s));
+      ++g_launches;
+    }
+    if (passes % 2)
+      CWB_CUDA(cudaMemcpyAsync(mine[0], other[0], 2 * slot_bytes, cudaMemcpyDeviceToDevice, s));
+    CWB_CUDA(cudaEventRecord(p->join, s));
+    CWB_CUDA(cudaStreamWaitEvent(user, p->join, 0));
+    return CWB_OK;
+  };
+  rc = run();
+  done = passes * K;
+  return true;
+}
+
 template <typename T>
 int march(cwb_plan *p, const cwb_op *ops, const int nops, const int t0, const int steps,
           const int graph, cudaStream_t user) {
   {
-    int rc = CWB_OK;
+    // small 2D grids: all steps in one cooperative launch; large ones: TB_K steps per
+    // pass over HBM (CWB_TBLOCK=2 takes that path first, whatever the grid's size)
+    int rc = CWB_OK, done = 0, left = steps;
+    const auto blocked = [&]() {
+      return sizeof(T) == 4 && tblock2d_path(p, ops, nops, t0, left, user, rc, done);
+    };
+    if (p->tblock == 2 && blocked()) {
+      if (rc || done == steps)
+        return rc;
+      return march<T>(p, ops, nops, t0 + done, steps - done, graph, user);
+    }
     if (march2d_path<T>(p, ops, nops, t0, steps, user, rc))
       return rc;
+    if (p->tblock == 1 && blocked()) {
+      if (rc || done == steps)
+        return rc;
+      return march<T>(p, ops, nops, t0 + done, steps - done, graph, user);
+    }
   }
   std::vector<Launch> launches;
   for (int i = 0; i < nops; ++i) {
@@ -1303,6 +1561,8 @@ int plan_geometry(const cwb_grid &G, cwb_plan &p) {
     p.blocked3 = std::atoi(env) != 0;
   if (const char *env = std::getenv("CWB_FLOW3D"))
     p.flow3 = std::atoi(env);
+  if (const char *env = std::getenv("CWB_TBLOCK"))
+    p.tblock = std::atoi(env);
   return CWB_OK;
 }
 
@@ -1810,12 +2070,16 @@ int cwb_plan_destroy(cwb_plan *p) {
     return CWB_OK;
   if (p->lane)
     cudaStreamSynchronize(p->lane);
+  for (Scratch *s : {&p->tb_src, &p->tb_rec})
+    p->scratch.push_back(*s);
   for (Scratch &s : p->scratch) {
     if (s.start)
       cudaFree(s.start);
     if (s.entry)
       cudaFree(s.entry);
   }
+  if (p->tb_fields)
+    cudaFree(p->tb_fields);
   if (p->ctr)
     cudaFree(p->ctr);
   if (p->err)

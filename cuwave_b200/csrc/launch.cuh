@@ -62,6 +62,13 @@ template <typename T, int R>
 cudaError_t march2d_unit(const March2Params<T> &p, int sms, cudaStream_t stream);
 
 template <typename T>
+struct TBlock2Params;
+// the temporally blocked 2D forward (float, radius <= 4): TB_K steps per pass over HBM,
+// a block of TB_TQ threads a tile
+template <typename T, int R>
+cudaError_t tblock2d_unit(const TBlock2Params<float> &p, dim3 grid, cudaStream_t stream);
+
+template <typename T>
 struct Pml3Params;
 
 // the pml memory update of a 3D step along axis 1 or 2, over its slab nodes (after the

@@ -38,38 +38,10 @@
 
 #include <type_traits>
 
+#include "pairs.cuh"
 #include "step3d.cuh"
 
 namespace cwb {
-
-// ------------------------------------------------------------------ pairs of nodes
-__device__ __forceinline__ unsigned long long f2_bits(const float2 v) {
-  return *reinterpret_cast<const unsigned long long *>(&v);
-}
-__device__ __forceinline__ float2 f2_of(const unsigned long long v) {
-  return *reinterpret_cast<const float2 *>(&v);
-}
-__device__ __forceinline__ float2 p_add(const float2 a, const float2 b) {
-  unsigned long long r;
-  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(f2_bits(a)), "l"(f2_bits(b)));
-  return f2_of(r);
-}
-__device__ __forceinline__ float2 p_sub(const float2 a, const float2 b) {
-  unsigned long long r;
-  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(f2_bits(a)), "l"(f2_bits(b)));
-  return f2_of(r);
-}
-__device__ __forceinline__ float2 p_mul(const float2 a, const float2 b) {
-  unsigned long long r;
-  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(f2_bits(a)), "l"(f2_bits(b)));
-  return f2_of(r);
-}
-__device__ __forceinline__ float2 p_fma(const float2 a, const float2 b, const float2 c) {
-  unsigned long long r;
-  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(f2_bits(a)), "l"(f2_bits(b)), "l"(f2_bits(c)));
-  return f2_of(r);
-}
-__device__ __forceinline__ float2 p_splat(const float v) { return make_float2(v, v); }
 
 // a quad as two pairs, from 16-byte aligned memory and back
 struct Quad2 {
@@ -96,19 +68,6 @@ __device__ __forceinline__ void set_lane(Quad2 &v, const int i, const float x) {
     v.hi.x = x;
   else
     v.hi.y = x;
-}
-
-// D+ of a pair: u(1) - uc, times w0 (R > 1), then w_{k-1} (u(k) - u(1-k)) fused in for
-// k = 2 .. R (dplus in step.cuh, lane by lane)
-template <int R, class Tap>
-__device__ __forceinline__ float2 p_dplus(const Tap &u, const float2 uc, const float2 *w) {
-  float2 d = p_sub(u(1), uc);
-  if (R > 1)
-    d = p_mul(w[0], d);
-#pragma unroll
-  for (int k = 2; k <= R; ++k)
-    d = p_fma(w[k - 1], p_sub(u(k), u(1 - k)), d);
-  return d;
 }
 
 // one warp's count past a stage; true for the warp that completes the count of `warps`

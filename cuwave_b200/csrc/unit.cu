@@ -12,6 +12,7 @@
 #include "step2d.cuh"
 #include "step3d.cuh"
 #include "step3d_flow.cuh"
+#include "tblock2d.cuh"
 
 #if !defined(CWB_REAL) || !defined(CWB_NDIM) || !defined(CWB_RADIUS)
 #error "unit.cu is compiled with CWB_REAL, CWB_NDIM and CWB_RADIUS"
@@ -181,6 +182,21 @@ cudaError_t march2d_unit(const March2Params<T> &mp, const int sms, cudaStream_t 
 }
 
 template <typename T, int R>
+cudaError_t tblock2d_unit(const TBlock2Params<float> &p, const dim3 grid, cudaStream_t s) {
+  if constexpr (sizeof(T) != 4 || R > 4) {
+    return cudaErrorInvalidValue;
+  } else {
+    const auto k = p.s.g.dir ? tblock2d_kernel<R, TB_K, true> : tblock2d_kernel<R, TB_K, false>;
+    const size_t smem = tblock_smem<R, TB_K>();
+    cudaError_t e = allow_smem(k, smem);
+    if (e != cudaSuccess)
+      return e;
+    k<<<grid, TB_TQ * TB_K, smem, s>>>(p);
+    return cudaGetLastError();
+  }
+}
+
+template <typename T, int R>
 cudaError_t adjoint2d_unit(const AdjointParams<T> &p, const int mode, const dim3 grid,
                            cudaStream_t s) {
   if constexpr (!Adj2Shape<T, R>::SUPPORTED) {
@@ -264,6 +280,8 @@ template cudaError_t batch2d_unit<CWB_REAL, CWB_RADIUS>(const Batch2Params<CWB_R
                                                         cudaStream_t);
 template cudaError_t march2d_unit<CWB_REAL, CWB_RADIUS>(const March2Params<CWB_REAL> &, int,
                                                          cudaStream_t);
+template cudaError_t tblock2d_unit<CWB_REAL, CWB_RADIUS>(const TBlock2Params<float> &, dim3,
+                                                          cudaStream_t);
 template cudaError_t adjoint2d_unit<CWB_REAL, CWB_RADIUS>(const AdjointParams<CWB_REAL> &, int,
                                                           dim3, cudaStream_t);
 template cudaError_t adjoint2d_pml_unit<CWB_REAL, CWB_RADIUS>(const AdjointParams<CWB_REAL> &,
