@@ -347,4 +347,127 @@ __global__ void __launch_bounds__(BX *BY) adjoint_kernel(const AdjointParams<T> 
   finish_step(p.ctr, flags & K_ADV);
 }
 
+// The nodes the 3D pml transpose reaches: those within R of a lined axis' slab, as three
+// disjoint regions -- the planes axis 0's slabs reach, whole; in the planes between, the
+// rows axis 1's reach, whole; in the rest, the columns axis 2's reach. `lo[d]` is the last
+// reached index near the low wall (0: none) and `hi[d]` the first near the high one
+// (n[d] - 1: none); the host merges ranges that meet.
+struct Adj3Reach {
+  int lo[3], hi[3];
+};
+
+constexpr int A3P_THREADS = 256;
+
+// The pml transpose of the 3D adjoint step, after the march has written lambda^n (and
+// g_mass) without it: node by node over the reached nodes, each lined axis in turn, the
+// taps of the memories' c+ and c- rows around the node summed in stencil order, then
+// the reads past the walls that land on it folded back (odd on a Dirichlet face), scaled
+// by 1/m and the wall cells' half weights; lambda^n takes the sum, g_mass its share
+// against u^n (pml_adjoint_kernel and pml_tap, scalar_sensitivity.cu:545-597, 237-251,
+// after adjoint_gradient_kernel's update, in the order cuwave launches them). The same
+// gather, in the same order, as the one adjoint_kernel runs inline.
+template <typename T, int R, bool UNIF, int MODE>
+__global__ void __launch_bounds__(A3P_THREADS) adjoint3d_pml_kernel(const AdjointParams<T> p,
+                                                                    const Adj3Reach reach) {
+  constexpr bool GR = MODE == MODE_STEP_GRAD;
+  const Geometry &g = p.g;
+  const int t = step_index(p.ctr);
+  const int n0 = g.n[0] - 2, n1 = g.n[1] - 2, n2 = g.n[2] - 2;  // interior extents
+  // reached and unreached counts along each axis
+  int rc[3], uc_[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    rc[d] = reach.lo[d] + (g.n[d] - 1 - reach.hi[d]);
+    uc_[d] = g.n[d] - 2 - rc[d];
+  }
+  const long long nA = (long long)rc[0] * n1 * n2;
+  const long long nB = (long long)uc_[0] * rc[1] * n2;
+  const long long nC = (long long)uc_[0] * uc_[1] * rc[2];
+  long long k = (long long)blockIdx.x * A3P_THREADS + threadIdx.x;
+  // index j of a reached (or unreached) coordinate along axis d
+  const auto reached_at = [&](const int d, const int j) {
+    return j < reach.lo[d] ? 1 + j : reach.hi[d] + (j - reach.lo[d]);
+  };
+  const auto unreached_at = [&](const int d, const int j) { return reach.lo[d] + 1 + j; };
+  int A[3] = {-1, -1, -1};
+  if (k < nA) {
+    A[2] = 1 + (int)(k % n2);
+    k /= n2;
+    A[1] = 1 + (int)(k % n1);
+    A[0] = reached_at(0, (int)(k / n1));
+  } else if ((k -= nA) < nB) {
+    A[2] = 1 + (int)(k % n2);
+    k /= n2;
+    A[1] = reached_at(1, (int)(k % rc[1]));
+    A[0] = unreached_at(0, (int)(k / rc[1]));
+  } else if ((k -= nB) < nC) {
+    A[2] = reached_at(2, (int)(k % rc[2]));
+    k /= rc[2];
+    A[1] = unreached_at(1, (int)(k % uc_[1]));
+    A[0] = unreached_at(0, (int)(k / uc_[1]));
+  }
+  if (A[0] >= 0) {
+    T *l0 = level<T>(p.l0, t);
+    const long long idx = (long long)A[0] * g.s[0] + (long long)A[1] * g.s[1] + A[2];
+    T mi;
+    if (p.flags & K_DERIVE)
+      mi = (T)1 / (UNIF ? p.sconst : p.stiff[idx]);
+    else
+      mi = p.minv[idx];
+    const T wcell = cell_weight<T>(g, A);
+    T ln = l0[idx];
+    T gm = GR ? p.g_mass[idx] : (T)0;
+    const T uc = GR ? level<T>(p.u1, t)[idx] : (T)0;
+#pragma unroll 1
+    for (int d = 0; d < 3; ++d) {
+      const int lo_d = g.lo[d], hi_d = g.hi[d];
+      if (!(lo_d + hi_d))
+        continue;
+      const int a = A[d], N = g.n[d];
+      const bool reached = (lo_d && a >= 1 && a <= lo_d + R) ||
+                           (hi_d && a <= N - 2 && a >= N - 1 - (hi_d + R));
+      if (!reached)
+        continue;
+      const T *mem = p.mem[d];
+      const int sz = p.memrow[d];
+      int B[3] = {A[0], A[1], A[2]};
+      const auto tap = [&](const int ai, const int q) -> T {
+        const int r = slab_row(ai, N, lo_d, hi_d);
+        B[d] = ai;
+        const int i = slab_index(g, d, r, B);
+        return mem[3 * sz + i] * plus_tap<T, R>(p.w, q) +
+               mem[4 * sz + i] * minus_tap<T, R>(p.w, q);
+      };
+      T sum = (T)0;
+#pragma unroll 1
+      for (int m = -R; m <= R; ++m)
+        if (slab_row(a + m, N, lo_d, hi_d) >= 0)
+          sum += tap(a + m, -m);
+#pragma unroll 1
+      for (int high = 0; high < 2; ++high) {
+        // the reads past the wall that land on a, folded back, odd on a Dirichlet face
+        const int ghost = high ? 2 * (N - 2) - a : 2 - a;
+        if (high ? ghost < N - 1 : ghost > 0)
+          continue;
+        T fold = (T)0;
+#pragma unroll 1
+        for (int kk = 1; kk <= R; ++kk) {
+          const int ai = high ? N - 1 - kk : kk;
+          if (slab_row(ai, N, lo_d, hi_d) >= 0 && ghost - ai >= -R && ghost - ai <= R)
+            fold += tap(ai, ghost - ai);
+        }
+        sum += ((g.dir >> (2 * d + high)) & 1) ? -fold : fold;
+      }
+      const T delta = mi * sum / wcell;
+      ln += delta;
+      if (GR)
+        gm -= p.mf * uc * delta;
+    }
+    l0[idx] = ln;
+    if (GR)
+      p.g_mass[idx] = gm;
+  }
+  finish_step(p.ctr, p.flags & K_ADV);
+}
+
 }  // namespace cwb

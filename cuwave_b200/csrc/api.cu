@@ -71,6 +71,7 @@ struct cwb_plan {
   // the temporally blocked 2D march: its second pair of field slots (the passes alternate
   // between the caller's and these) and its per-block source and receiver lists
   int tblock = 1;  // temporal blocking on 2D grids too large for L2 (CWB_TBLOCK=0: off; 2: any size)
+  bool adj_split = true;  // the 3D adjoint's pml transpose as a launch of its own (CWB_ADJSPLIT=0: inline)
   void *tb_fields = nullptr;
   size_t tb_fields_bytes = 0;
   Scratch tb_src, tb_rec;
@@ -462,6 +463,23 @@ cudaError_t adjoint2d_pml_r(const cwb::AdjointParams<T> &p, const cwb::Adj2Reach
   case 2: return cwb::adjoint2d_pml_unit<T, 2>(p, reach, mode, grid, s);
   case 3: return cwb::adjoint2d_pml_unit<T, 3>(p, reach, mode, grid, s);
   case 4: return cwb::adjoint2d_pml_unit<T, 4>(p, reach, mode, grid, s);
+  }
+  return cudaErrorInvalidValue;
+}
+
+template <typename T>
+cudaError_t adjoint3d_pml_r(const cwb::AdjointParams<T> &p, const cwb::Adj3Reach &reach,
+                            const int R, const bool u, const int mode, const dim3 grid,
+                            cudaStream_t s) {
+  switch (R) {
+  case 1: return cwb::adjoint3d_pml_unit<T, 1>(p, reach, u, mode, grid, s);
+  case 2: return cwb::adjoint3d_pml_unit<T, 2>(p, reach, u, mode, grid, s);
+  case 3: return cwb::adjoint3d_pml_unit<T, 3>(p, reach, u, mode, grid, s);
+  case 4: return cwb::adjoint3d_pml_unit<T, 4>(p, reach, u, mode, grid, s);
+  case 5: return cwb::adjoint3d_pml_unit<T, 5>(p, reach, u, mode, grid, s);
+  case 6: return cwb::adjoint3d_pml_unit<T, 6>(p, reach, u, mode, grid, s);
+  case 7: return cwb::adjoint3d_pml_unit<T, 7>(p, reach, u, mode, grid, s);
+  case 8: return cwb::adjoint3d_pml_unit<T, 8>(p, reach, u, mode, grid, s);
   }
   return cudaErrorInvalidValue;
 }
@@ -920,12 +938,41 @@ int translate(cwb_plan *p, const cwb_op &op, const size_t slot, cudaStream_t str
     }
     dim3 grid;
     stencil_grid(p, grid, ap.chunk);
-    out.push_back([ap, ndim, R, uniform, mode, grid](cudaStream_t s, bool adv) {
-      cwb::AdjointParams<T> q = ap;
+    // 3D with a pml: the march without the pml transpose, which a launch of its own then
+    // gathers over the nodes within R of a slab (the same gather, in the same order)
+    const bool split = ndim == 3 && (flags & cwb::K_PML) && mode != cwb::MODE_GRAD && p->adj_split;
+    cwb::AdjointParams<T> am = ap;
+    if (split)
+      am.flags &= ~cwb::K_PML;
+    out.push_back([am, ndim, R, uniform, mode, grid](cudaStream_t s, bool adv) {
+      cwb::AdjointParams<T> q = am;
       if (adv)
         q.flags |= cwb::K_ADV;
       return adjoint_dispatch<T>(q, ndim, R, uniform, mode, grid, s);
     });
+    if (split) {
+      cwb::Adj3Reach reach;
+      long long counts[3][2];
+      for (int d = 0; d < 3; ++d) {
+        const int N = g.n[d];
+        reach.lo[d] = g.lo[d] ? std::min(g.lo[d] + R, N - 2) : 0;
+        reach.hi[d] = g.hi[d] ? std::max(N - 1 - (g.hi[d] + R), 1) : N - 1;
+        if (reach.lo[d] >= reach.hi[d])
+          reach.lo[d] = N - 2, reach.hi[d] = N - 1;
+        counts[d][0] = reach.lo[d] + (N - 1 - reach.hi[d]);  // reached
+        counts[d][1] = N - 2 - counts[d][0];                 // not
+      }
+      const long long nodes = counts[0][0] * (g.n[1] - 2) * (g.n[2] - 2) +
+                              counts[0][1] * counts[1][0] * (g.n[2] - 2) +
+                              counts[0][1] * counts[1][1] * counts[2][0];
+      const dim3 pgrid((unsigned)std::max<long long>(1, (nodes + cwb::A3P_THREADS - 1) / cwb::A3P_THREADS));
+      out.push_back([ap, reach, R, uniform, mode, pgrid](cudaStream_t s, bool adv) {
+        cwb::AdjointParams<T> q = ap;
+        if (adv)
+          q.flags |= cwb::K_ADV;
+        return adjoint3d_pml_r<T>(q, reach, R, uniform, mode, pgrid, s);
+      });
+    }
     return CWB_OK;
   }
   case CWB_OP_FRECHET: {
@@ -1563,6 +1610,8 @@ int plan_geometry(const cwb_grid &G, cwb_plan &p) {
     p.flow3 = std::atoi(env);
   if (const char *env = std::getenv("CWB_TBLOCK"))
     p.tblock = std::atoi(env);
+  if (const char *env = std::getenv("CWB_ADJSPLIT"))
+    p.adj_split = std::atoi(env) != 0;
   return CWB_OK;
 }
 

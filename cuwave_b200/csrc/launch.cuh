@@ -79,6 +79,11 @@ cudaError_t pml3d_unit(const Pml3Params<T> &p, int axis, dim3 grid, cudaStream_t
 template <typename T, int NDIM, int R>
 cudaError_t adjoint_unit(const AdjointParams<T> &p, bool uniform, int mode, dim3 grid,
                          cudaStream_t stream);
+struct Adj3Reach;
+// the 3D adjoint's pml transpose, a launch after the march over the nodes within R of a slab
+template <typename T, int R>
+cudaError_t adjoint3d_pml_unit(const AdjointParams<T> &p, const Adj3Reach &reach, bool uniform,
+                               int mode, dim3 grid, cudaStream_t stream);
 
 template <typename T>
 cudaError_t launch_transfer(int kind, const TransferParams<T> &p, T *g_mass, int faces,

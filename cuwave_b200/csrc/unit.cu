@@ -267,6 +267,23 @@ cudaError_t adjoint_unit(const AdjointParams<T> &p, const bool u, const int mode
            : adjoint_one<T, NDIM, R, false, MODE_GRAD>(p, grid, s);
 }
 
+#if CWB_NDIM == 3
+template <typename T, int R>
+cudaError_t adjoint3d_pml_unit(const AdjointParams<T> &p, const Adj3Reach &reach, const bool u,
+                               const int mode, const dim3 grid, cudaStream_t s) {
+  if (mode == MODE_STEP_GRAD)
+    u ? adjoint3d_pml_kernel<T, R, true, MODE_STEP_GRAD><<<grid, A3P_THREADS, 0, s>>>(p, reach)
+      : adjoint3d_pml_kernel<T, R, false, MODE_STEP_GRAD><<<grid, A3P_THREADS, 0, s>>>(p, reach);
+  else
+    u ? adjoint3d_pml_kernel<T, R, true, MODE_STEP><<<grid, A3P_THREADS, 0, s>>>(p, reach)
+      : adjoint3d_pml_kernel<T, R, false, MODE_STEP><<<grid, A3P_THREADS, 0, s>>>(p, reach);
+  return cudaGetLastError();
+}
+template cudaError_t adjoint3d_pml_unit<CWB_REAL, CWB_RADIUS>(const AdjointParams<CWB_REAL> &,
+                                                               const Adj3Reach &, bool, int, dim3,
+                                                               cudaStream_t);
+#endif
+
 template cudaError_t step_unit<CWB_REAL, CWB_NDIM, CWB_RADIUS>(const StepParams<CWB_REAL> &,
                                                                bool, dim3, cudaStream_t);
 template cudaError_t step_tma_unit<CWB_REAL, CWB_NDIM, CWB_RADIUS>(
