@@ -532,8 +532,8 @@ def three_d_kernels(peak: float, n: int = 256, steps: int = 100) -> dict:
         if R == 4:
             V = torch.zeros((N + 2, *sim.Nx_padded), dtype=torch.float32, device=dev)
             P = torch.zeros((2, *sim.Nx_padded), dtype=torch.float32, device=dev)
-            sensors = torch.tensor([[20] * 64, list(range(20, 20 + 64 * 3, 3)), [n // 2] * 64],
-                                   dtype=torch.int32, device=dev)
+            cols = np.linspace(20, n - 21, 64).round().astype(int).tolist()
+            sensors = torch.tensor([[20] * 64, cols, [n // 2] * 64], dtype=torch.int32, device=dev)
             lin = flatten_indices(sim, sensors)
             adj_signal = torch.zeros((N, 64), dtype=torch.float32, device=dev)
             aops = _adjoint_ops(sim, mat, P, pml_memory(sim, 5, dev), u_level=nat.level(V, mul=-1, add=N + 1),
@@ -879,7 +879,23 @@ def main(argv=None) -> int:
     parser.add_argument("--no-batch", action="store_true", help="skip the batched 2D march")
     parser.add_argument("--learned", action="store_true",
                         help="also train and time the learned corrector (not yet a gain)")
+    parser.add_argument("--case", choices=("kernels_2d", "kernels_3d", "blocked_2d"),
+                        help="run one of the kernel measurements alone and print it (profiling)")
+    parser.add_argument("--case-size", type=int, default=None, help="grid nodes per axis of --case")
     args = parser.parse_args(argv)
+    if args.case:
+        import torch
+
+        torch.cuda.set_device(0)
+        peak = hbm_peak()[0]
+        if args.case == "kernels_2d":
+            out = two_d_kernels(peak)
+        elif args.case == "kernels_3d":
+            out = three_d_kernels(peak, n=args.case_size or 256)
+        else:
+            out = blocked_2d(peak, n=args.case_size or 8192)
+        print(json.dumps(out))
+        return 0
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)
