@@ -828,7 +828,9 @@ def run_ours(args) -> int:
 
 def step_kernel_name() -> str:
     if os.environ.get("CWB_STEP3D", "1") != "0" and os.environ.get("CWB_NO_TMA", "0") == "0":
-        return ("one march step: step3d_kernel<float,4,uniform> (fd + axis-0 pml) + "
+        step = ("step3d_flow_kernel<float,4>" if os.environ.get("CWB_FLOW3D", "1") != "0"
+                else "step3d_kernel<float,4,uniform>")
+        return (f"one march step: {step} (fd + axis-0 pml) + "
                 "pml_axis1_kernel + pml_axis2_kernel (axes 1-2) + excite_kernel + refill_kernel")
     return "step_tma_kernel<float,3,4,uniform> (row step: fd + pml + sources + refill)"
 
