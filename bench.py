@@ -607,6 +607,48 @@ def batch_measure(count: int = 64, steps: int = 300) -> dict:
     return out
 
 
+def sensitivity_e2e(kernels: dict | None, n: int = 2048, steps: int = 300) -> dict:
+    """The 2D gradient job end to end through `sensitivity` (forward with its history,
+    the traces' misfit, the adjoint with the gradients): the first call (plan, CUDA
+    graphs, the history's allocation) and the best of three warm calls, timed with CUDA
+    events, against the march kernels alone (the forward and adjoint steps of
+    `kernels_2d` at the same grid, times the steps)."""
+    import torch
+
+    from cuwave_b200 import Source, simulate
+    from cuwave_b200.sensitivity import l2_misfit, sensitivity
+
+    w = sensitivity_workload(n, steps)
+    sim = make_sim_2d(w)
+    dev = torch.device("cuda")
+    src = Source(torch.as_tensor(w["source"], device=dev), torch.as_tensor(w["signal"], device=dev))
+    sens = torch.as_tensor(w["sensors"], device=dev)
+    _, observed = simulate(sim, src, torch.as_tensor(w["indicator_obs"], device=dev).clone(), sens)
+    objective = l2_misfit(observed)
+    ind = torch.as_tensor(w["indicator"], device=dev)
+
+    def timed() -> float:
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record()
+        cost, grads, _, _ = sensitivity(sim, src, ind.clone(), sens, objective)
+        b.record()
+        torch.cuda.synchronize()
+        assert bool(torch.isfinite(grads["mass"]).all()) and np.isfinite(float(cost))
+        return a.elapsed_time(b)
+
+    first = timed()
+    warm = min(timed() for _ in range(3))
+    updates = 2 * steps * (n - 2) ** 2  # forward and adjoint
+    out = {"grid": [n, n], "steps": steps, "pml": w["width"], "first_call_ms": first, "warm_ms": warm,
+           "gpts": updates / (warm / 1e3) / 1e9}
+    entry = (kernels or {}).get("sensitivity_2d_2048")
+    if entry and n == 2048:
+        kernel_ms = steps * (entry["forward_ms_per_step"] + entry["adjoint_ms_per_step"])
+        out.update({"kernels_ms": kernel_ms, "over_kernels": warm / kernel_ms})
+    return out
+
+
 def shots_measure(count: int = 96, steps: int = 2000, n: int = 1024) -> dict:
     """A multi-shot gradient: `count` shots on a shared n^2 grid (blob speeds, radius 4),
     sources evenly spaced along the top, 256 receivers 50 cells down, `steps` steps;
@@ -783,6 +825,7 @@ def run_ours(args) -> int:
     peak, peak_kind = hbm_peak()
     traffic = profile_traffic(w)
     kernels_2d = two_d_kernels(peak) if args.size == 512 and not args.no_2d and world == 1 else None
+    sens_2d = sensitivity_e2e(kernels_2d) if kernels_2d is not None else None
     kernels_3d = three_d_kernels(peak) if args.size == 512 and not args.no_3d and world == 1 else None
     blocked = blocked_2d(peak) if args.size == 512 and not args.no_2d and world == 1 else None
     batch = batch_measure() if args.size == 512 and not args.no_batch and world == 1 else None
@@ -816,6 +859,7 @@ def run_ours(args) -> int:
         "clocks": clock,
         "kernel_updates_per_s": interior_updates(w) / (kernel_ms / 1e3) / 1e9,
         "kernels_2d": kernels_2d,
+        "sensitivity_2d": sens_2d,
         "kernels_3d": kernels_3d,
         "blocked_2d": blocked,
         "batch_2d": batch,

@@ -170,11 +170,13 @@ def test_uniform_stiffness_path_matches_oracle():
 @pytest.mark.parametrize("R,dirichlet,pml,damping", [
     (1, 0b000000, 0, False), (2, 0b100110, 0, False), (3, 0b011001, 3, False),
     (4, 0b100110, 4, False), (4, 0b000000, 0, True), (4, 0b111111, 0, False), (2, 0b010101, 6, False),
+    (4, 0b011010, 13, False), (3, 0b000000, 23, False),
 ])
 def test_blocked_uniform_step_matches_oracle(R, dirichlet, pml, damping):
     """Several 64 x 16 tiles and 32-plane chunks, an axis-2 extent with padding, Dirichlet
     and Neumann faces, pml slabs, damping and folded sources on the blocked 3D kernel of a
-    uniform stiffness."""
+    uniform stiffness. Slabs of 13 and 23 cells give the axis-1 pml kernel several
+    segments of rows a side, the last one short."""
     case, meta = _random_case(3, R, dirichlet=dirichlet, pml=pml, uniform=True, damping=damping,
                               seed=11 + R, nsrc=6, nsens=9, Nx=(45, 37, 139))
     field, traces = _product(case, meta)
