@@ -74,6 +74,8 @@ struct cwb_plan {
   bool adj_split = true;  // the 3D adjoint's pml transpose as a launch of its own (CWB_ADJSPLIT=0: inline)
   void *tb_fields = nullptr;
   size_t tb_fields_bytes = 0;
+  void *tb_psi = nullptr;  // temporal blocking with a pml: the levels' copies of the memory
+  size_t tb_psi_bytes = 0;
   Scratch tb_src, tb_rec;
 };
 
@@ -1282,11 +1284,12 @@ int upload_lists(Scratch &sc, const std::vector<std::vector<int4>> &per, cudaStr
 }
 
 // A 2D op list [step (sources and refill folded), records] of a uniform stiffness
-// (float, radius <= 4, no pml, no damping) on a grid too large for L2, its levels the two
-// slots a simulation rotates (u^s in slot (s + add) mod 2), runs TB_K steps per pass over
-// HBM (tblock2d_kernel): the passes alternate between the caller's slots and the plan's
-// second pair, the last result is copied back, and the steps short of a whole pass are
-// left to the per-step march. Returns false where the list is another shape.
+// (float, radius <= 4, no damping; a pml or none) on a grid too large for L2, its levels
+// the two slots a simulation rotates (u^s in slot (s + add) mod 2), runs TB_K steps per
+// pass over HBM (tblock2d_kernel): the passes alternate between the caller's slots and
+// the plan's second pair (the pml memory around a ring of K + 1 copies), the last result
+// is copied back, and the steps short of a whole pass are left to the per-step march.
+// Returns false where the list is another shape.
 bool tblock2d_path(cwb_plan *p, const cwb_op *ops, const int nops, const int t0, int &steps,
                    cudaStream_t user, int &rc, int &done) {
   using T = float;
@@ -1296,7 +1299,7 @@ bool tblock2d_path(cwb_plan *p, const cwb_op *ops, const int nops, const int t0,
   done = 0;
   if (!p->tblock || p->fixed || p->grid.precision != 4 || g.ndim != 2 || R > 4 ||
       steps < 2 * K || nops < 1 || nops > 1 + cwb::TB_RECORDS || ops[0].kind != CWB_OP_STEP ||
-      ops[0].mat.cells || (ops[0].flags & CWB_PML) || !(ops[0].flags & CWB_FOLD_REFILL) ||
+      ops[0].mat.cells || !(ops[0].flags & CWB_FOLD_REFILL) ||
       ((p->grid.neumann | p->grid.dirichlet) & 15) != 15 || g.n[0] < 3 * R + 2 || g.n[1] < 3 * R + 2)
     return false;
   const cwb_op &op = ops[0];
@@ -1318,7 +1321,7 @@ bool tblock2d_path(cwb_plan *p, const cwb_op *ops, const int nops, const int t0,
   cwb::StepParams<T> &sp = tp.s;
   int flags = 0;
   bool uniform = false;
-  if (step_setup<T>(p, op, sp, flags, uniform) || !uniform || (flags & (cwb::K_DAMP | cwb::K_PML)))
+  if (step_setup<T>(p, op, sp, flags, uniform) || !uniform || (flags & cwb::K_DAMP))
     return false;
   const auto aligned16 = [](const void *ptr, const long long stride_elems) {
     return reinterpret_cast<uintptr_t>(ptr) % 16 == 0 && (stride_elems * (long long)sizeof(T)) % 16 == 0;
@@ -1326,8 +1329,11 @@ bool tblock2d_path(cwb_plan *p, const cwb_op *ops, const int nops, const int t0,
   if (!aligned16(A.base, A.stride) || (!(flags & cwb::K_DERIVE) && !aligned16(sp.minv, 0)))
     return false;
   const long long rows = g.n[0] - 2, quads = (g.n[1] - 2) / 4 + 1;
-  // grids L2 holds step well one step a launch; this pays where the fields stream from HBM
-  if (p->tblock < 2 && rows * quads * 4 * (long long)sizeof(T) * 3 < 96LL * 1024 * 1024)
+  // grids L2 holds step well one step a launch; this pays where the fields stream from HBM.
+  // With a pml it is bit-exact but slower than one step a launch on every grid measured
+  // (2048^2 .. 8192^2, 20-cell slabs): only CWB_TBLOCK=2 takes it
+  if (p->tblock < 2 && ((flags & cwb::K_PML) ||
+                        rows * quads * 4 * (long long)sizeof(T) * 3 < 96LL * 1024 * 1024))
     return false;
   const int qx_step = cwb::TB_TQ - 2 * K;
   const int gx = (int)((quads + qx_step - 1) / qx_step);
@@ -1440,6 +1446,33 @@ bool tblock2d_path(cwb_plan *p, const cwb_op *ops, const int nops, const int t0,
       return rc = fail(CWB_ERR_ALLOC, "temporal blocking's second slots"), true;
     p->tb_fields_bytes = 2 * slot_bytes;
   }
+  // with a pml, K + 1 copies of the memory of axes 0 and 1 in a ring: the plan's own
+  // (copy 0) and K of the plan's scratch; a pass reads copy `in` and its level j writes
+  // copy in + j, so the next pass reads copy in + K (mod K + 1)
+  const bool pml = flags & cwb::K_PML;
+  size_t psi_copy = 0;  // floats of one copy, both axes
+  size_t psi_off[2] = {0, 0};
+  for (int d = 0; d < 2 && pml; ++d) {
+    psi_off[d] = psi_copy;
+    if (sp.aux[d])
+      psi_copy += 3 * (size_t)sp.auxrow[d];
+  }
+  if (pml && p->tb_psi_bytes < K * psi_copy * sizeof(T)) {
+    if (p->tb_psi)
+      cudaFree(p->tb_psi);
+    p->tb_psi = nullptr;
+    p->tb_psi_bytes = 0;
+    if (cudaMalloc(&p->tb_psi, K * psi_copy * sizeof(T)) != cudaSuccess)
+      return rc = fail(CWB_ERR_ALLOC, "temporal blocking's copies of the pml memory"), true;
+    p->tb_psi_bytes = K * psi_copy * sizeof(T);
+  }
+  const auto psi_at = [&](const int copy, const int d) -> T * {
+    if (!pml || !sp.aux[d])
+      return nullptr;
+    if (copy == 0)
+      return sp.aux[d];
+    return static_cast<T *>(p->tb_psi) + (size_t)(copy - 1) * psi_copy + psi_off[d];
+  };
   T *mine[2] = {static_cast<T *>(A.base), static_cast<T *>(A.base) + A.stride};
   T *other[2] = {static_cast<T *>(p->tb_fields), static_cast<T *>(p->tb_fields) + A.stride};
   const auto slot_of = [&](const int m) { return ((m + C.add) % 2 + 2) % 2; };  // u^m's slot
@@ -1449,9 +1482,14 @@ bool tblock2d_path(cwb_plan *p, const cwb_op *ops, const int nops, const int t0,
     CWB_CUDA(cudaStreamWaitEvent(p->lane, p->fork, 0));
     cudaStream_t s = p->lane;
     CWB_CUDA(cudaMemcpyAsync(other[0], mine[0], 2 * slot_bytes, cudaMemcpyDeviceToDevice, s));
+    int in = 0;  // the pml memory copy the pass reads
     for (int k = 0; k < passes; ++k) {
       const int t = t0 + k * K;
       T **from = k % 2 ? other : mine, **to = k % 2 ? mine : other;
+      for (int j = 0; j <= K; ++j)
+        for (int d = 0; d < 2; ++d)
+          tp.psi[j][d] = psi_at((in + j) % (K + 1), d);
+      in = (in + K) % (K + 1);
       tp.t = t;
       tp.A = from[slot_of(t - 2)];
       tp.B = from[slot_of(t - 1)];
@@ -1462,6 +1500,10 @@ bool tblock2d_path(cwb_plan *p, const cwb_op *ops, const int nops, const int t0,
     }
     if (passes % 2)
       CWB_CUDA(cudaMemcpyAsync(mine[0], other[0], 2 * slot_bytes, cudaMemcpyDeviceToDevice, s));
+    for (int d = 0; d < 2 && in != 0; ++d)
+      if (psi_at(0, d))
+        CWB_CUDA(cudaMemcpyAsync(psi_at(0, d), psi_at(in, d), 3 * (size_t)sp.auxrow[d] * sizeof(T),
+                                 cudaMemcpyDeviceToDevice, s));
     CWB_CUDA(cudaEventRecord(p->join, s));
     CWB_CUDA(cudaStreamWaitEvent(user, p->join, 0));
     return CWB_OK;
@@ -2129,6 +2171,8 @@ int cwb_plan_destroy(cwb_plan *p) {
   }
   if (p->tb_fields)
     cudaFree(p->tb_fields);
+  if (p->tb_psi)
+    cudaFree(p->tb_psi);
   if (p->ctr)
     cudaFree(p->ctr);
   if (p->err)

@@ -30,7 +30,17 @@
 // a ghost row read its mirror row), then the receivers of the tile's own nodes recorded.
 // Rings hold interior rows only; a tap row b past a wall reads row 2 - b or 2 (N0 - 2) - b,
 // negated past a Dirichlet face (cuwave common.cuh:50-54).
+//
+// With a pml (the PML instance), each level advances the memory of its slab nodes after
+// the update, axis 0 then axis 1 (cuwave pml_kernel, scalar.cu:500-532; the order and
+// arithmetic of step2d.cuh's): an axis-0 slab row takes its taps from the window of the
+// level before, an axis-1 slab node from its run. Every level reads the memory the level
+// before it wrote and writes its own copy (K + 1 copies, the pass's input the first), so
+// a node that neighbouring tiles or chunks both recompute is written twice with the same
+// value and no block reads a copy another block may still be writing.
 #pragma once
+
+#include <type_traits>
 
 #include "pairs.cuh"
 #include "step2d.cuh"
@@ -63,6 +73,9 @@ struct TBlock2Params {
   const int4 *rec_entry;
   TransferParams<T> rec[TB_RECORDS];
   int nrec;
+  // the pml memory, axes 0 and 1, in the plan's (3, slab) layout: [0] the pass's input,
+  // [j] what level j writes
+  T *psi[TB_K + 1][2];
 };
 
 template <int R>
@@ -81,7 +94,7 @@ constexpr int tblock_smem() {
   return K * TBlockShape<R>::NR * TB_TQ * 16;
 }
 
-template <int R, int K, bool HOLD>
+template <int R, int K, bool HOLD, bool PML>
 __global__ void __launch_bounds__(TB_TQ * K, 2) tblock2d_kernel(const __grid_constant__ TBlock2Params<float> P) {
   using T = float;
   using S = TBlockShape<R>;
@@ -106,8 +119,8 @@ __global__ void __launch_bounds__(TB_TQ * K, 2) tblock2d_kernel(const __grid_con
   const auto at = [&](const int j, const int slot) -> float4 * {
     return tb_ring + (j * NR + slot) * TB_TQ;
   };
-  // the thread's nodes
-  int inner = 0, xheld = 0;
+  // the thread's nodes, its Dirichlet wall nodes, its axis-1 slab nodes
+  int inner = 0, xheld = 0, xslab = 0;
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
     const int x = xq + i;
@@ -116,6 +129,8 @@ __global__ void __launch_bounds__(TB_TQ * K, 2) tblock2d_kernel(const __grid_con
     inner |= 1 << i;
     if (HOLD && held_wall(x, NF, dirF))
       xheld |= 1 << i;
+    if (PML && slab_row(x, NF, g.lo[1], g.hi[1]) >= 0)
+      xslab |= 1 << i;
   }
   const bool fix_lo = xq - H < 0;
   const int e_hi = NF - (xq - H);
@@ -175,6 +190,17 @@ __global__ void __launch_bounds__(TB_TQ * K, 2) tblock2d_kernel(const __grid_con
   int wslot0 = (int)(((unsigned)(first - (lev - 1) * L - R + 64 * NR)) % NR);
   int rslot0 = (int)(((unsigned)(first - (lev - 1) * L + 64 * NR)) % NR);
 
+  // a block whose rows or quads (the widest level's) meet no slab runs the march without
+  // the pml's code: one kernel, two bodies, the choice uniform over the block
+  const auto slab_block = [&]() {
+    const int lo0 = g.lo[0], hi0 = g.hi[0], lo1 = g.lo[1], hi1 = g.hi[1];
+    const int ra = row_lo(1), rb = row_hi(1) - 1;  // rows, inclusive
+    const int xa = 4 * (qx0 + 1), xb = 4 * (qx0 + TB_TQ - 1) - 1;  // nodes, inclusive
+    return (lo0 && ra <= lo0) || (hi0 && rb >= N0 - 1 - hi0) || (lo1 && xa <= lo1) ||
+           (hi1 && xb >= NF - 1 - hi1);
+  };
+  const auto march = [&](auto pml_c) {
+  constexpr bool DO_PML = decltype(pml_c)::value;
   for (int front = first; front - (K - 1) * L < row_hi(K); front += M) {
     // level 1's group fetches the rows of u^(t-1) it reads M ahead next tick
     float4 next[M];
@@ -293,12 +319,79 @@ __global__ void __launch_bounds__(TB_TQ * K, 2) tblock2d_kernel(const __grid_con
           v[2 * h] = r2.x;
           v[2 * h + 1] = r2.y;
         }
+        const int held = HOLD ? (held_wall(r, N0, dir0) ? inner : xheld) : 0;
         if (HOLD) {
-          const int held = held_wall(r, N0, dir0) ? inner : xheld;
 #pragma unroll
           for (int i = 0; i < 4; ++i)
             if ((held >> i) & 1)
               v[i] = (T)0;
+        }
+        if constexpr (DO_PML) {
+          // one node's memory step and share of the update along axis d (pml_kernel's order)
+          const auto node = [&](const int i, const int d, const int a, const int N, const T Dpu,
+                                const T Dmu, T &m0, T &m1, T &m2) {
+            const T *prof = p.prof[d];
+            const T an = prof[a], bn = prof[N + a];
+            const T ah = prof[2 * N + a], bh = prof[3 * N + a];
+            const T ah1 = prof[2 * N + a - 1], bh1 = prof[3 * N + a - 1];
+            const T f = p.f[d];
+            const T pp = bh * m0 + ah * Dpu;
+            const T pm = bh1 * m1 + ah1 * Dmu;
+            const T zz = bn * m2 + an * f * (gg * (Dpu + pp) - gg * (Dmu + pm));
+            m0 = pp;
+            m1 = pm;
+            m2 = zz;
+            if (!((held >> i) & 1))
+              v[i] += mi[i] * (f * (gg * pp - gg * pm) + zz);
+          };
+          const int zrow = slab_row(r, N0, g.lo[0], g.hi[0]);
+          if (zrow >= 0) {
+            // an axis-0 slab row: its taps from the window, its memory row contiguous
+            const T *src = P.psi[lev - 1][0];
+            T *dst = P.psi[lev][0];
+            const long long sz = p.auxrow[0], si = (long long)zrow * ext + xq;
+            T m0[4], m1[4], m2[4];
+            load4(m0, src + si);
+            load4(m1, src + sz + si);
+            load4(m2, src + 2 * sz + si);
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+              if (!((inner >> i) & 1))
+                continue;
+              const auto tap = [&](const int j) { return win[c + j][i]; };
+              T Dpu, Dmu;
+              diffs_plain<T, R>(tap, win[c][i], p.w, Dpu, Dmu);
+              node(i, 0, r, N0, Dpu, Dmu, m0[i], m1[i], m2[i]);
+            }
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+              if ((inner >> i) & 1) {
+                dst[si + i] = m0[i];
+                dst[sz + si + i] = m1[i];
+                dst[2 * sz + si + i] = m2[i];
+              }
+          }
+          if (xslab) {
+            const T *src = P.psi[lev - 1][1];
+            T *dst = P.psi[lev][1];
+            const long long sz = p.auxrow[1];
+            const int lo = g.lo[1], hi = g.hi[1];
+            const long long base = (long long)r * (lo + hi);
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+              if (!((xslab >> i) & 1))
+                continue;
+              const auto tap = [&](const int j) { return xr[H + i + j]; };
+              T Dpu, Dmu;
+              diffs_plain<T, R>(tap, xr[H + i], p.w, Dpu, Dmu);
+              const long long si = base + slab_row(xq + i, NF, lo, hi);
+              T m0 = src[si], m1 = src[sz + si], m2 = src[2 * sz + si];
+              node(i, 1, xq + i, NF, Dpu, Dmu, m0, m1, m2);
+              dst[si] = m0;
+              dst[sz + si] = m1;
+              dst[2 * sz + si] = m2;
+            }
+          }
         }
         // the sources on this quad, in the list's order
         if (src_hi > src_lo) {
@@ -401,6 +494,11 @@ __global__ void __launch_bounds__(TB_TQ * K, 2) tblock2d_kernel(const __grid_con
         at(0, slot_of(front + M + R + m))[qi] = next[m];
     __syncthreads();
   }
+  };
+  if (PML && slab_block())
+    march(std::true_type{});
+  else
+    march(std::false_type{});
 }
 
 }  // namespace cwb

@@ -186,7 +186,9 @@ cudaError_t tblock2d_unit(const TBlock2Params<float> &p, const dim3 grid, cudaSt
   if constexpr (sizeof(T) != 4 || R > 4) {
     return cudaErrorInvalidValue;
   } else {
-    const auto k = p.s.g.dir ? tblock2d_kernel<R, TB_K, true> : tblock2d_kernel<R, TB_K, false>;
+    const bool pml = p.s.flags & K_PML;
+    const auto k = p.s.g.dir ? (pml ? tblock2d_kernel<R, TB_K, true, true> : tblock2d_kernel<R, TB_K, true, false>)
+                             : (pml ? tblock2d_kernel<R, TB_K, false, true> : tblock2d_kernel<R, TB_K, false, false>);
     const size_t smem = tblock_smem<R, TB_K>();
     cudaError_t e = allow_smem(k, smem);
     if (e != cudaSuccess)

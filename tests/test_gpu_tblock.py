@@ -102,3 +102,33 @@ def test_blocked_march_matches_oracle():
     field, traces = case.forward(sim.N)
     np.testing.assert_array_equal(t_blk, traces)
     np.testing.assert_array_equal(f_blk, field[:, : Nx[1]])
+
+
+@pytest.mark.parametrize("R,dirichlet,pml", [(4, 0b0000, 20), (3, 0b0110, 7), (2, 0b1001, 12),
+                                             (1, 0b0000, 5)])
+def test_blocked_march_with_pml_matches_oracle(R, dirichlet, pml):
+    """With pml slabs on every face (their memory advanced level by level inside the pass,
+    around the ring of copies), Dirichlet and Neumann faces, sources anywhere in the
+    interior: the oracle's fields and traces, bit for bit, and the single-step march's."""
+    from cuwave_b200 import _native as nat
+    from test_gpu_parity import _product, _random_case
+
+    case, meta = _random_case(2, R, dirichlet=dirichlet, pml=pml, uniform=True, seed=50 + R,
+                              nsrc=4, nsens=9, Nx=(150, 530))
+    counts = {}
+    results = {}
+    for mode in ("0", "2"):
+        os.environ["CWB_TBLOCK"] = mode
+        try:
+            n0 = nat.launches()
+            results[mode] = _product(case, meta)
+            torch.cuda.synchronize()
+            counts[mode] = nat.launches() - n0
+        finally:
+            os.environ.pop("CWB_TBLOCK", None)
+    assert counts["2"] != counts["0"], counts
+    ref_field, ref_traces = case.forward(meta["N"])
+    for mode in ("0", "2"):
+        field, traces = results[mode]
+        np.testing.assert_array_equal(traces, ref_traces)
+        np.testing.assert_array_equal(field, ref_field)
