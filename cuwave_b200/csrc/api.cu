@@ -553,7 +553,8 @@ cudaError_t pml3d_r(const cwb::Pml3Params<T> &p, const int R, const int axis, co
 // memory in its march): a launch per lined axis, axis 1 first, so a node in both slabs
 // takes its shares in the reference's order.
 template <typename T>
-int pml_launch(const cwb_plan *p, const cwb::StepParams<T> &sp, std::vector<Launch> &out) {
+int pml_launch(const cwb_plan *p, const cwb::StepParams<T> &sp, const int fold,
+               std::vector<Launch> &out) {
   const Geometry &g = p->geo;
   const int R = p->grid.radius;
   if (g.ndim != 3)
@@ -598,6 +599,7 @@ int pml_launch(const cwb_plan *p, const cwb::StepParams<T> &sp, std::vector<Laun
     q2.nlo = g.lo[2] > 0 ? g.lo[2] / 4 + 1 : 0;
     q2.xhi = (NF - 1 - g.hi[2]) / 4 * 4;
     q2.nhi = g.hi[2] > 0 ? (NF - 2) / 4 - (NF - 1 - g.hi[2]) / 4 + 1 : 0;
+    q2.fold = fold;
     const int nq = q2.nlo + q2.nhi;
     if (nq > cwb::PML2_THREADS)
       return fail(CWB_ERR_UNSUPPORTED, "pml slabs wider than 500 nodes along axis 2");
@@ -636,6 +638,42 @@ int step_setup(const cwb_plan *p, const cwb_op &op, cwb::StepParams<T> &sp, int 
       sp.auxrow[d] = (int)p->pml_row[d];
       if (lined(p, d) && !sp.aux[d])
         return fail(CWB_ERR_ARG, "a lined axis needs its pml memory");
+    }
+  }
+  return CWB_OK;
+}
+
+// An internal refill op's flags: the fast axis' faces (bit 0 low, bit 1 high, times
+// this) that an earlier launch of the step refilled already.
+constexpr int OP_REFILLED_FAST = 1 << 28;
+
+// The 3D step's fast-axis face ghosts the axis-2 pml launch may refill itself (1 low,
+// 2 high): the face lined by the pml and refilled this step, its ghost and mirror in one
+// quad that only that side's slab threads write, and no folded source on the mirror
+// column (the sources are added after the pml, the refill after them).
+template <typename T>
+int x_ghost_fold(const cwb_plan *p, const cwb_op &op, cudaStream_t stream, int &fold) {
+  const Geometry &g = p->geo;
+  fold = 0;
+  if (g.ndim != 3 || !(op.flags & CWB_FOLD_REFILL))
+    return CWB_OK;
+  const int NF = g.n[2], lo = g.lo[2], hi = g.hi[2];
+  const int faces = p->grid.neumann | p->grid.dirichlet;
+  if (lo > 0 && ((faces >> 4) & 1) && NF - 1 - hi > 3)
+    fold |= 1;
+  if (hi > 0 && ((faces >> 5) & 1) && (NF - 1) % 4 >= 2 && lo < (NF - 1) / 4 * 4)
+    fold |= 2;
+  const cwb_points &src = op.points;
+  if (fold && (op.flags & CWB_FOLD_SOURCES) && src.num > 0) {
+    std::vector<int> lin(src.num);
+    CWB_CUDA(cudaMemcpyAsync(lin.data(), src.lin, sizeof(int) * src.num, cudaMemcpyDeviceToHost, stream));
+    CWB_CUDA(cudaStreamSynchronize(stream));
+    for (const int l : lin) {
+      const int x = l % g.s[1];
+      if (x == 2)
+        fold &= ~1;
+      if (x == NF - 3)
+        fold &= ~2;
     }
   }
   return CWB_OK;
@@ -729,6 +767,7 @@ int translate(cwb_plan *p, const cwb_op &op, const size_t slot, cudaStream_t str
       });
     }
     if (blocked || quad2) {
+      int fold = 0;  // fast-axis face ghosts the pml launch refills
       // after the update (and its pml memory), the sources and the refill, each a
       // launch of its own in the order of cuwave's step
       if (blocked) {
@@ -748,8 +787,12 @@ int translate(cwb_plan *p, const cwb_op &op, const size_t slot, cudaStream_t str
             q.s.flags |= cwb::K_ADV;
           return step3d_r<T>(q, R, uniform, grid, s);
         });
-        if ((op.flags & CWB_PML) && (rc = pml_launch<T>(p, sp, out)))
-          return rc;
+        if (op.flags & CWB_PML) {
+          if ((rc = x_ghost_fold<T>(p, op, stream, fold)))
+            return rc;
+          if ((rc = pml_launch<T>(p, sp, fold, out)))
+            return rc;
+        }
       }
       if ((op.flags & CWB_FOLD_SOURCES) && op.points.num > 0) {
         if (!op.points.weight || !op.points.record)
@@ -766,6 +809,7 @@ int translate(cwb_plan *p, const cwb_op &op, const size_t slot, cudaStream_t str
         cwb_op rf;
         std::memset(&rf, 0, sizeof rf);
         rf.kind = CWB_OP_REFILL;
+        rf.flags = fold * OP_REFILLED_FAST;  // faces the pml launch refilled
         rf.a = op.c;
         if ((rc = translate<T>(p, rf, slot, stream, out)))
           return rc;
@@ -1057,6 +1101,9 @@ int translate(cwb_plan *p, const cwb_op &op, const size_t slot, cudaStream_t str
     if (op.kind == CWB_OP_REFILL) {
       kind = cwb::TR_REFILL;
       faces = p->grid.neumann | p->grid.dirichlet;
+      // an internal refill after the 3D pml launches: the fast axis' faces that launch
+      // refilled are left out
+      faces &= ~(((op.flags / OP_REFILLED_FAST) & 3) << (2 * (ndim - 1)));
       for (int d = 0; d < ndim; ++d) {
         int face = 1;
         for (int e = 0; e < ndim; ++e)

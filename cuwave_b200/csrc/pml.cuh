@@ -40,6 +40,7 @@ struct Pml3Params {
   T *aux;         // 3 rows of `auxrow`: psi+, psi-, zeta
   long long auxrow;
   int nlo, nhi, xhi;  // axis 2: slab quads on each side, the first high one's x
+  int fold;           // axis 2: the face ghosts refilled here (1 low, 2 high) from final mirrors
   int *ctr;
 };
 
@@ -239,7 +240,24 @@ __global__ void __launch_bounds__(PML2_THREADS) pml_axis2_kernel(const __grid_co
                  prof[2 * NF + x - 1], prof[3 * NF + x - 1], Dpu, Dmu, aux[si], aux[sz + si],
                  aux[2 * sz + si], v[i], mi[i], (held >> i) & 1);
       }
-      put4m(u2 + idx, v, in);
+      // the face ghosts of axis 2 in this quad, refilled from their mirrors two nodes in
+      // (homogeneous_neumann/dirichlet_kernel, scalar.cu:535-555), whose values are final
+      // here: the host folds a face only when no source sits on its mirror column (the
+      // sources come after the pml), its wall node held at zero already on a Dirichlet face
+      int wmask = in;
+      if ((p.fold & 1) && xq == 0) {
+        v[0] = (dirF & 1) ? -v[2] : v[2];
+        wmask |= 1;
+      }
+      if ((p.fold & 2) && xq + 2 <= NF - 1 && NF - 1 <= xq + 3) {
+#pragma unroll
+        for (int a = 2; a < 4; ++a)
+          if (NF - 1 - xq == a) {
+            v[a] = (dirF & 2) ? -v[a - 2] : v[a - 2];
+            wmask |= 1 << a;
+          }
+      }
+      put4m(u2 + idx, v, wmask);
     }
   }
   finish_step(p.ctr, p.flags & K_ADV);

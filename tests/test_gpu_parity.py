@@ -185,6 +185,26 @@ def test_blocked_uniform_step_matches_oracle(R, dirichlet, pml, damping):
     np.testing.assert_array_equal(traces, ref_traces)
 
 
+@pytest.mark.parametrize("dirichlet", [0b000000, 0b110000])
+def test_blocked_step_with_sources_on_the_ghost_mirrors(dirichlet):
+    """Sources on the columns whose values the fast axis' face ghosts copy (x = 2 and
+    NF - 3): the ghosts must take the value after the excitation, so the axis-2 pml
+    launch leaves those faces to the refill; the other cases fold them into it."""
+    case, meta = _random_case(3, 4, dirichlet=dirichlet, pml=4, uniform=True, seed=91, nsrc=3,
+                              nsens=9, Nx=(45, 37, 139))
+    Nx = meta["Nx"]
+    src = meta["src"].copy()
+    src[2, 0] = 2
+    src[2, 1] = Nx[2] - 3
+    meta["src"] = src
+    case.source_lin = cases.flat({"Nx": np.array(Nx)}, src)
+    case.source_weight = case.excitation_weights(case.source_lin)
+    field, traces = _product(case, meta)
+    ref_field, ref_traces = case.forward(meta["N"])
+    np.testing.assert_array_equal(field, ref_field)
+    np.testing.assert_array_equal(traces, ref_traces)
+
+
 @pytest.mark.parametrize("R,dirichlet,pml,damping", [
     (1, 0b0000, 0, False), (2, 0b0110, 0, False), (3, 0b1001, 3, False),
     (4, 0b0110, 4, False), (4, 0b0000, 0, True), (4, 0b1111, 0, False), (2, 0b0101, 6, False),
