@@ -230,10 +230,23 @@ __device__ __forceinline__ void step2d_rows(const StepParams<T> &p, const int t,
             }
         }
         if (xslab) {
+          // the quad's memories loaded before any is stored, so their loads are in flight
+          // together (a store between them would order each load after it)
           T *aux = p.aux[1];
           const long long sz = p.auxrow[1];
           const int lo = g.lo[1], hi = g.hi[1];
           const long long base = (long long)z * (lo + hi);
+          long long si[4];
+          T m0[4], m1[4], m2[4];
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            si[i] = base + ((xslab >> i) & 1 ? slab_row(xq + i, NF, lo, hi) : 0);
+            if ((xslab >> i) & 1) {
+              m0[i] = aux[si[i]];
+              m1[i] = aux[sz + si[i]];
+              m2[i] = aux[2 * sz + si[i]];
+            }
+          }
 #pragma unroll
           for (int i = 0; i < 4; ++i) {
             if (!((xslab >> i) & 1))
@@ -242,9 +255,15 @@ __device__ __forceinline__ void step2d_rows(const StepParams<T> &p, const int t,
             const auto tap = [&](const int j) { return xr[H + i + j]; };
             T Dpu, Dmu;
             diffs_plain<T, R>(tap, xr[H + i], p.w, Dpu, Dmu);
-            const long long si = base + slab_row(x, NF, lo, hi);
-            node(i, 1, x, NF, Dpu, Dmu, aux[si], aux[sz + si], aux[2 * sz + si]);
+            node(i, 1, x, NF, Dpu, Dmu, m0[i], m1[i], m2[i]);
           }
+#pragma unroll
+          for (int i = 0; i < 4; ++i)
+            if ((xslab >> i) & 1) {
+              aux[si[i]] = m0[i];
+              aux[sz + si[i]] = m1[i];
+              aux[2 * sz + si[i]] = m2[i];
+            }
         }
       }
       if (fold.nsrc) {
