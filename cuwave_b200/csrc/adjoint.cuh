@@ -40,7 +40,9 @@ struct AdjFields {
   static constexpr int COUNT = 1 + (U ? 1 : 0) + (K ? 1 : 0);
 };
 
-template <typename T, int NDIM, int R, bool UNIF, int MODE, int BX, int BY>
+// PML: the pml transpose gathered here where the flags ask (else a launch of its own, or
+// none, and no code for it)
+template <typename T, int NDIM, int R, bool UNIF, int MODE, int BX, int BY, bool PML = true>
 __global__ void __launch_bounds__(BX *BY) adjoint_kernel(const AdjointParams<T> p) {
   using S = AdjShape<NDIM, R, BX, BY>;
   using FL = AdjFields<MODE, UNIF>;
@@ -272,7 +274,7 @@ __global__ void __launch_bounds__(BX *BY) adjoint_kernel(const AdjointParams<T> 
             gstiff = p.g_stiff[idx] - p.mf * gs;
           }
 
-          if (flags & K_PML) {
+          if (PML && (flags & K_PML)) {
             const T wcell = cell_weight<T>(g, A);
 #pragma unroll 1
             for (int d = 0; d < NDIM; ++d) {

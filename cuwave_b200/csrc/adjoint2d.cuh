@@ -94,8 +94,8 @@ __device__ __forceinline__ void image_run(T *xr, const T *row, const int xq, con
 }
 
 // HOLD: the grid has a Dirichlet face (without one, the faces' masks are zero at compile
-// time and every wall test folds away)
-template <typename T, int R, int MODE, bool HOLD = true>
+// time and every wall test folds away); DAMP: a damping field (without one, no code for it)
+template <typename T, int R, int MODE, bool HOLD = true, bool DAMP = true>
 __global__ void __launch_bounds__(A2_THREADS, A2_MIN_BLOCKS) adjoint2d_kernel(const AdjointParams<T> p) {
   using S = Adj2Shape<T, R>;
   static_assert(S::SUPPORTED && MODE != MODE_GRAD, "the 2D quad adjoint: float, radius <= 4");
@@ -320,7 +320,7 @@ __global__ void __launch_bounds__(A2_THREADS, A2_MIN_BLOCKS) adjoint2d_kernel(co
           }
           const T lo = lov[i], mi = miv[i];
           T v;
-          if (flags & K_DAMP) {
+          if (DAMP && (flags & K_DAMP)) {
             const T dmp = ((inner >> i) & 1) ? p.damping[row + i] : (T)0;
             const T beta = (T)0.5 * mi * dmp * p.dt;
             v = ((T)2 * lc[i] - lo * ((T)1 - beta) + mi * div_l) / ((T)1 + beta);

@@ -58,6 +58,7 @@ struct cwb_plan {
   bool tma = true;     // stage planes with tensor-map copies where the layout allows
   bool blocked3 = true;  // uniform-stiffness steps on the register-blocked kernels (CWB_STEP3D=0: off)
   int flow3 = 1;  // the 3D blocked step without a block barrier per plane (CWB_FLOW3D=0: with; 2: deeper ring)
+  int pml2d = 1;  // the 2D quad step's pml terms by a launch of their own (CWB_PML2D=0: inside the update kernel)
   cudaStream_t lane = nullptr;
   cudaEvent_t fork = nullptr, join = nullptr;
   int sms = 148;
@@ -70,7 +71,10 @@ struct cwb_plan {
   size_t fixed_cap = 0, fixed_used = 0;
   // the temporally blocked 2D march: its second pair of field slots (the passes alternate
   // between the caller's and these) and its per-block source and receiver lists
-  int tblock = 1;  // temporal blocking on 2D grids too large for L2 (CWB_TBLOCK=0: off; 2: any size)
+  // temporal blocking of 2D marches (CWB_TBLOCK=1: grids too large for L2; 2: any size).
+  // Off by default: one step a launch measured faster on every grid once the update
+  // kernel lost its slab code (8192^2: 233 against 214 Gpt-updates/s)
+  int tblock = 0;
   bool adj_split = true;  // the 3D adjoint's pml transpose as a launch of its own (CWB_ADJSPLIT=0: inline)
   void *tb_fields = nullptr;
   size_t tb_fields_bytes = 0;
@@ -442,6 +446,22 @@ bool step2d_built_r(const int R) {
 }
 
 template <typename T>
+cudaError_t pml2d_r(const cwb::StepParams<T> &p, const cwb::Pml2Layout &lay, const int R,
+                    cudaStream_t s) {
+  switch (R) {
+  case 1: return cwb::pml2d_unit<T, 1>(p, lay, s);
+  case 2: return cwb::pml2d_unit<T, 2>(p, lay, s);
+  case 3: return cwb::pml2d_unit<T, 3>(p, lay, s);
+  case 4: return cwb::pml2d_unit<T, 4>(p, lay, s);
+  case 5: return cwb::pml2d_unit<T, 5>(p, lay, s);
+  case 6: return cwb::pml2d_unit<T, 6>(p, lay, s);
+  case 7: return cwb::pml2d_unit<T, 7>(p, lay, s);
+  case 8: return cwb::pml2d_unit<T, 8>(p, lay, s);
+  }
+  return cudaErrorInvalidValue;
+}
+
+template <typename T>
 cudaError_t step2d_r(const cwb::StepParams<T> &p, const int R, const bool u, const dim3 grid,
                      cudaStream_t s) {
   switch (R) {
@@ -759,12 +779,35 @@ int translate(cwb_plan *p, const cwb_op &op, const size_t slot, cudaStream_t str
       sp.u1 = to_level(op.b, bytes);
       sp.u2 = to_level(op.c, bytes);
       sp.ctr = p->ctr;
-      out.push_back([sp, R, uniform, grid](cudaStream_t s, bool adv) {
-        cwb::StepParams<T> q = sp;
+      // the pml terms by a launch of their own over the slab nodes, the update kernel
+      // built without them (CWB_PML2D=0: inside the update kernel)
+      const bool split = (flags & cwb::K_PML) && p->pml2d;
+      cwb::StepParams<T> su = sp;
+      if (split)
+        su.flags &= ~cwb::K_PML;
+      out.push_back([su, R, uniform, grid](cudaStream_t s, bool adv) {
+        cwb::StepParams<T> q = su;
         if (adv)
           q.flags |= cwb::K_ADV;
         return step2d_r<T>(q, R, uniform, grid, s);
       });
+      if (split) {
+        cwb::Pml2Layout lay;
+        const int NF = g.n[1], lo1 = g.lo[1], hi1 = g.hi[1];
+        lay.nq = (int)quads;
+        lay.nlo = lo1 > 0 ? lo1 / 4 + 1 : 0;
+        lay.xhi = (NF - 1 - hi1) / 4 * 4;
+        lay.nhi = hi1 > 0 ? (NF - 2) / 4 - (NF - 1 - hi1) / 4 + 1 : 0;
+        lay.na = (long long)(g.lo[0] + g.hi[0]) * quads;
+        lay.total = lay.na + (long long)(g.n[0] - 2 - g.lo[0] - g.hi[0]) * (lay.nlo + lay.nhi);
+        if (lay.total > 0)
+          out.push_back([sp, lay, R](cudaStream_t s, bool adv) {
+            cwb::StepParams<T> q = sp;
+            if (adv)
+              q.flags |= cwb::K_ADV;
+            return pml2d_r<T>(q, lay, R, s);
+          });
+      }
     }
     if (blocked || quad2) {
       int fold = 0;  // fast-axis face ghosts the pml launch refills
@@ -1695,6 +1738,8 @@ int plan_geometry(const cwb_grid &G, cwb_plan &p) {
     p.tma = std::atoi(env) == 0;
   if (const char *env = std::getenv("CWB_STEP3D"))
     p.blocked3 = std::atoi(env) != 0;
+  if (const char *env = std::getenv("CWB_PML2D"))
+    p.pml2d = std::atoi(env);
   if (const char *env = std::getenv("CWB_FLOW3D"))
     p.flow3 = std::atoi(env);
   if (const char *env = std::getenv("CWB_TBLOCK"))
@@ -1736,6 +1781,7 @@ struct cwb_batch {
     int count = 0;
     long long total = 0;
     bool hold = true;  // an item of the group has a Dirichlet face
+    bool pml = true;   // an item of the group has a pml
   };
   std::vector<Group> groups;
   void *recs = nullptr;  // device BatchRecord<float>[items]
@@ -1818,8 +1864,11 @@ int batch_layout(cwb_batch *b, const long long want) {
     grp.count = (int)host.size();
     grp.total = first;
     grp.hold = false;
-    for (const auto &it : host)
+    grp.pml = false;
+    for (const auto &it : host) {
       grp.hold = grp.hold || it.s.g.dir != 0;
+      grp.pml = grp.pml || (it.s.flags & cwb::K_PML) != 0;
+    }
     CWB_CUDA(cudaMalloc(&grp.items, sizeof(cwb::Batch2Item<T>) * host.size()));
     b->groups.push_back(grp);
     CWB_CUDA(cudaMemcpy(grp.items, host.data(), sizeof(cwb::Batch2Item<T>) * host.size(),
@@ -1839,6 +1888,7 @@ std::vector<Launch> batch_launches(cwb_batch *b, const bool records) {
     bp.count = g.count;
     bp.total = g.total;
     bp.hold = g.hold ? 1 : 0;
+    bp.pml = g.pml ? 1 : 0;
     bp.ctr = b->ctr;
     const dim3 grid((unsigned)((g.total + cwb::S2_THREADS - 1) / cwb::S2_THREADS));
     const int R = g.R;

@@ -29,11 +29,13 @@ struct Batch2Params {
   long long total;  // threads of the launch
   int flags;        // K_ADV
   int hold;         // an item has a Dirichlet face
+  int pml;          // an item has a pml
   int *ctr;
 };
 
-// HOLD: an item of the launch has a Dirichlet face (without one, the wall tests fold away)
-template <typename T, int R, bool HOLD = true>
+// HOLD: an item of the launch has a Dirichlet face (without one, the wall tests fold away);
+// PML: an item has a pml (without one, the step carries no slab code)
+template <typename T, int R, bool HOLD = true, bool PML = true>
 __global__ void __launch_bounds__(S2_THREADS, Step2Shape<T, R>::MIN_BLOCKS)
     batch2d_kernel(const __grid_constant__ Batch2Params<T> p) {
   static_assert(Step2Shape<T, R>::SUPPORTED, "the 2D quad step is built for float");
@@ -50,7 +52,7 @@ __global__ void __launch_bounds__(S2_THREADS, Step2Shape<T, R>::MIN_BLOCKS)
     }
     const Batch2Item<T> &it = p.items[lo];
     if (t < it.steps)
-      step2d_rows<T, R, HOLD>(it.s, t, k - it.first, it.fold);
+      step2d_rows<T, R, HOLD, PML>(it.s, t, k - it.first, it.fold);
   }
   finish_step(p.ctr, p.flags & K_ADV);
 }

@@ -50,8 +50,9 @@ struct Fold2 {
 };
 
 // unit k (a quad and a chunk of rows) of the step at t; HOLD: the grid has a Dirichlet
-// face (without one, the faces' masks are zero at compile time and the wall tests fold)
-template <typename T, int R, bool HOLD = true>
+// face (without one, the faces' masks are zero at compile time and the wall tests fold);
+// PML: the pml memory terms are applied here (else pml2d_kernel applies them after)
+template <typename T, int R, bool HOLD = true, bool PML = true>
 __device__ __forceinline__ void step2d_rows(const StepParams<T> &p, const int t, const long long k,
                                             const Fold2<T> &fold) {
   using S = Step2Shape<T, R>;
@@ -83,7 +84,7 @@ __device__ __forceinline__ void step2d_rows(const StepParams<T> &p, const int t,
       inner |= 1 << i;
       if (held_wall(x, NF, dirF))
         xheld |= 1 << i;
-      if ((flags & K_PML) && slab_row(x, NF, g.lo[1], g.hi[1]) >= 0)
+      if (PML && (flags & K_PML) && slab_row(x, NF, g.lo[1], g.hi[1]) >= 0)
         xslab |= 1 << i;
     }
     const bool fix_lo = xq - H < 0;
@@ -182,7 +183,7 @@ __device__ __forceinline__ void step2d_rows(const StepParams<T> &p, const int t,
           if ((held >> i) & 1)
             v[i] = (T)0;
       }
-      if (flags & K_PML) {
+      if (PML && (flags & K_PML)) {
         // one node's memory step and share of the update along axis d (pml_kernel's order)
         const auto node = [&](const int i, const int d, const int a, const int N, const T Dpu,
                               const T Dmu, T &m0, T &m1, T &m2) {
@@ -314,14 +315,185 @@ __device__ __forceinline__ void step2d_rows(const StepParams<T> &p, const int t,
   }
 }
 
-template <typename T, int R, bool UNIF, bool HOLD = true>
+template <typename T, int R, bool UNIF, bool HOLD = true, bool PML = true>
 __global__ void __launch_bounds__(S2_THREADS, Step2Shape<T, R>::MIN_BLOCKS)
     step2d_kernel(const StepParams<T> p) {
   static_assert(Step2Shape<T, R>::SUPPORTED && UNIF,
                 "the 2D quad step is built for float and a uniform stiffness");
   const Fold2<T> none{};
-  step2d_rows<T, R, HOLD>(p, step_index(p.ctr), (long long)blockIdx.x * S2_THREADS + threadIdx.x,
-                          none);
+  step2d_rows<T, R, HOLD, PML>(p, step_index(p.ctr), (long long)blockIdx.x * S2_THREADS + threadIdx.x,
+                               none);
+  finish_step(p.ctr, p.flags & K_ADV);
+}
+
+// The pml memory terms of a 2D quad step, after step2d_kernel<..., PML = false> wrote the
+// update and before the sources: the nodes of the axis-0 slab rows (every quad of those
+// rows; a quad there holding axis-1 slab nodes takes that axis' share after axis 0's),
+// then, in the other rows, the axis-1 slab quads of each side. A thread per quad and
+// row, its update, 1/m and memories loaded, the memory advanced from the plain
+// differences of u^(t-1) along the axis and the share added unless the node is held
+// (cuwave pml_kernel, scalar.cu:500-532, in step2d_rows' arithmetic and order). Kept out
+// of the update kernel, whose every thread would otherwise carry the slab code's
+// registers and wait on the memory's loads in the few warps that hold slab nodes.
+struct Pml2Layout {
+  int nq;            // quads a row
+  int nlo, nhi, xhi;  // axis-1 slab quads on each side, the first high one's x
+  long long na;      // threads of the axis-0 slab rows
+  long long total;   // all threads
+};
+
+template <typename T, int R, bool HOLD>
+__global__ void __launch_bounds__(S2_THREADS) pml2d_kernel(const StepParams<T> p, const Pml2Layout lay) {
+  using S = Step2Shape<T, R>;
+  constexpr int H = S::H, XR = S::XR;
+  const long long k = (long long)blockIdx.x * S2_THREADS + threadIdx.x;
+  const Geometry &g = p.g;
+  const int t = step_index(p.ctr);
+  if (k < lay.total) {
+    const int N0 = g.n[0], NF = g.n[1], ext = g.ext[1];
+    const int lo0 = g.lo[0], hi0 = g.hi[0], lo1 = g.lo[1], hi1 = g.hi[1];
+    int z, xq, side = 0;  // side: 0 both axes' slab nodes, 1 the low axis-1 slab, 2 the high
+    if (k < lay.na) {
+      const int ra = (int)(k / lay.nq);
+      z = ra < lo0 ? 1 + ra : N0 - 1 - hi0 + (ra - lo0);
+      xq = 4 * (int)(k % lay.nq);
+    } else {
+      const long long kb = k - lay.na;
+      const int nqs = lay.nlo + lay.nhi;
+      const int qi = (int)(kb % nqs);
+      z = lo0 + 1 + (int)(kb / nqs);
+      side = qi < lay.nlo ? 1 : 2;
+      xq = side == 1 ? 4 * qi : lay.xhi + 4 * (qi - lay.nlo);
+    }
+    const T *__restrict__ u1 = level<T>(p.u1, t);
+    T *u2 = level<T>(p.u2, t);
+    const int dir0 = HOLD ? g.dir & 3 : 0, dirF = HOLD ? (g.dir >> 2) & 3 : 0;
+    const int s0 = g.s[0];
+    const T gg = p.gconst;
+    int inner = 0, xheld = 0, xslab = 0;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int x = xq + i;
+      if (x < 1 || x > NF - 2)
+        continue;
+      inner |= 1 << i;
+      if (held_wall(x, NF, dirF))
+        xheld |= 1 << i;
+      const bool lo_node = lo1 && x <= lo1, hi_node = hi1 && x >= NF - 1 - hi1;
+      if (side == 0 ? (lo_node || hi_node) : side == 1 ? lo_node : hi_node)
+        xslab |= 1 << i;
+    }
+    const int mine = side == 0 ? inner : xslab;  // the nodes this thread writes
+    if (mine) {
+      const long long row = (long long)z * s0 + xq;
+      T v[4], mi[4];
+      load4(v, u2 + row);
+      if (p.flags & K_DERIVE) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+          mi[i] = (T)1 / p.sconst;
+      } else {
+        load4(mi, p.minv + row);
+      }
+      const int held = held_wall(z, N0, dir0) ? inner : xheld;
+      const auto node = [&](const int i, const int d, const int a, const int N, const T Dpu,
+                            const T Dmu, T &m0, T &m1, T &m2) {
+        const T *prof = p.prof[d];
+        const T an = prof[a], bn = prof[N + a];
+        const T ah = prof[2 * N + a], bh = prof[3 * N + a];
+        const T ah1 = prof[2 * N + a - 1], bh1 = prof[3 * N + a - 1];
+        const T f = p.f[d];
+        const T pp = bh * m0 + ah * Dpu;
+        const T pm = bh1 * m1 + ah1 * Dmu;
+        const T zz = bn * m2 + an * f * (gg * (Dpu + pp) - gg * (Dmu + pm));
+        m0 = pp;
+        m1 = pm;
+        m2 = zz;
+        if (!((held >> i) & 1))
+          v[i] += mi[i] * (f * (gg * pp - gg * pm) + zz);
+      };
+      if (side == 0) {
+        // an axis-0 slab row: u^(t-1) on rows z - R .. z + R through the axis-0 mirrors
+        T col[2 * R + 1][4];
+#pragma unroll
+        for (int j = -R; j <= R; ++j) {
+          const int b = z + j;
+          int sg = 1;
+          const int m = (b >= 0 && b <= N0 - 1) ? b : mirror_node(b, N0, dir0, sg);
+          load4(col[R + j], u1 + (long long)m * s0 + xq);
+          if (sg < 0) {
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+              col[R + j][i] = -col[R + j][i];
+          }
+        }
+        T *aux = p.aux[0];
+        const long long sz = p.auxrow[0], si = (long long)slab_row(z, N0, lo0, hi0) * ext + xq;
+        T m0[4], m1[4], m2[4];
+        load4(m0, aux + si);
+        load4(m1, aux + sz + si);
+        load4(m2, aux + 2 * sz + si);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          if (!((inner >> i) & 1))
+            continue;
+          const auto tap = [&](const int j) { return col[R + j][i]; };
+          T Dpu, Dmu;
+          diffs_plain<T, R>(tap, col[R][i], p.w, Dpu, Dmu);
+          node(i, 0, z, N0, Dpu, Dmu, m0[i], m1[i], m2[i]);
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+          if ((inner >> i) & 1) {
+            aux[si + i] = m0[i];
+            aux[sz + si + i] = m1[i];
+            aux[2 * sz + si + i] = m2[i];
+          }
+      }
+      if (xslab) {
+        // the quad's run of u^(t-1) along axis 1, mirrored past the walls
+        T xr[XR];
+#pragma unroll
+        for (int c = 0; c < XR / 4; ++c) {
+          const int x = xq - H + 4 * c;
+          if (x >= 0 && x + 3 <= ext - 1) {
+            load4(xr + 4 * c, u1 + row - H + 4 * c);
+          } else {
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+              xr[4 * c + i] = (T)0;
+          }
+        }
+        if (xq - H < 0)
+          mirror_run_lo_at<T, XR, H>(xr, (dirF & 1) ? (T)-1 : (T)1, H - xq);
+        const int e_hi = NF - (xq - H);
+        if (e_hi <= XR - 1)
+          mirror_run_hi_at<T, XR, H + 2>(xr, (dirF & 2) ? (T)-1 : (T)1, e_hi);
+        T *aux = p.aux[1];
+        const long long sz = p.auxrow[1];
+        const long long base = (long long)z * (lo1 + hi1);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          if (!((xslab >> i) & 1))
+            continue;
+          const int x = xq + i;
+          const auto tap = [&](const int j) { return xr[H + i + j]; };
+          T Dpu, Dmu;
+          diffs_plain<T, R>(tap, xr[H + i], p.w, Dpu, Dmu);
+          const long long si = base + slab_row(x, NF, lo1, hi1);
+          node(i, 1, x, NF, Dpu, Dmu, aux[si], aux[sz + si], aux[2 * sz + si]);
+        }
+      }
+      if (mine == 15) {
+        store4(u2 + row, v);
+      } else {
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+          if ((mine >> i) & 1)
+            u2[row + i] = v[i];
+      }
+    }
+  }
   finish_step(p.ctr, p.flags & K_ADV);
 }
 
@@ -342,7 +514,7 @@ struct March2Params {
   long long units;  // quads x row chunks
 };
 
-template <typename T, int R, bool HOLD = true>
+template <typename T, int R, bool HOLD = true, bool PML = true>
 __global__ void __launch_bounds__(S2_THREADS, Step2Shape<T, R>::MIN_BLOCKS)
     march2d_kernel(const __grid_constant__ March2Params<T> mp) {
   static_assert(Step2Shape<T, R>::SUPPORTED, "the 2D quad step is built for float");
@@ -353,7 +525,7 @@ __global__ void __launch_bounds__(S2_THREADS, Step2Shape<T, R>::MIN_BLOCKS)
   for (int s = 0; s < mp.steps; ++s) {
     const int t = mp.t0 + s;
     for (long long k = gtid; k < mp.units; k += gsize)
-      step2d_rows<T, R, HOLD>(mp.s, t, k, mp.fold);
+      step2d_rows<T, R, HOLD, PML>(mp.s, t, k, mp.fold);
     grid.sync();  // the step's nodes and ghosts are all written
     for (int r = 0; r < mp.nrec; ++r) {
       const TransferParams<T> &rp = mp.rec[r];

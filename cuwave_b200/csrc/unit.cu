@@ -48,7 +48,8 @@ cudaError_t adjoint_one(const AdjointParams<T> &p, const dim3 grid, cudaStream_t
   constexpr int BY = NDIM == 3 ? ADJ_BY3 : 1;
   const size_t smem =
       2 * AdjFields<MODE, U>::COUNT * AdjShape<NDIM, R, BX, BY>::PLANE * sizeof(T);
-  const auto k = adjoint_kernel<T, NDIM, R, U, MODE, BX, BY>;
+  const auto k = (p.flags & K_PML) ? adjoint_kernel<T, NDIM, R, U, MODE, BX, BY, true>
+                                  : adjoint_kernel<T, NDIM, R, U, MODE, BX, BY, false>;
   cudaError_t e = allow_smem(k, smem);
   if (e != cudaSuccess)
     return e;
@@ -134,10 +135,29 @@ cudaError_t step2d_unit(const StepParams<T> &p, const bool uniform, const dim3 g
   } else {
     if (!uniform)
       return cudaErrorInvalidValue;
+    // the pml inside the update kernel where its flag is on; without it (no pml, or
+    // pml2d_kernel applying it after) the instance without the slab code
+    const bool pml = p.flags & K_PML;
     if (p.g.dir)
-      step2d_kernel<T, R, true, true><<<grid, S2_THREADS, 0, s>>>(p);
+      (pml ? step2d_kernel<T, R, true, true, true> : step2d_kernel<T, R, true, true, false>)
+          <<<grid, S2_THREADS, 0, s>>>(p);
     else
-      step2d_kernel<T, R, true, false><<<grid, S2_THREADS, 0, s>>>(p);
+      (pml ? step2d_kernel<T, R, true, false, true> : step2d_kernel<T, R, true, false, false>)
+          <<<grid, S2_THREADS, 0, s>>>(p);
+    return cudaGetLastError();
+  }
+}
+
+template <typename T, int R>
+cudaError_t pml2d_unit(const StepParams<T> &p, const Pml2Layout &lay, cudaStream_t s) {
+  if constexpr (!Step2Shape<T, R>::SUPPORTED) {
+    return cudaErrorInvalidValue;
+  } else {
+    const dim3 grid((unsigned)((lay.total + S2_THREADS - 1) / S2_THREADS));
+    if (p.g.dir)
+      pml2d_kernel<T, R, true><<<grid, S2_THREADS, 0, s>>>(p, lay);
+    else
+      pml2d_kernel<T, R, false><<<grid, S2_THREADS, 0, s>>>(p, lay);
     return cudaGetLastError();
   }
 }
@@ -153,9 +173,11 @@ cudaError_t batch2d_unit(const Batch2Params<T> &p, const dim3 grid, cudaStream_t
     return cudaErrorInvalidValue;
   } else {
     if (p.hold)
-      batch2d_kernel<T, R, true><<<grid, S2_THREADS, 0, s>>>(p);
+      (p.pml ? batch2d_kernel<T, R, true, true> : batch2d_kernel<T, R, true, false>)
+          <<<grid, S2_THREADS, 0, s>>>(p);
     else
-      batch2d_kernel<T, R, false><<<grid, S2_THREADS, 0, s>>>(p);
+      (p.pml ? batch2d_kernel<T, R, false, true> : batch2d_kernel<T, R, false, false>)
+          <<<grid, S2_THREADS, 0, s>>>(p);
     return cudaGetLastError();
   }
 }
@@ -165,7 +187,9 @@ cudaError_t march2d_unit(const March2Params<T> &mp, const int sms, cudaStream_t 
   if constexpr (!Step2Shape<T, R>::SUPPORTED) {
     return cudaErrorInvalidValue;
   } else {
-    const auto k = mp.s.g.dir ? march2d_kernel<T, R, true> : march2d_kernel<T, R, false>;
+    const bool pml = mp.s.flags & K_PML;
+    const auto k = mp.s.g.dir ? (pml ? march2d_kernel<T, R, true, true> : march2d_kernel<T, R, true, false>)
+                              : (pml ? march2d_kernel<T, R, false, true> : march2d_kernel<T, R, false, false>);
     int per = 0;
     cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, S2_THREADS, 0);
     if (e != cudaSuccess)
@@ -204,17 +228,22 @@ cudaError_t adjoint2d_unit(const AdjointParams<T> &p, const int mode, const dim3
   if constexpr (!Adj2Shape<T, R>::SUPPORTED) {
     return cudaErrorInvalidValue;
   } else {
-    const bool hold = p.g.dir != 0;
-    if (mode == MODE_STEP_GRAD && hold)
-      adjoint2d_kernel<T, R, MODE_STEP_GRAD, true><<<grid, A2_THREADS, 0, s>>>(p);
-    else if (mode == MODE_STEP_GRAD)
-      adjoint2d_kernel<T, R, MODE_STEP_GRAD, false><<<grid, A2_THREADS, 0, s>>>(p);
-    else if (mode == MODE_STEP && hold)
-      adjoint2d_kernel<T, R, MODE_STEP, true><<<grid, A2_THREADS, 0, s>>>(p);
+    const bool hold = p.g.dir != 0, damp = p.flags & K_DAMP;
+    using K = void (*)(const AdjointParams<T>);
+    K k;
+    if (mode == MODE_STEP_GRAD)
+      k = hold ? (damp ? adjoint2d_kernel<T, R, MODE_STEP_GRAD, true, true>
+                       : adjoint2d_kernel<T, R, MODE_STEP_GRAD, true, false>)
+               : (damp ? adjoint2d_kernel<T, R, MODE_STEP_GRAD, false, true>
+                       : adjoint2d_kernel<T, R, MODE_STEP_GRAD, false, false>);
     else if (mode == MODE_STEP)
-      adjoint2d_kernel<T, R, MODE_STEP, false><<<grid, A2_THREADS, 0, s>>>(p);
+      k = hold ? (damp ? adjoint2d_kernel<T, R, MODE_STEP, true, true>
+                       : adjoint2d_kernel<T, R, MODE_STEP, true, false>)
+               : (damp ? adjoint2d_kernel<T, R, MODE_STEP, false, true>
+                       : adjoint2d_kernel<T, R, MODE_STEP, false, false>);
     else
       return cudaErrorInvalidValue;
+    k<<<grid, A2_THREADS, 0, s>>>(p);
     return cudaGetLastError();
   }
 }
@@ -295,6 +324,8 @@ template int step_tma_halo<CWB_REAL, CWB_NDIM, CWB_RADIUS>();
 template cudaError_t step2d_unit<CWB_REAL, CWB_RADIUS>(const StepParams<CWB_REAL> &, bool, dim3,
                                                        cudaStream_t);
 template bool step2d_built<CWB_REAL, CWB_RADIUS>();
+template cudaError_t pml2d_unit<CWB_REAL, CWB_RADIUS>(const StepParams<CWB_REAL> &, const Pml2Layout &,
+                                                      cudaStream_t);
 template cudaError_t batch2d_unit<CWB_REAL, CWB_RADIUS>(const Batch2Params<CWB_REAL> &, dim3,
                                                         cudaStream_t);
 template cudaError_t march2d_unit<CWB_REAL, CWB_RADIUS>(const March2Params<CWB_REAL> &, int,
