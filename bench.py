@@ -898,7 +898,8 @@ def profile_traffic(w: dict):
     n, wd = w["Nx"][0] - 2, w["width"]
     units = {"interior nodes": n**3, "slab nodes of axes 1 and 2": n * 2 * wd * n + n * (n - 2 * wd) * 2 * wd,
              "slab nodes of axis 1": n * 2 * wd * n, "slab nodes of axis 2": n * n * 2 * wd,
-             "face nodes": 6 * n * n, "sources": w["source"].shape[1]}
+             "face nodes": 6 * n * n, "face nodes of axes 0 and 1": 4 * n * n,
+             "sources": w["source"].shape[1]}
     total = 0.0
     for entry in data.values():
         if entry["unit"] not in units:
