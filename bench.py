@@ -652,9 +652,11 @@ def sensitivity_e2e(kernels: dict | None, n: int = 2048, steps: int = 300) -> di
 def shots_measure(count: int = 96, steps: int = 2000, n: int = 1024) -> dict:
     """A multi-shot gradient: `count` shots on a shared n^2 grid (blob speeds, radius 4),
     sources evenly spaced along the top, 256 receivers 50 cells down, `steps` steps;
-    the summed misfit gradient (a forward with its history and an adjoint per shot, in
-    turn) timed with CUDA events after one warm-up shot. Observed data are zero, so the
-    misfit is the traces' energy."""
+    the summed misfit gradient (a forward with its history and an adjoint per shot),
+    the shots side by side on `misfit_gradient`'s lanes and then in turn, wall-clock
+    with the device synchronized on both sides, after a warm-up of one shot a lane; the
+    two results compared to the bit. Observed data are zero, so the misfit is the
+    traces' energy."""
     import torch
 
     from cuwave_b200 import AcousticWave, ricker
@@ -674,18 +676,28 @@ def shots_measure(count: int = 96, steps: int = 2000, n: int = 1024) -> dict:
     sources = shots(sim, coords, signal)
     sensors = Sensors(sim, np.stack([np.full(256, 50.0), np.linspace(20.0, n - 21.0, 256)], axis=1))
     observed = [torch.zeros((steps, 256), dtype=torch.float32, device="cuda")] * count
-    misfit_gradient(sim, sources[:1], ind, sensors, observed[:1])
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize()
-    e0.record()
-    cost, gradient = misfit_gradient(sim, sources, ind, sensors, observed)
-    e1.record()
-    torch.cuda.synchronize()
-    seconds = e0.elapsed_time(e1) / 1e3
+    from cuwave_b200.utils import _lanes
+    from cuwave_b200.sensitivity import sensitivity
+
+    lanes = _lanes(sim, count, sensitivity)
+    misfit_gradient(sim, sources[:lanes], ind, sensors, observed[:lanes])  # plans, graphs
+
+    def timed(k):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        out = misfit_gradient(sim, sources, ind, sensors, observed, lanes=k)
+        torch.cuda.synchronize()
+        return time.perf_counter() - t0, out
+
+    seconds, (cost, gradient) = timed(lanes)
+    turn_s, (cost1, gradient1) = timed(1)
+    same = bool(cost == cost1 and torch.equal(gradient, gradient1))
     updates = 2 * count * steps * (n - 2) ** 2  # forward and adjoint
     return {"shots": count, "steps": steps, "grid": [n, n], "space_order": 8,
-            "receivers": 256, "in_turn_s": seconds, "shots_per_s": count / seconds,
-            "gpts": updates / seconds / 1e9, "finite": bool(np.isfinite(cost))}
+            "receivers": 256, "lanes": lanes, "seconds": seconds, "in_turn_s": turn_s,
+            "shots_per_s": count / seconds, "gpts": updates / seconds / 1e9,
+            "over_in_turn": turn_s / seconds, "equal_to_in_turn": same,
+            "finite": bool(np.isfinite(cost))}
 
 
 def learned_measure(coarse_nodes: int = 256, coarse_steps: int = 600) -> dict:

@@ -336,25 +336,81 @@ def misfit(sim: Simulation, sources: Sequence[Source], indicator, sensors: Senso
     return sum(objective(data)(t)[0] for t, data in zip(traces, observed))
 
 
+def _lanes(sim: Simulation, shots: int, adjoint: Callable) -> int:
+    """Shots to run side by side: up to four, as many as half the free device memory
+    holds the stored histories of (`sensitivity` keeps N + 2 fields a shot)."""
+    if shots <= 1:
+        return 1
+    field = int(np.prod(sim.Nx_padded)) * torch.empty((), dtype=sim.dtype).element_size()
+    per_shot = (sim.N + 8) * field if adjoint is sensitivity else 16 * field
+    free, _ = torch.cuda.mem_get_info(device())
+    return int(max(1, min(4, shots, (free // 2) // max(per_shot, 1))))
+
+
 def misfit_gradient(sim: Simulation, sources: Sequence[Source], indicator, sensors: Sensors,
                     observed, objective: Callable = l2_misfit,
-                    adjoint: Callable = sensitivity, devices: Sequence[int] | None = None):
+                    adjoint: Callable = sensitivity, devices: Sequence[int] | None = None,
+                    lanes: int | None = None):
     """Cost summed over the shots and its derivative with respect to `indicator` (cuwave utils.py:410-459).
 
     Each shot is one `adjoint` solve (`sensitivity`, or `reconstruction_sensitivity`
     where the history does not fit) with the receivers' objective lifted onto their
     corner nodes; the gradients are reparametrized onto the indicator and summed over
     the padded grid in shot order.
+
+    The shots are independent, so `lanes` of them run side by side, each lane a CUDA
+    stream with a plan of its own driven from its own host thread (by default as many
+    as the free memory holds, at most four); every shot's gradient is kept apart and the
+    sum taken in shot order afterwards, so the result is the one-at-a-time result to the
+    bit. `lanes=1` runs them in turn.
     """
     _one_device(devices)
-    cost = 0.0
+    pairs = list(zip(sources, observed))
+    lanes = _lanes(sim, len(pairs), adjoint) if lanes is None else max(1, min(int(lanes), len(pairs)))
     gradient = torch.zeros(sim.Nx_padded, dtype=sim.dtype, device=device())
-    for source, data in zip(sources, observed):
-        shot_cost, grads, _, _ = adjoint(
-            sim, source, indicator, sensors.nodes, sensors.objective(objective(data))
-        )
+    if lanes <= 1:
+        cost = 0.0
+        for source, data in pairs:
+            shot_cost, grads, _, _ = adjoint(
+                sim, source, indicator, sensors.nodes, sensors.objective(objective(data))
+            )
+            cost += shot_cost
+            gradient += _reparametrize(sim, indicator, grads)
+        return cost, gradient
+
+    from concurrent.futures import ThreadPoolExecutor
+    from dataclasses import replace
+
+    main = torch.cuda.current_stream()
+    ready = torch.cuda.Event()
+    ready.record(main)
+    sims = [replace(sim) for _ in range(lanes)]  # a plan (step counter, graphs) per lane
+    streams = [torch.cuda.Stream(device=device()) for _ in range(lanes)]
+    results: list = [None] * len(pairs)
+
+    def lane(k: int) -> torch.cuda.Event:
+        stream = streams[k]
+        stream.wait_event(ready)
+        with torch.cuda.stream(stream):
+            for i in range(k, len(pairs), lanes):
+                source, data = pairs[i]
+                shot_cost, grads, _, _ = adjoint(
+                    sims[k], source, indicator, sensors.nodes, sensors.objective(objective(data))
+                )
+                results[i] = (shot_cost, _reparametrize(sim, indicator, grads))
+            done = torch.cuda.Event()
+            done.record(stream)
+        return done
+
+    with ThreadPoolExecutor(max_workers=lanes) as pool:
+        finished = list(pool.map(lane, range(lanes)))
+    for done in finished:
+        main.wait_event(done)
+    cost = 0.0
+    for shot_cost, shot_gradient in results:
+        shot_gradient.record_stream(main)
         cost += shot_cost
-        gradient += _reparametrize(sim, indicator, grads)
+        gradient += shot_gradient
     return cost, gradient
 
 

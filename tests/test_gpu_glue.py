@@ -90,3 +90,29 @@ def test_glue_arguments_are_checked():
         Sensors(sim, [[1000.0, 2.0]])
     with pytest.raises(NotImplementedError):
         measure(sim, [], design, Sensors(sim, [[3.0, 4.0]]), devices=(0, 1))
+
+
+@pytest.mark.parametrize("name", GLUE)
+def test_misfit_gradient_lanes_match_one_at_a_time(name):
+    """Shots run side by side on their own streams and plans (`lanes`) give the gradient
+    and cost of the shots run in turn, bit for bit, with either adjoint."""
+    from cuwave_b200.sensitivity import reconstruction_sensitivity
+    from cuwave_b200.utils import Sensors, misfit_gradient, shots
+
+    fx = cases.load(name)
+    sim, design = cases.product_sim(fx)
+    dev = torch.device("cuda")
+    signal = fx["signal"][:, 0]
+    coords = np.concatenate([fx["shot_coords"]] * 3)  # more shots than lanes
+    sources = shots(sim, coords, signal)
+    sensors = Sensors(sim, fx["receiver_coords"])
+    observed = [torch.as_tensor(fx["observed"][k % len(fx["observed"])], device=dev)
+                for k in range(len(sources))]
+    for adjoint in (None, reconstruction_sensitivity):
+        kw = {} if adjoint is None else {"adjoint": adjoint}
+        results = {}
+        for lanes in (1, 3):
+            ind = torch.as_tensor(design, device=dev).clone()
+            results[lanes] = misfit_gradient(sim, sources, ind, sensors, observed, lanes=lanes, **kw)
+        assert results[1][0] == results[3][0]
+        np.testing.assert_array_equal(_np(results[1][1]), _np(results[3][1]))
