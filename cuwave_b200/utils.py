@@ -320,29 +320,76 @@ class Sensors:
 
 # ------------------------------------------------------------------------------- fwi
 def measure(sim: Simulation, sources: Sequence[Source], indicator, sensors: Sensors,
-            devices: Sequence[int] | None = None) -> list[torch.Tensor]:
-    """Receiver traces of every shot (cuwave utils.py:369-393)."""
+            devices: Sequence[int] | None = None, lanes: int | None = None) -> list[torch.Tensor]:
+    """Receiver traces of every shot (cuwave utils.py:369-393), the shots side by side on
+    `lanes` (see `misfit_gradient`)."""
     _one_device(devices)
-    return [
-        sensors.traces(simulate(sim, source, indicator, sensors=sensors.nodes)[1])
-        for source in sources
-    ]
+    sources = list(sources)
+    lanes = _lanes(sim, len(sources), simulate) if lanes is None else lanes
+    return _on_lanes(sim, len(sources), lanes, lambda s, i: sensors.traces(
+        simulate(s, sources[i], indicator, sensors=sensors.nodes)[1]))
 
 
 def misfit(sim: Simulation, sources: Sequence[Source], indicator, sensors: Sensors, observed,
-           objective: Callable = l2_misfit, devices: Sequence[int] | None = None) -> float:
+           objective: Callable = l2_misfit, devices: Sequence[int] | None = None,
+           lanes: int | None = None) -> float:
     """The summed cost of `misfit_gradient`, forward passes only (cuwave utils.py:396-407)."""
-    traces = measure(sim, sources, indicator, sensors, devices)
+    traces = measure(sim, sources, indicator, sensors, devices, lanes)
     return sum(objective(data)(t)[0] for t, data in zip(traces, observed))
 
 
-def _lanes(sim: Simulation, shots: int, adjoint: Callable) -> int:
+def _on_lanes(sim: Simulation, count: int, lanes: int, work: Callable) -> list:
+    """[work(sim, i) for i in range(count)], the items side by side on `lanes` lanes: a
+    CUDA stream, a copy of `sim` (so a plan: step counter, graphs) and a host thread
+    each, lane k taking items k, k + lanes, ...; the results in item order, their tensors
+    usable on the caller's stream. The items must be independent."""
+    lanes = max(1, min(int(lanes), count))
+    if lanes <= 1:
+        return [work(sim, i) for i in range(count)]
+    from concurrent.futures import ThreadPoolExecutor
+    from dataclasses import replace
+
+    main = torch.cuda.current_stream()
+    ready = torch.cuda.Event()
+    ready.record(main)
+    sims = [replace(sim) for _ in range(lanes)]
+    streams = [torch.cuda.Stream(device=device()) for _ in range(lanes)]
+    results: list = [None] * count
+
+    def lane(k: int) -> torch.cuda.Event:
+        stream = streams[k]
+        stream.wait_event(ready)
+        with torch.cuda.stream(stream):
+            for i in range(k, count, lanes):
+                results[i] = work(sims[k], i)
+            done = torch.cuda.Event()
+            done.record(stream)
+        return done
+
+    with ThreadPoolExecutor(max_workers=lanes) as pool:
+        finished = list(pool.map(lane, range(lanes)))
+    for done in finished:
+        main.wait_event(done)
+
+    def hand_over(x):
+        if isinstance(x, torch.Tensor):
+            x.record_stream(main)
+        elif isinstance(x, (tuple, list)):
+            for y in x:
+                hand_over(y)
+
+    for r in results:
+        hand_over(r)
+    return results
+
+
+def _lanes(sim: Simulation, shots: int, solver: Callable) -> int:
     """Shots to run side by side: up to four, as many as half the free device memory
-    holds the stored histories of (`sensitivity` keeps N + 2 fields a shot)."""
+    holds the fields of (`sensitivity` keeps N + 2 fields a shot)."""
     if shots <= 1:
         return 1
     field = int(np.prod(sim.Nx_padded)) * torch.empty((), dtype=sim.dtype).element_size()
-    per_shot = (sim.N + 8) * field if adjoint is sensitivity else 16 * field
+    per_shot = (sim.N + 8) * field if solver is sensitivity else 16 * field
     free, _ = torch.cuda.mem_get_info(device())
     return int(max(1, min(4, shots, (free // 2) // max(per_shot, 1))))
 
@@ -378,37 +425,14 @@ def misfit_gradient(sim: Simulation, sources: Sequence[Source], indicator, senso
             gradient += _reparametrize(sim, indicator, grads)
         return cost, gradient
 
-    from concurrent.futures import ThreadPoolExecutor
-    from dataclasses import replace
+    def shot(s: Simulation, i: int):
+        source, data = pairs[i]
+        shot_cost, grads, _, _ = adjoint(s, source, indicator, sensors.nodes,
+                                         sensors.objective(objective(data)))
+        return shot_cost, _reparametrize(sim, indicator, grads)
 
-    main = torch.cuda.current_stream()
-    ready = torch.cuda.Event()
-    ready.record(main)
-    sims = [replace(sim) for _ in range(lanes)]  # a plan (step counter, graphs) per lane
-    streams = [torch.cuda.Stream(device=device()) for _ in range(lanes)]
-    results: list = [None] * len(pairs)
-
-    def lane(k: int) -> torch.cuda.Event:
-        stream = streams[k]
-        stream.wait_event(ready)
-        with torch.cuda.stream(stream):
-            for i in range(k, len(pairs), lanes):
-                source, data = pairs[i]
-                shot_cost, grads, _, _ = adjoint(
-                    sims[k], source, indicator, sensors.nodes, sensors.objective(objective(data))
-                )
-                results[i] = (shot_cost, _reparametrize(sim, indicator, grads))
-            done = torch.cuda.Event()
-            done.record(stream)
-        return done
-
-    with ThreadPoolExecutor(max_workers=lanes) as pool:
-        finished = list(pool.map(lane, range(lanes)))
-    for done in finished:
-        main.wait_event(done)
     cost = 0.0
-    for shot_cost, shot_gradient in results:
-        shot_gradient.record_stream(main)
+    for shot_cost, shot_gradient in _on_lanes(sim, len(pairs), lanes, shot):
         cost += shot_cost
         gradient += shot_gradient
     return cost, gradient

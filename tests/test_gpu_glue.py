@@ -116,3 +116,10 @@ def test_misfit_gradient_lanes_match_one_at_a_time(name):
             results[lanes] = misfit_gradient(sim, sources, ind, sensors, observed, lanes=lanes, **kw)
         assert results[1][0] == results[3][0]
         np.testing.assert_array_equal(_np(results[1][1]), _np(results[3][1]))
+    from cuwave_b200.utils import measure
+
+    ind = torch.as_tensor(design, device=dev).clone()
+    one = measure(sim, sources, ind, sensors, lanes=1)
+    side = measure(sim, sources, ind, sensors, lanes=3)
+    for a, b in zip(one, side):
+        np.testing.assert_array_equal(_np(a), _np(b))
