@@ -112,51 +112,93 @@ __global__ void __launch_bounds__(BX *BY) adjoint_kernel(const AdjointParams<T> 
     }
   }
 
+  // the loads of a plane, issued one plane ahead so that they arrive during the plane
+  // before's arithmetic: the queues' feed (plane a + R) and the tile's halo at plane a
+  // (a thread holds at most one halo node per side along each in-plane axis: R <= BX, BY)
+  static_assert(R <= BX && (NDIM == 2 || R <= BY), "one halo node a side per thread");
+  const bool xh = tx < R, yh = NDIM == 3 && ty < R;
+  T nq[3] = {(T)0, (T)0, (T)0}, nx[3][2], ny[3][2];
+  const auto fetch = [&](const int a) {
+    if (own) {
+      nq[0] = row_val(l1, a + R, true);
+      if constexpr (FL::U)
+        nq[1] = row_val(u1, a + R, true);
+      if constexpr (FL::K)
+        nq[2] = row_val(stiff, a + R, false);
+    }
+    if (xh) {
+      nx[0][0] = plane_val(l1, a, py, x0 - R + tx, true);
+      nx[0][1] = plane_val(l1, a, py, x0 + BX + tx, true);
+      if constexpr (FL::U) {
+        nx[1][0] = plane_val(u1, a, py, x0 - R + tx, true);
+        nx[1][1] = plane_val(u1, a, py, x0 + BX + tx, true);
+      }
+      if constexpr (FL::K) {
+        nx[2][0] = plane_val(stiff, a, py, x0 - R + tx, false);
+        nx[2][1] = plane_val(stiff, a, py, x0 + BX + tx, false);
+      }
+    }
+    if (yh) {
+      ny[0][0] = plane_val(l1, a, y0 - R + ty, px, true);
+      ny[0][1] = plane_val(l1, a, y0 + BY + ty, px, true);
+      if constexpr (FL::U) {
+        ny[1][0] = plane_val(u1, a, y0 - R + ty, px, true);
+        ny[1][1] = plane_val(u1, a, y0 + BY + ty, px, true);
+      }
+      if constexpr (FL::K) {
+        ny[2][0] = plane_val(stiff, a, y0 - R + ty, px, false);
+        ny[2][1] = plane_val(stiff, a, y0 + BY + ty, px, false);
+      }
+    }
+  };
+  if (c0 < c1)
+    fetch(c0);
+
   for (int a0 = c0; a0 < c1; ++a0) {
     T *tL = tiles + ((a0 - c0) & 1) * FL::COUNT * S::PLANE;
     T *tU = tL + S::PLANE;
     T *tK = tL + (FL::U ? 2 : 1) * S::PLANE;
     if (own) {
-      ql[2 * R] = row_val(l1, a0 + R, true);
+      ql[2 * R] = nq[0];
       if constexpr (FL::U)
-        qu[2 * R] = row_val(u1, a0 + R, true);
+        qu[2 * R] = nq[1];
       if constexpr (FL::K)
-        qk[2 * R] = row_val(stiff, a0 + R, false);
+        qk[2 * R] = nq[2];
     }
     const int cc = (ty + HY) * TW + tx + R;
+    if (xh) {
+      const int cl = (ty + HY) * TW + tx, cr = (ty + HY) * TW + BX + R + tx;
+      tL[cl] = nx[0][0];
+      tL[cr] = nx[0][1];
+      if constexpr (FL::U) {
+        tU[cl] = nx[1][0];
+        tU[cr] = nx[1][1];
+      }
+      if constexpr (FL::K) {
+        tK[cl] = nx[2][0];
+        tK[cr] = nx[2][1];
+      }
+    }
+    if (yh) {
+      const int ct = ty * TW + tx + R, cb = (BY + HY + ty) * TW + tx + R;
+      tL[ct] = ny[0][0];
+      tL[cb] = ny[0][1];
+      if constexpr (FL::U) {
+        tU[ct] = ny[1][0];
+        tU[cb] = ny[1][1];
+      }
+      if constexpr (FL::K) {
+        tK[ct] = ny[2][0];
+        tK[cb] = ny[2][1];
+      }
+    }
+    if (a0 + 1 < c1)
+      fetch(a0 + 1);
     tL[cc] = own ? ql[R] : plane_val(l1, a0, py, px, true);
     if constexpr (FL::U)
       tU[cc] = own ? qu[R] : plane_val(u1, a0, py, px, true);
     if constexpr (FL::K)
       tK[cc] = own ? qk[R] : plane_val(stiff, a0, py, px, false);
-    for (int e = tx; e < R; e += BX) {
-      const int cl = (ty + HY) * TW + e, cr = (ty + HY) * TW + BX + R + e;
-      tL[cl] = plane_val(l1, a0, py, x0 - R + e, true);
-      tL[cr] = plane_val(l1, a0, py, x0 + BX + e, true);
-      if constexpr (FL::U) {
-        tU[cl] = plane_val(u1, a0, py, x0 - R + e, true);
-        tU[cr] = plane_val(u1, a0, py, x0 + BX + e, true);
-      }
-      if constexpr (FL::K) {
-        tK[cl] = plane_val(stiff, a0, py, x0 - R + e, false);
-        tK[cr] = plane_val(stiff, a0, py, x0 + BX + e, false);
-      }
-    }
-    if (NDIM == 3) {
-      for (int e = ty; e < R; e += BY) {
-        const int ct = e * TW + tx + R, cb = (BY + HY + e) * TW + tx + R;
-        tL[ct] = plane_val(l1, a0, y0 - R + e, px, true);
-        tL[cb] = plane_val(l1, a0, y0 + BY + e, px, true);
-        if constexpr (FL::U) {
-          tU[ct] = plane_val(u1, a0, y0 - R + e, px, true);
-          tU[cb] = plane_val(u1, a0, y0 + BY + e, px, true);
-        }
-        if constexpr (FL::K) {
-          tK[ct] = plane_val(stiff, a0, y0 - R + e, px, false);
-          tK[cb] = plane_val(stiff, a0, y0 + BY + e, px, false);
-        }
-      }
-    }
     __syncthreads();
 
     if (inner) {
@@ -416,11 +458,17 @@ __global__ void __launch_bounds__(A3P_THREADS) adjoint3d_pml_kernel(const Adjoin
       mi = (T)1 / (UNIF ? p.sconst : p.stiff[idx]);
     else
       mi = p.minv[idx];
-    const T wcell = cell_weight<T>(g, A);
+    T wcell = (T)1;  // the cell weight: a half per axis on whose wall the node sits
+#pragma unroll
+    for (int e = 0; e < 3; ++e)
+      if (A[e] == 1 || A[e] == g.n[e] - 2)
+        wcell *= (T)0.5;
     T ln = l0[idx];
     T gm = GR ? p.g_mass[idx] : (T)0;
     const T uc = GR ? level<T>(p.u1, t)[idx] : (T)0;
-#pragma unroll 1
+    // the axes in order, every loop unrolled: a tap's memory index is base + r * rs for
+    // its slab row r (the grid with axis d replaced by its slab rows)
+#pragma unroll
     for (int d = 0; d < 3; ++d) {
       const int lo_d = g.lo[d], hi_d = g.hi[d];
       if (!(lo_d + hi_d))
@@ -432,27 +480,34 @@ __global__ void __launch_bounds__(A3P_THREADS) adjoint3d_pml_kernel(const Adjoin
         continue;
       const T *mem = p.mem[d];
       const int sz = p.memrow[d];
-      int B[3] = {A[0], A[1], A[2]};
+      const int rows = lo_d + hi_d;
+      const int e1 = g.ext[1], e2 = g.ext[2];
+      const int base = d == 0 ? A[1] * e2 + A[2]
+                     : d == 1 ? A[0] * rows * e2 + A[2]
+                              : (A[0] * e1 + A[1]) * rows;
+      const int rs = d == 0 ? e1 * e2 : d == 1 ? e2 : 1;
       const auto tap = [&](const int ai, const int q) -> T {
-        const int r = slab_row(ai, N, lo_d, hi_d);
-        B[d] = ai;
-        const int i = slab_index(g, d, r, B);
+        const int i = base + slab_row(ai, N, lo_d, hi_d) * rs;
         return mem[3 * sz + i] * plus_tap<T, R>(p.w, q) +
                mem[4 * sz + i] * minus_tap<T, R>(p.w, q);
       };
       T sum = (T)0;
-#pragma unroll 1
+#pragma unroll
       for (int m = -R; m <= R; ++m)
         if (slab_row(a + m, N, lo_d, hi_d) >= 0)
           sum += tap(a + m, -m);
-#pragma unroll 1
+#pragma unroll
       for (int high = 0; high < 2; ++high) {
-        // the reads past the wall that land on a, folded back, odd on a Dirichlet face
+        // the reads past the wall that land on a, folded back, odd on a Dirichlet face;
+        // none reaches a node more than R + 1 from the wall (skipping its zero fold
+        // leaves the sum's bits as they are: it starts at +0 and cannot turn -0)
+        if (high ? a < N - 2 - R : a > R + 1)
+          continue;
         const int ghost = high ? 2 * (N - 2) - a : 2 - a;
         if (high ? ghost < N - 1 : ghost > 0)
           continue;
         T fold = (T)0;
-#pragma unroll 1
+#pragma unroll
         for (int kk = 1; kk <= R; ++kk) {
           const int ai = high ? N - 1 - kk : kk;
           if (slab_row(ai, N, lo_d, hi_d) >= 0 && ghost - ai >= -R && ghost - ai <= R)

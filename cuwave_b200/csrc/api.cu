@@ -663,9 +663,62 @@ int step_setup(const cwb_plan *p, const cwb_op &op, cwb::StepParams<T> &sp, int 
   return CWB_OK;
 }
 
-// An internal refill op's flags: the fast axis' faces (bit 0 low, bit 1 high, times
+// An internal refill op's flags: the faces (bit 2d low, 2d + 1 high of axis d, times
 // this) that an earlier launch of the step refilled already.
-constexpr int OP_REFILLED_FAST = 1 << 28;
+constexpr int OP_REFILLED = 1 << 24;
+
+// The sources' mirror positions on `axis`: whether a folded source sits at index a there.
+int sources_at(const cwb_plan *p, const cwb_op &op, cudaStream_t stream, const int axis,
+               const int a, const int b, bool &at_a, bool &at_b) {
+  const Geometry &g = p->geo;
+  at_a = at_b = false;
+  const cwb_points &src = op.points;
+  if (!(op.flags & CWB_FOLD_SOURCES) || src.num <= 0)
+    return CWB_OK;
+  std::vector<int> lin(src.num);
+  CWB_CUDA(cudaMemcpyAsync(lin.data(), src.lin, sizeof(int) * src.num, cudaMemcpyDeviceToHost, stream));
+  CWB_CUDA(cudaStreamSynchronize(stream));
+  for (const int l : lin) {
+    const int c = axis == 0 ? l / g.s[0] : (l % g.s[axis - 1]) / g.s[axis];
+    at_a = at_a || c == a;
+    at_b = at_b || c == b;
+  }
+  return CWB_OK;
+}
+
+// The 2D quad step's face ghosts pml2d_kernel may refill itself (1 row 0, 2 row N0 - 1,
+// 4 column 0, 8 column NF - 1): a face refilled this step whose mirror row or column the
+// pml launch's threads hold (an axis-0 slab reaching row 2 or N0 - 3; an axis-1 slab on
+// that side with ghost and mirror in one quad that only that side's threads write) and
+// no folded source on it.
+int ghost_fold_2d(const cwb_plan *p, const cwb_op &op, cudaStream_t stream, int &fold) {
+  const Geometry &g = p->geo;
+  fold = 0;
+  if (g.ndim != 2 || !(op.flags & CWB_FOLD_REFILL))
+    return CWB_OK;
+  const int N0 = g.n[0], NF = g.n[1];
+  const int faces = p->grid.neumann | p->grid.dirichlet;
+  if ((faces & 1) && g.lo[0] >= 2)
+    fold |= 1;
+  if ((faces & 2) && g.hi[0] >= 2)
+    fold |= 2;
+  if ((faces & 4) && g.lo[1] > 0 && NF - 1 - g.hi[1] > 3)
+    fold |= 4;
+  if ((faces & 8) && g.hi[1] > 0 && (NF - 1) % 4 >= 2 && g.lo[1] < (NF - 1) / 4 * 4)
+    fold |= 8;
+  bool r2, rn, c2, cn;
+  int rc;
+  if (fold && ((rc = sources_at(p, op, stream, 0, 2, N0 - 3, r2, rn)) ||
+               (rc = sources_at(p, op, stream, 1, 2, NF - 3, c2, cn))))
+    return rc;
+  if (fold) {
+    if (r2) fold &= ~1;
+    if (rn) fold &= ~2;
+    if (c2) fold &= ~4;
+    if (cn) fold &= ~8;
+  }
+  return CWB_OK;
+}
 
 // The 3D step's fast-axis face ghosts the axis-2 pml launch may refill itself (1 low,
 // 2 high): the face lined by the pml and refilled this step, its ghost and mirror in one
@@ -683,18 +736,14 @@ int x_ghost_fold(const cwb_plan *p, const cwb_op &op, cudaStream_t stream, int &
     fold |= 1;
   if (hi > 0 && ((faces >> 5) & 1) && (NF - 1) % 4 >= 2 && lo < (NF - 1) / 4 * 4)
     fold |= 2;
-  const cwb_points &src = op.points;
-  if (fold && (op.flags & CWB_FOLD_SOURCES) && src.num > 0) {
-    std::vector<int> lin(src.num);
-    CWB_CUDA(cudaMemcpyAsync(lin.data(), src.lin, sizeof(int) * src.num, cudaMemcpyDeviceToHost, stream));
-    CWB_CUDA(cudaStreamSynchronize(stream));
-    for (const int l : lin) {
-      const int x = l % g.s[1];
-      if (x == 2)
-        fold &= ~1;
-      if (x == NF - 3)
-        fold &= ~2;
-    }
+  bool at_lo, at_hi;
+  if (fold) {
+    if (const int rc = sources_at(p, op, stream, 2, 2, NF - 3, at_lo, at_hi))
+      return rc;
+    if (at_lo)
+      fold &= ~1;
+    if (at_hi)
+      fold &= ~2;
   }
   return CWB_OK;
 }
@@ -766,6 +815,7 @@ int translate(cwb_plan *p, const cwb_op &op, const size_t slot, cudaStream_t str
                        aligned16(op.a.base, op.a.stride) && aligned16(op.b.base, op.b.stride) &&
                        aligned16(op.c.base, op.c.stride) && (derive || aligned16(sp.minv, 0)) &&
                        g.n[0] >= 3 * R && g.n[1] >= 3 * R;
+    int refilled = 0;  // face ghosts a launch before the refill has written (face bits)
     if (quad2) {
       // enough quads x row chunks to give every SM a few blocks of 128 threads
       const long long rows = g.n[0] - 2, quads = (g.n[1] - 2) / 4 + 1;
@@ -800,6 +850,11 @@ int translate(cwb_plan *p, const cwb_op &op, const size_t slot, cudaStream_t str
         lay.nhi = hi1 > 0 ? (NF - 2) / 4 - (NF - 1 - hi1) / 4 + 1 : 0;
         lay.na = (long long)(g.lo[0] + g.hi[0]) * quads;
         lay.total = lay.na + (long long)(g.n[0] - 2 - g.lo[0] - g.hi[0]) * (lay.nlo + lay.nhi);
+        if ((rc = ghost_fold_2d(p, op, stream, lay.fold)))
+          return rc;
+        if (lay.total <= 0)
+          lay.fold = 0;
+        refilled = lay.fold;
         if (lay.total > 0)
           out.push_back([sp, lay, R](cudaStream_t s, bool adv) {
             cwb::StepParams<T> q = sp;
@@ -835,6 +890,7 @@ int translate(cwb_plan *p, const cwb_op &op, const size_t slot, cudaStream_t str
             return rc;
           if ((rc = pml_launch<T>(p, sp, fold, out)))
             return rc;
+          refilled = fold << 4;
         }
       }
       if ((op.flags & CWB_FOLD_SOURCES) && op.points.num > 0) {
@@ -852,7 +908,7 @@ int translate(cwb_plan *p, const cwb_op &op, const size_t slot, cudaStream_t str
         cwb_op rf;
         std::memset(&rf, 0, sizeof rf);
         rf.kind = CWB_OP_REFILL;
-        rf.flags = fold * OP_REFILLED_FAST;  // faces the pml launch refilled
+        rf.flags = refilled * OP_REFILLED;  // faces the pml launch refilled
         rf.a = op.c;
         if ((rc = translate<T>(p, rf, slot, stream, out)))
           return rc;
@@ -1099,6 +1155,9 @@ int translate(cwb_plan *p, const cwb_op &op, const size_t slot, cudaStream_t str
     if ((rc = fill_material<T>(p, op.mat, &stiff, &minv, &damping, prof, sconst, gconst,
                                dgconst, flags, uniform, true)))
       return rc;
+    cwb::PmlAuxSet<T> set;
+    std::memset(&set, 0, sizeof set);
+    set.ctr = p->ctr;
     for (int d = 0; d < ndim; ++d) {
       if (!lined(p, d))
         continue;
@@ -1118,12 +1177,17 @@ int translate(cwb_plan *p, const cwb_op &op, const size_t slot, cudaStream_t str
       pa.sconst = sconst;
       pa.uniform = uniform;
       pa.ctr = p->ctr;
-      out.push_back([pa](cudaStream_t s, bool adv) {
-        cwb::PmlAuxParams<T> q = pa;
+      set.ax[set.nax] = pa;
+      set.first[set.nax + 1] =
+          set.first[set.nax] + (pa.memrow + cwb::TRANSFER_THREADS - 1) / cwb::TRANSFER_THREADS;
+      ++set.nax;
+    }
+    if (set.nax)
+      out.push_back([set](cudaStream_t s, bool adv) {
+        cwb::PmlAuxSet<T> q = set;
         q.flags = adv ? cwb::K_ADV : 0;
         return cwb::launch_pml_aux<T>(q, s);
       });
-    }
     return CWB_OK;
   }
   case CWB_OP_EXCITE:
@@ -1144,9 +1208,8 @@ int translate(cwb_plan *p, const cwb_op &op, const size_t slot, cudaStream_t str
     if (op.kind == CWB_OP_REFILL) {
       kind = cwb::TR_REFILL;
       faces = p->grid.neumann | p->grid.dirichlet;
-      // an internal refill after the 3D pml launches: the fast axis' faces that launch
-      // refilled are left out
-      faces &= ~(((op.flags / OP_REFILLED_FAST) & 3) << (2 * (ndim - 1)));
+      // an internal refill after the pml launch: the faces that launch refilled are left out
+      faces &= ~((op.flags / OP_REFILLED) & 63);
       for (int d = 0; d < ndim; ++d) {
         int face = 1;
         for (int e = 0; e < ndim; ++e)

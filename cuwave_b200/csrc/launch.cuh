@@ -93,7 +93,7 @@ template <typename T>
 cudaError_t launch_transfer(int kind, const TransferParams<T> &p, T *g_mass, int faces,
                             int threads_total, cudaStream_t stream);
 template <typename T>
-cudaError_t launch_pml_aux(const PmlAuxParams<T> &p, cudaStream_t stream);
+cudaError_t launch_pml_aux(const PmlAuxSet<T> &set, cudaStream_t stream);
 template <typename T>
 cudaError_t launch_frechet(const FrechetParams<T> &p, cudaStream_t stream);
 cudaError_t launch_set_counter(int *ctr, int t0, cudaStream_t stream);

@@ -101,4 +101,15 @@ struct PmlAuxParams {
   int *ctr;
 };
 
+// the adjoint pml memory of every lined axis in one launch: axis ax[i]'s slab elements
+// on blocks first[i] .. first[i + 1] - 1
+template <typename T>
+struct PmlAuxSet {
+  PmlAuxParams<T> ax[3];
+  int nax;
+  int first[4];
+  int flags;  // K_ADV
+  int *ctr;
+};
+
 }  // namespace cwb

@@ -340,6 +340,7 @@ struct Pml2Layout {
   int nlo, nhi, xhi;  // axis-1 slab quads on each side, the first high one's x
   long long na;      // threads of the axis-0 slab rows
   long long total;   // all threads
+  int fold;          // face ghosts refilled here (1 row 0, 2 row N0-1, 4 column 0, 8 column NF-1)
 };
 
 template <typename T, int R, bool HOLD>
@@ -484,13 +485,38 @@ __global__ void __launch_bounds__(S2_THREADS) pml2d_kernel(const StepParams<T> p
           node(i, 1, x, NF, Dpu, Dmu, aux[si], aux[sz + si], aux[2 * sz + si]);
         }
       }
-      if (mine == 15) {
+      // the face ghosts whose mirrors this thread holds, refilled from them (cuwave
+      // scalar.cu:535-555): the host folds a face here only when no source sits on its
+      // mirror row or column (the sources come after the pml, the refill after them)
+      int wmask = mine;
+      if ((lay.fold & 4) && xq == 0) {
+        v[0] = (dirF & 1) ? -v[2] : v[2];
+        wmask |= 1;
+      }
+      if ((lay.fold & 8) && xq + 2 <= NF - 1 && NF - 1 <= xq + 3) {
+#pragma unroll
+        for (int a = 2; a < 4; ++a)
+          if (NF - 1 - xq == a) {
+            v[a] = (dirF & 2) ? -v[a - 2] : v[a - 2];
+            wmask |= 1 << a;
+          }
+      }
+      if (wmask == 15) {
         store4(u2 + row, v);
       } else {
 #pragma unroll
         for (int i = 0; i < 4; ++i)
-          if ((mine >> i) & 1)
+          if ((wmask >> i) & 1)
             u2[row + i] = v[i];
+      }
+      if (side == 0 && (((lay.fold & 1) && z == 2) || ((lay.fold & 2) && z == N0 - 3))) {
+        const bool top = z == 2;
+        const T sg = (dir0 & (top ? 1 : 2)) ? (T)-1 : (T)1;
+        T *ghost = u2 + row + (top ? -2LL : 2LL) * s0;
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+          if ((inner >> i) & 1)
+            ghost[i] = sg * v[i];
       }
     }
   }

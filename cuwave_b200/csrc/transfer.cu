@@ -6,6 +6,9 @@
 namespace cwb {
 
 template <typename T>
+cudaError_t launch_refill3d(const TransferParams<T> &p, int faces, cudaStream_t stream);
+
+template <typename T>
 cudaError_t launch_transfer(const int kind, const TransferParams<T> &p, T *g_mass,
                             const int faces, const int threads_total, cudaStream_t stream) {
   const int blocks = (threads_total + TRANSFER_THREADS - 1) / TRANSFER_THREADS;
@@ -16,7 +19,11 @@ cudaError_t launch_transfer(const int kind, const TransferParams<T> &p, T *g_mas
   case TR_LOAD: load_kernel<T><<<blocks, TRANSFER_THREADS, 0, stream>>>(p, g_mass); break;
   case TR_RECORD: record_kernel<T><<<blocks, TRANSFER_THREADS, 0, stream>>>(p); break;
   case TR_REPLAY: replay_kernel<T><<<blocks, TRANSFER_THREADS, 0, stream>>>(p); break;
-  case TR_REFILL: refill_kernel<T><<<blocks, TRANSFER_THREADS, 0, stream>>>(p, faces); break;
+  case TR_REFILL:
+    if (p.g.ndim == 3)
+      return launch_refill3d<T>(p, faces, stream);
+    refill_kernel<T><<<blocks, TRANSFER_THREADS, 0, stream>>>(p, faces);
+    break;
   case TR_DFT: dft_kernel<T><<<blocks, TRANSFER_THREADS, 0, stream>>>(p, g_mass); break;
   default: return cudaErrorInvalidValue;
   }
@@ -24,11 +31,28 @@ cudaError_t launch_transfer(const int kind, const TransferParams<T> &p, T *g_mas
 }
 
 template <typename T>
-cudaError_t launch_pml_aux(const PmlAuxParams<T> &p, cudaStream_t stream) {
-  const int blocks = (p.memrow + TRANSFER_THREADS - 1) / TRANSFER_THREADS;
-  if (blocks <= 0)
+cudaError_t launch_refill3d(const TransferParams<T> &p, const int faces, cudaStream_t stream) {
+  const Geometry &g = p.g;
+  Refill3Layout lay;
+  lay.faces = faces;
+  lay.nq = (g.n[2] - 2) / 4 + 1;
+  lay.n0 = (faces & 3) ? 2LL * (g.n[1] - 2) * lay.nq : 0;
+  lay.n1 = (faces & 12) ? 2LL * (g.n[0] - 2) * lay.nq : 0;
+  const long long n2 = (faces & 48) ? (long long)(g.n[0] - 2) * (g.n[1] - 2) : 0;
+  lay.total = lay.n0 + lay.n1 + n2;
+  if (lay.total <= 0)
+    return cudaSuccess;
+  const long long blocks = (lay.total + TRANSFER_THREADS - 1) / TRANSFER_THREADS;
+  refill3d_kernel<T><<<(unsigned)blocks, TRANSFER_THREADS, 0, stream>>>(p, lay);
+  return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_pml_aux(const PmlAuxSet<T> &set, cudaStream_t stream) {
+  const int blocks = set.first[set.nax];
+  if (set.nax <= 0 || blocks <= 0)
     return cudaErrorInvalidValue;
-  pml_aux_kernel<T><<<blocks, TRANSFER_THREADS, 0, stream>>>(p);
+  pml_aux_kernel<T><<<blocks, TRANSFER_THREADS, 0, stream>>>(set);
   return cudaGetLastError();
 }
 
@@ -69,7 +93,7 @@ template cudaError_t launch_frechet<float>(const FrechetParams<float> &, cudaStr
 template cudaError_t launch_frechet<double>(const FrechetParams<double> &, cudaStream_t);
 template cudaError_t launch_batch_record<float>(const BatchRecordParams<float> &, cudaStream_t);
 template cudaError_t launch_batch_record<double>(const BatchRecordParams<double> &, cudaStream_t);
-template cudaError_t launch_pml_aux<float>(const PmlAuxParams<float> &, cudaStream_t);
-template cudaError_t launch_pml_aux<double>(const PmlAuxParams<double> &, cudaStream_t);
+template cudaError_t launch_pml_aux<float>(const PmlAuxSet<float> &, cudaStream_t);
+template cudaError_t launch_pml_aux<double>(const PmlAuxSet<double> &, cudaStream_t);
 
 }  // namespace cwb

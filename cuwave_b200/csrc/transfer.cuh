@@ -134,16 +134,107 @@ __global__ void refill_kernel(const TransferParams<T> p, const int faces) {
   finish_step(p.ctr, p.flags & K_ADV);
 }
 
+// The same refill on a 3D grid, the faces of axes 0 and 1 a quad of four fast-axis nodes
+// a thread (their ghost rows are contiguous along axis 2), those of axis 2 a row a
+// thread (both sides): for each face asked, the threads of its (side, row, quad) or
+// (plane, row) come one after another on the launch. The values and the nodes written are
+// refill_kernel's; a wall node of a Dirichlet face is zeroed as there.
+struct Refill3Layout {
+  int faces;
+  int nq;            // quads covering nodes 0 .. NF - 2 of a row
+  long long n0, n1;  // threads of axis 0's faces, of axis 1's (both sides each)
+  long long total;
+};
+
+template <typename T>
+__global__ void refill3d_kernel(const TransferParams<T> p, const Refill3Layout lay) {
+  const int t = step_index(p.ctr);
+  const Geometry &g = p.g;
+  long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < lay.total) {
+    T *u = level<T>(p.a, t);
+    const int N0 = g.n[0], NM = g.n[1], NF = g.n[2];
+    const long long s0 = g.s[0], s1 = g.s[1];
+    if (k < lay.n0 + lay.n1) {
+      // a quad of a ghost row of axis 0 or 1: side, the other in-plane index, the quad
+      const int d = k < lay.n0 ? 0 : 1;
+      if (d == 1)
+        k -= lay.n0;
+      const int q = (int)(k % lay.nq);
+      k /= lay.nq;
+      const int other = 1 + (int)(k % (d == 0 ? NM - 2 : N0 - 2));
+      const int side = (int)(k / (d == 0 ? NM - 2 : N0 - 2));
+      if (((lay.faces >> (2 * d + side)) & 1)) {
+        const int N = g.n[d];
+        const long long sd = d == 0 ? s0 : s1;
+        const long long base = (d == 0 ? other * s1 : other * s0) + 4LL * q;
+        const long long ghost = base + (side ? N - 1 : 0) * sd;
+        const long long normal = side ? -sd : sd;
+        const bool odd = (g.dir >> (2 * d + side)) & 1;
+        const int xq = 4 * q;
+        T v[4];
+        load4(v, u + ghost + 2 * normal);
+        int mask = 0;
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+          if (xq + i >= 1 && xq + i <= NF - 2)
+            mask |= 1 << i;
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+          v[i] = odd ? -v[i] : v[i];
+        if (mask == 15) {
+          store4(u + ghost, v);
+        } else {
+#pragma unroll
+          for (int i = 0; i < 4; ++i)
+            if ((mask >> i) & 1)
+              u[ghost + i] = v[i];
+        }
+        if (odd) {
+#pragma unroll
+          for (int i = 0; i < 4; ++i)
+            if ((mask >> i) & 1)
+              u[ghost + normal + i] = (T)0;
+        }
+      }
+    } else {
+      // a row of axis 2's faces: both sides
+      k -= lay.n0 + lay.n1;
+      const int y = 1 + (int)(k % (NM - 2));
+      const int z = 1 + (int)(k / (NM - 2));
+      const long long row = z * s0 + y * s1;
+#pragma unroll
+      for (int side = 0; side < 2; ++side) {
+        if (!((lay.faces >> (4 + side)) & 1))
+          continue;
+        const long long ghost = row + (side ? NF - 1 : 0);
+        const long long normal = side ? -1 : 1;
+        const bool odd = (g.dir >> (4 + side)) & 1;
+        const T v = u[ghost + 2 * normal];
+        u[ghost] = odd ? -v : v;
+        if (odd)
+          u[ghost + normal] = (T)0;
+      }
+    }
+  }
+  finish_step(p.ctr, p.flags & K_ADV);
+}
+
 // The adjoint pml memory of one lined axis from lambda^(n+1), then the coefficients
 // c+ and c- the transposed step gathers (pml_aux_kernel and pml_tap,
 // cuwave/kernels/scalar_sensitivity.cu:518-542, 237-251). One thread per slab node.
+// One launch for every lined axis (PmlAuxSet): a block finds its axis by its index.
 template <typename T>
-__global__ void pml_aux_kernel(const PmlAuxParams<T> p) {
-  const int t = step_index(p.ctr);
+__global__ void pml_aux_kernel(const __grid_constant__ PmlAuxSet<T> set) {
+  int ai = 0;
+  while (ai + 1 < set.nax && (int)blockIdx.x >= set.first[ai + 1])
+    ++ai;
+  const PmlAuxParams<T> &p = set.ax[ai];
+  const int t = step_index(set.ctr);
   const Geometry &g = p.g;
   const int d = p.d;
   const int lo = g.lo[d], hi = g.hi[d], N = g.n[d];
-  long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  long long k = (long long)(blockIdx.x - set.first[ai]) * blockDim.x + threadIdx.x;
   const bool active = k < p.memrow;
   if (active) {
     // decompose the slab index over the grid with axis d replaced by its rows
@@ -201,7 +292,7 @@ __global__ void pml_aux_kernel(const PmlAuxParams<T> p) {
       mem[4 * sz + k] = ah[a - 1] * e1 - gm * (1 + ah[a - 1]) * ez2;
     }
   }
-  finish_step(p.ctr, p.flags & K_ADV);
+  finish_step(set.ctr, set.flags & K_ADV);
 }
 
 // A running DFT at the points: acc[k * num + j] += table[row * columns + k] * a[lin[j]],

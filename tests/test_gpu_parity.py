@@ -185,6 +185,33 @@ def test_blocked_uniform_step_matches_oracle(R, dirichlet, pml, damping):
     np.testing.assert_array_equal(traces, ref_traces)
 
 
+@pytest.mark.parametrize("dirichlet,on_mirrors", [(0b0000, True), (0b1010, True),
+                                                   (0b0101, False), (0b0000, False)])
+def test_quad_2d_pml_step_ghosts_folded_or_not(dirichlet, on_mirrors):
+    """The 2D quad step with a pml refills the face ghosts inside its pml launch where no
+    source sits on the mirror rows and columns (2, N0 - 3; 2, NF - 3), and leaves a face to
+    the refill launch where one does: both equal to the oracle, on a grid of several row
+    chunks too large for the multi-step march."""
+    case, meta = _random_case(2, 4, dirichlet=dirichlet, pml=6, uniform=True, seed=57, nsrc=4,
+                              nsens=9, Nx=(611, 1090))
+    meta["N"] = 12
+    case.signal = case.signal[:12]
+    if on_mirrors:
+        Nx = meta["Nx"]
+        src = meta["src"].copy()
+        src[:, 0] = (2, Nx[1] // 2)
+        src[:, 1] = (Nx[0] - 3, Nx[1] // 3)
+        src[:, 2] = (Nx[0] // 2, 2)
+        src[:, 3] = (Nx[0] // 3, Nx[1] - 3)
+        meta["src"] = src
+        case.source_lin = cases.flat({"Nx": np.array(Nx)}, src)
+        case.source_weight = case.excitation_weights(case.source_lin)
+    field, traces = _product(case, meta)
+    ref_field, ref_traces = case.forward(meta["N"])
+    np.testing.assert_array_equal(field, ref_field)
+    np.testing.assert_array_equal(traces, ref_traces)
+
+
 @pytest.mark.parametrize("dirichlet", [0b000000, 0b110000])
 def test_blocked_step_with_sources_on_the_ghost_mirrors(dirichlet):
     """Sources on the columns whose values the fast axis' face ghosts copy (x = 2 and
