@@ -43,7 +43,9 @@ struct AdjFields {
 // PML: the pml transpose gathered here where the flags ask (else a launch of its own, or
 // none, and no code for it)
 template <typename T, int NDIM, int R, bool UNIF, int MODE, int BX, int BY, bool PML = true>
-__global__ void __launch_bounds__(BX *BY) adjoint_kernel(const AdjointParams<T> p) {
+// (three blocks of 256 an SM for a uniform stiffness in 3D up to radius 4: its registers
+// fit, and the march waits on loads more warps hide)
+__global__ void __launch_bounds__(BX *BY, NDIM == 3 && UNIF && R <= 4 ? 3 : 1) adjoint_kernel(const AdjointParams<T> p) {
   using S = AdjShape<NDIM, R, BX, BY>;
   using FL = AdjFields<MODE, UNIF>;
   constexpr int HY = S::HY, TW = S::TW, F = NDIM - 1;
@@ -118,7 +120,22 @@ __global__ void __launch_bounds__(BX *BY) adjoint_kernel(const AdjointParams<T> 
   static_assert(R <= BX && (NDIM == 2 || R <= BY), "one halo node a side per thread");
   const bool xh = tx < R, yh = NDIM == 3 && ty < R;
   T nq[3] = {(T)0, (T)0, (T)0}, nx[3][2], ny[3][2];
+  // the node's own lambda^(n+2), 1/m and gradient densities at plane a (the transposed
+  // update's point reads), fetched with the rest
+  T nn[4] = {(T)0, (T)0, (T)0, (T)0};
   const auto fetch = [&](const int a) {
+    if constexpr (MODE != MODE_GRAD) {
+      if (inner) {
+        const long long i2 = (long long)a * s0 + col;
+        nn[0] = l0[i2];
+        if (!(p.flags & K_DERIVE))
+          nn[1] = p.minv[i2];
+        if constexpr (MODE == MODE_STEP_GRAD) {
+          nn[2] = p.g_mass[i2];
+          nn[3] = p.g_stiff[i2];
+        }
+      }
+    }
     if (own) {
       nq[0] = row_val(l1, a + R, true);
       if constexpr (FL::U)
@@ -192,6 +209,7 @@ __global__ void __launch_bounds__(BX *BY) adjoint_kernel(const AdjointParams<T> 
         tK[cb] = ny[2][1];
       }
     }
+    const T cur_lo = nn[0], cur_mi = nn[1], cur_gm = nn[2], cur_gs = nn[3];
     if (a0 + 1 < c1)
       fetch(a0 + 1);
     tL[cc] = own ? ql[R] : plane_val(l1, a0, py, px, true);
@@ -273,8 +291,8 @@ __global__ void __launch_bounds__(BX *BY) adjoint_kernel(const AdjointParams<T> 
             gs += stiff_density(d);
           p.g_stiff[idx] -= gs;
         } else {
-          const T lo = l0[idx];
-          const T mi = (flags & K_DERIVE) ? (T)1 / sc : p.minv[idx];
+          const T lo = cur_lo;
+          const T mi = (flags & K_DERIVE) ? (T)1 / sc : cur_mi;
           T div_l = (T)0, gs = (T)0;
 #pragma unroll
           for (int d = 0; d < NDIM; ++d) {
@@ -312,8 +330,8 @@ __global__ void __launch_bounds__(BX *BY) adjoint_kernel(const AdjointParams<T> 
             ln = (T)0;
           T gmass = (T)0, gstiff = (T)0;
           if constexpr (MODE == MODE_STEP_GRAD) {
-            gmass = p.g_mass[idx] - p.mf * uc * (ln - (T)2 * lc + lo);
-            gstiff = p.g_stiff[idx] - p.mf * gs;
+            gmass = cur_gm - p.mf * uc * (ln - (T)2 * lc + lo);
+            gstiff = cur_gs - p.mf * gs;
           }
 
           if (PML && (flags & K_PML)) {

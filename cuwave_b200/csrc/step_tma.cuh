@@ -63,8 +63,15 @@ __device__ __forceinline__ int level_index(const int *L, const int t) {
   return k;
 }
 
+// resident blocks an SM the register budget is cut for: three, or two for the 3D rows
+// of radius 5 and up, whose queues would otherwise spill (364 bytes a thread at radius 8)
+template <int NDIM, int R>
+constexpr int tma_min_blocks() {
+  return NDIM == 3 && R >= 5 ? 2 : TMA_MIN_BLOCKS;
+}
+
 template <typename T, int NDIM, int R, bool UNIF, int BX, int BY, int RY>
-__global__ void __launch_bounds__(BX *(BY / RY), TMA_MIN_BLOCKS)
+__global__ void __launch_bounds__(BX *(BY / RY), tma_min_blocks<NDIM, R>())
     step_tma_kernel(const __grid_constant__ StepTmaParams<T> P) {
   using S = TmaShape<T, NDIM, R, BX, BY>;
   constexpr int H = S::H, HY = S::HY, WB = S::WB, NS = S::STAGES, F = NDIM - 1;

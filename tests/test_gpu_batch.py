@@ -55,6 +55,39 @@ def test_a_batch_of_uneven_problems_is_each_simulate():
         assert torch.equal(got_traces, traces), k
 
 
+def test_a_batch_matches_the_oracle():
+    """The batch against the CPU oracle's restatement of the reference's step sequence,
+    not only against `simulate`: problems of four radius groups (orders 2, 6, 8 and 16),
+    Neumann and mixed Dirichlet faces, different lengths, fields and traces to the bit."""
+    from oracle import oracle as o
+
+    from cuwave_b200.batch import simulate_batch
+
+    rng = np.random.default_rng(11)
+    specs = [dict(Nx=(64, 70), order=2, N=40), dict(Nx=(97, 201), order=8, N=30, dirichlet=True),
+             dict(Nx=(70, 77), order=16, N=35), dict(Nx=(150, 130), order=6, N=25)]
+    problems = [_problem(rng, **spec) for spec in specs]
+    sims, sources, indicators, sensors = (list(x) for x in zip(*problems))
+    batched = simulate_batch(sims, sources, [i.copy() for i in indicators], sensors)
+    for k, (sim, source, indicator, sens) in enumerate(problems):
+        Nx = sim.Nx
+        R = sim.space_order // 2
+        stiff, minv = o.acoustic_materials(Nx, indicator.copy(), 1.0, 1.0, 1.0, 0.5, np.float32)
+        shape = sim.Nx_padded
+        flat = lambda q: (q[0].astype(np.int64) * shape[1] + q[1]).astype(np.int32)  # noqa: E731
+        dirichlet = 0b1001 if specs[k].get("dirichlet") else 0
+        case = o.Case(Nx=Nx, R=R, coeffs=o.cell_coefficients(R, "optimized"),
+                      factors=[np.float32(2.0 * sim.dt**2)] * 2, dt=sim.dt, stiff=stiff, minv=minv,
+                      dtype=np.float32, dirichlet=dirichlet,
+                      source_lin=flat(np.asarray(source.position)),
+                      signal=np.asarray(source.signal, np.float32), sensor_lin=flat(sens))
+        case.source_weight = case.excitation_weights(case.source_lin)
+        field, traces = case.forward(sim.N)
+        got_field, got_traces = batched[k]
+        np.testing.assert_array_equal(got_traces.cpu().numpy(), traces)
+        np.testing.assert_array_equal(got_field.cpu().numpy(), field[:, : Nx[1]])
+
+
 def test_the_batch_refuses_what_it_does_not_step():
     from cuwave_b200 import AcousticWave
     from cuwave_b200.batch import simulate_batch
