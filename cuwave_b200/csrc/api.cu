@@ -13,6 +13,7 @@
 
 #include "cuwave_b200.h"
 #include "launch.cuh"
+#include "march3d.cuh"
 #include "pml.cuh"
 #include "batch.cuh"
 #include "conv.cuh"
@@ -57,6 +58,10 @@ struct cwb_plan {
   int *err = nullptr;  // raised by a kernel whose bounded wait ran out
   bool tma = true;     // stage planes with tensor-map copies where the layout allows
   bool blocked3 = true;  // uniform-stiffness steps on the register-blocked kernels (CWB_STEP3D=0: off)
+  // all steps of a 3D grid whose fields fit march3_bytes in one cooperative launch
+  // (CWB_MARCH3D=0: off; 2: any size)
+  int march3 = 1;
+  long long march3_bytes = 8LL << 20;
   int flow3 = 1;  // the 3D blocked step without a block barrier per plane (CWB_FLOW3D=0: with; 2: deeper ring)
   int pml2d = 1;  // the 2D quad step's pml terms by a launch of their own (CWB_PML2D=0: inside the update kernel)
   cudaStream_t lane = nullptr;
@@ -94,8 +99,15 @@ int chunk_for(const cwb_plan *p, const int plane_blocks) {
   if (p->chunk_override > 0)
     return p->chunk_override;
   const int rows = p->geo.n[0] - 2;
-  if (p->geo.ndim == 3)
-    return std::min(rows, 32);  // the fastest of 32 .. 255 planes measured on 512^3
+  if (p->geo.ndim == 3) {
+    // 32 planes, the fastest of 32 .. 255 measured on 512^3; fewer (down to 8) where
+    // 32-plane chunks would leave the device short of blocks (two a slot of every SM):
+    // a chunk's planes are a chain of waits on staged tiles, so a small grid in long
+    // chunks is as slow as a large one
+    const long long want = 2LL * p->sms;
+    const long long chunk = (rows * (long long)plane_blocks + want - 1) / want;
+    return (int)std::min<long long>(rows, std::max<long long>(8, std::min<long long>(32, chunk)));
+  }
   const long long want = 8LL * p->sms;
   const long long chunk = (rows * (long long)plane_blocks + want - 1) / want;
   return (int)std::max<long long>(8, std::min<long long>(rows, chunk));
@@ -1282,6 +1294,118 @@ int enqueue_step(const std::vector<Launch> &launches, cudaStream_t s) {
 }
 
 template <typename T>
+cudaError_t march3d_r(const cwb::March3Params<T> &mp, const int R, const bool uniform,
+                      const int sms, cudaStream_t s) {
+  switch (R) {
+  case 1: return cwb::march3d_unit<T, 1>(mp, uniform, sms, s);
+  case 2: return cwb::march3d_unit<T, 2>(mp, uniform, sms, s);
+  case 3: return cwb::march3d_unit<T, 3>(mp, uniform, sms, s);
+  case 4: return cwb::march3d_unit<T, 4>(mp, uniform, sms, s);
+  case 5: return cwb::march3d_unit<T, 5>(mp, uniform, sms, s);
+  case 6: return cwb::march3d_unit<T, 6>(mp, uniform, sms, s);
+  case 7: return cwb::march3d_unit<T, 7>(mp, uniform, sms, s);
+  case 8: return cwb::march3d_unit<T, 8>(mp, uniform, sms, s);
+  }
+  return cudaErrorInvalidValue;
+}
+
+// A 3D op list [step (sources and refill folded), records] on a grid small enough for its
+// fields to stay in L2 runs as one cooperative launch of all its steps (march3d_kernel:
+// the generic tile step, a grid barrier before the records). Returns false where the
+// list is another shape or the grid too large, leaving it to the per-step march.
+template <typename T>
+bool march3d_path(cwb_plan *p, const cwb_op *ops, const int nops, const int t0, const int steps,
+                  cudaStream_t user, int &rc) {
+  const Geometry &g = p->geo;
+  const int R = p->grid.radius;
+  if (!p->march3 || g.ndim != 3 || steps < 16 || nops < 1 || nops > 1 + cwb::MARCH3_RECORDS ||
+      ops[0].kind != CWB_OP_STEP || ops[0].mat.cells || !(ops[0].flags & CWB_FOLD_REFILL))
+    return false;
+  for (int i = 1; i < nops; ++i)
+    if (ops[i].kind != CWB_OP_RECORD || ops[i].points.num <= 0 || !ops[i].points.lin ||
+        !ops[i].points.record || ops[i].points.store < 0 || ops[i].points.store > 2 ||
+        (ops[i].points.store == 2 && sizeof(T) == 4) || check_level(ops[i].a, "a"))
+      return false;
+  // fields L2 holds between steps, where a step's launches cost more than its work
+  const long long field = (long long)g.n[0] * g.n[1] * g.ext[2] * (long long)sizeof(T);
+  if (p->march3 < 2 && 3 * field > p->march3_bytes)
+    return false;
+  const cwb_op &op = ops[0];
+  cwb::March3Params<T> mp;
+  std::memset(&mp, 0, sizeof mp);
+  cwb::StepParams<T> &sp = mp.s;
+  int flags = 0;
+  bool uniform = false;
+  if (step_setup<T>(p, op, sp, flags, uniform))
+    return false;
+  const int bytes = sizeof(T);
+  int bx, by;
+  cwb::block_shape(3, bx, by);
+  const int gx = (g.ext[2] + bx - 1) / bx, gy = (g.n[1] + by - 1) / by;
+  const int rows = g.n[0] - 2;
+  // about two tiles a resident block slot, no chunk under two planes
+  const long long want = 2LL * p->sms;
+  int chunk = (int)std::max<long long>(2, ((long long)rows * gx * gy + want - 1) / want);
+  if (p->chunk_override > 0)
+    chunk = p->chunk_override;
+  chunk = std::min(chunk, rows);
+  const int gz = (rows + chunk - 1) / chunk;
+  sp.chunk = chunk;
+  flags |= cwb::K_REFILL;
+  sp.refill = p->grid.neumann | p->grid.dirichlet;
+  rc = CWB_OK;
+  if ((op.flags & CWB_FOLD_SOURCES) && op.points.num > 0) {
+    if (!op.points.weight || !op.points.record)
+      return rc = fail(CWB_ERR_ARG, "folded sources need weights and a signal"), true;
+    flags |= cwb::K_SRC;
+    if ((rc = build_sources<T>(p, 0, op.points, dim3(gx, gy, gz), chunk, bx, by, user,
+                               &sp.src_start, &sp.src_entry)))
+      return true;
+    sp.src_weight = static_cast<const T *>(op.points.weight);
+    sp.signal = static_cast<const T *>(op.points.record);
+    sp.nsrc = op.points.num;
+    sp.sig_mul = op.points.row_mul;
+    sp.sig_add = op.points.row_add;
+  }
+  sp.flags = flags;
+  sp.u0 = to_level(op.a, bytes);
+  sp.u1 = to_level(op.b, bytes);
+  sp.u2 = to_level(op.c, bytes);
+  sp.ctr = p->ctr;
+  mp.nbx = gx;
+  mp.nby = gy;
+  mp.nbz = gz;
+  mp.nrec = nops - 1;
+  for (int i = 1; i < nops; ++i) {
+    cwb::TransferParams<T> &tp = mp.rec[i - 1];
+    tp.g = g;
+    tp.a = to_level(ops[i].a, bytes);
+    tp.lin = ops[i].points.lin;
+    tp.record = ops[i].points.record;
+    tp.num = ops[i].points.num;
+    tp.row_mul = ops[i].points.row_mul;
+    tp.row_add = ops[i].points.row_add;
+    tp.store = ops[i].points.store;
+    tp.ctr = p->ctr;
+  }
+  mp.t0 = t0;
+  mp.steps = steps;
+  const auto run = [&]() -> int {
+    CWB_CUDA(cudaEventRecord(p->fork, user));
+    CWB_CUDA(cudaStreamWaitEvent(p->lane, p->fork, 0));
+    cudaStream_t s = p->lane;
+    CWB_CUDA(cwb::launch_set_counter(p->ctr, t0, s));
+    CWB_CUDA(march3d_r<T>(mp, R, uniform, p->sms, s));
+    g_launches += 2;
+    CWB_CUDA(cudaEventRecord(p->join, s));
+    CWB_CUDA(cudaStreamWaitEvent(user, p->join, 0));
+    return CWB_OK;
+  };
+  rc = run();
+  return true;
+}
+
+template <typename T>
 cudaError_t march2d_r(const cwb::March2Params<T> &mp, const int R, const int sms, cudaStream_t s) {
   switch (R) {
   case 1: return cwb::march2d_unit<T, 1>(mp, sms, s);
@@ -1683,6 +1807,8 @@ int march(cwb_plan *p, const cwb_op *ops, const int nops, const int t0, const in
     }
     if (march2d_path<T>(p, ops, nops, t0, steps, user, rc))
       return rc;
+    if (march3d_path<T>(p, ops, nops, t0, steps, user, rc))
+      return rc;
     if (p->tblock == 1 && blocked()) {
       if (rc || done == steps)
         return rc;
@@ -1801,6 +1927,8 @@ int plan_geometry(const cwb_grid &G, cwb_plan &p) {
     p.tma = std::atoi(env) == 0;
   if (const char *env = std::getenv("CWB_STEP3D"))
     p.blocked3 = std::atoi(env) != 0;
+  if (const char *env = std::getenv("CWB_MARCH3D"))
+    p.march3 = std::atoi(env);
   if (const char *env = std::getenv("CWB_PML2D"))
     p.pml2d = std::atoi(env);
   if (const char *env = std::getenv("CWB_FLOW3D"))

@@ -60,6 +60,12 @@ cudaError_t adjoint2d_pml_unit(const AdjointParams<T> &p, const Adj2Reach &reach
                                dim3 grid, cudaStream_t stream);
 
 template <typename T>
+struct March3Params;
+// all steps of an L2-resident 3D grid in one cooperative launch (the generic tile step)
+template <typename T, int R>
+cudaError_t march3d_unit(const March3Params<T> &p, bool uniform, int sms, cudaStream_t stream);
+
+template <typename T>
 struct March2Params;
 // the multi-step 2D march, one cooperative launch of as many blocks as fit on `sms` SMs
 template <typename T, int R>

@@ -107,23 +107,24 @@ struct StepShape {
   static constexpr int PLANE = TW * TH;
 };
 
+// One block's tile of step t: the tile (bx, by) of the plane, chunk bz along axis 0 (in
+// 2D: bx, chunk by), of a grid of nbx x nby tiles; `tiles` the block's shared memory.
 template <typename T, int NDIM, int R, bool UNIF, int BX, int BY>
-__global__ void __launch_bounds__(BX *BY) step_kernel(const StepParams<T> p) {
+__device__ __forceinline__ void step_block(const StepParams<T> &p, const int t, const int bx,
+                                           const int by, const int bz, const int nbx,
+                                           const int nby, T *tiles) {
   using S = StepShape<NDIM, R, BX, BY>;
   constexpr int HY = S::HY, TW = S::TW, F = NDIM - 1;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  T *tiles = reinterpret_cast<T *>(smem_raw);
 
   const Geometry &g = p.g;
-  const int t = step_index(p.ctr);
   const T *u0 = level<T>(p.u0, t);
   const T *__restrict__ u1 = level<T>(p.u1, t);
   T *u2 = level<T>(p.u2, t);
 
   const int tx = threadIdx.x, ty = threadIdx.y;
-  const int x0 = blockIdx.x * BX;
-  const int y0 = NDIM == 3 ? blockIdx.y * BY : 0;
-  const int cz = NDIM == 3 ? blockIdx.z : blockIdx.y;
+  const int x0 = bx * BX;
+  const int y0 = NDIM == 3 ? by * BY : 0;
+  const int cz = NDIM == 3 ? bz : by;
   const int N0 = g.n[0], NF = g.n[F], NM = NDIM == 3 ? g.n[1] : 1;
   const int s0 = g.s[0], sM = NDIM == 3 ? g.s[1] : 0;
   const int px = x0 + tx, py = y0 + ty;
@@ -167,7 +168,7 @@ __global__ void __launch_bounds__(BX *BY) step_kernel(const StepParams<T> p) {
   int sfirst = 0, slast = 0, srow = 0;
   const int lane = ty * BX + tx;
   if (flags & K_SRC) {
-    const int blk = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+    const int blk = bx + nbx * (by + nby * bz);
     sfirst = p.src_start[blk];
     slast = p.src_start[blk + 1];
     srow = p.sig_mul * t + p.sig_add;
@@ -334,7 +335,14 @@ __global__ void __launch_bounds__(BX *BY) step_kernel(const StepParams<T> p) {
     for (int k = 0; k < 2 * R; ++k)
       q[k] = q[k + 1];
   }
-  finish_step(p.ctr, flags & K_ADV);
+}
+
+template <typename T, int NDIM, int R, bool UNIF, int BX, int BY>
+__global__ void __launch_bounds__(BX *BY) step_kernel(const StepParams<T> p) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  step_block<T, NDIM, R, UNIF, BX, BY>(p, step_index(p.ctr), blockIdx.x, blockIdx.y, blockIdx.z,
+                                       gridDim.x, gridDim.y, reinterpret_cast<T *>(smem_raw));
+  finish_step(p.ctr, p.flags & K_ADV);
 }
 
 }  // namespace cwb

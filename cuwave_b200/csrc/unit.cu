@@ -13,6 +13,7 @@
 #include "step3d.cuh"
 #include "step3d_flow.cuh"
 #include "tblock2d.cuh"
+#include "march3d.cuh"
 
 #if !defined(CWB_REAL) || !defined(CWB_NDIM) || !defined(CWB_RADIUS)
 #error "unit.cu is compiled with CWB_REAL, CWB_NDIM and CWB_RADIUS"
@@ -299,6 +300,30 @@ cudaError_t adjoint_unit(const AdjointParams<T> &p, const bool u, const int mode
 }
 
 #if CWB_NDIM == 3
+template <typename T, int R>
+cudaError_t march3d_unit(const March3Params<T> &mp, const bool uniform, const int sms,
+                         cudaStream_t s) {
+  constexpr int BX = STEP_BX3, BY = STEP_BY3;
+  const auto k = uniform ? march3d_kernel<T, R, true, BX, BY> : march3d_kernel<T, R, false, BX, BY>;
+  const size_t smem = 2 * StepShape<3, R, BX, BY>::PLANE * sizeof(T);
+  cudaError_t e = allow_smem(k, smem);
+  if (e != cudaSuccess)
+    return e;
+  int per = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, BX * BY, smem);
+  if (e != cudaSuccess)
+    return e;
+  if (per < 1)
+    return cudaErrorInvalidConfiguration;
+  const long long ntiles = (long long)mp.nbx * mp.nby * mp.nbz;
+  const unsigned blocks = (unsigned)std::min<long long>(ntiles, (long long)per * sms);
+  void *args[] = {const_cast<March3Params<T> *>(&mp)};
+  return cudaLaunchCooperativeKernel(reinterpret_cast<const void *>(k), dim3(blocks), dim3(BX, BY),
+                                     args, smem, s);
+}
+template cudaError_t march3d_unit<CWB_REAL, CWB_RADIUS>(const March3Params<CWB_REAL> &, bool, int,
+                                                        cudaStream_t);
+
 template <typename T, int R>
 cudaError_t adjoint3d_pml_unit(const AdjointParams<T> &p, const Adj3Reach &reach, const bool u,
                                const int mode, const dim3 grid, cudaStream_t s) {
