@@ -59,7 +59,7 @@ def test_sensitivity_matches_reference(name):
 
 
 def _random_case(ndim, R, *, dirichlet=0, pml=0, uniform=False, damping=False, seed=1,
-                 dtype=np.float32, nsrc=3, nsens=5, Nx=None):
+                 dtype=np.float32, nsrc=3, nsens=5, Nx=None, faces=None):
     """A seeded case with a heterogeneous stiffness, for the oracle and the product."""
     rng = np.random.default_rng(seed)
     if Nx is None:
@@ -74,7 +74,10 @@ def _random_case(ndim, R, *, dirichlet=0, pml=0, uniform=False, damping=False, s
     o.mirror_ghosts(Nx, stiff)
     o.mirror_ghosts(Nx, minv)
     dt = 0.4 * o.stable_dt((1.0,) * ndim, 1.3 * 1.2, 2 * R, "optimized")
-    widths = tuple((pml, pml) for _ in range(ndim)) if pml else None
+    widths = None
+    if pml:
+        lined = set(range(2 * ndim)) if faces is None else set(faces)
+        widths = tuple(tuple(pml if 2 * d + side in lined else 0 for side in (0, 1)) for d in range(ndim))
     profiles = o.pml_profiles(Nx, (1.0,) * ndim, dt, widths, pml, 1.6, 1e-6, 0.0, dtype) if pml else None
     src = np.stack([rng.integers(2, n - 2, nsrc) for n in Nx]).astype(np.int32)
     sens = np.stack([rng.integers(1, n - 1, nsens) for n in Nx]).astype(np.int32)
@@ -91,7 +94,7 @@ def _random_case(ndim, R, *, dirichlet=0, pml=0, uniform=False, damping=False, s
                   profiles=profiles, source_lin=cases.flat({"Nx": np.array(Nx)}, src),
                   signal=signal, sensor_lin=cases.flat({"Nx": np.array(Nx)}, sens))
     case.source_weight = case.excitation_weights(case.source_lin)
-    return case, dict(Nx=Nx, dt=dt, src=src, sens=sens, N=N, pml=pml, dirichlet=dirichlet)
+    return case, dict(Nx=Nx, dt=dt, src=src, sens=sens, N=N, pml=pml, dirichlet=dirichlet, faces=faces)
 
 
 def _product(case, meta):
@@ -105,7 +108,7 @@ def _product(case, meta):
         tuple(Dirichlet if (meta["dirichlet"] >> (2 * d + s)) & 1 else Neumann for s in (0, 1))
         for d in range(ndim)
     )
-    pml = Pml(width=meta["pml"], wavespeed=1.6) if meta["pml"] else None
+    pml = Pml(width=meta["pml"], wavespeed=1.6, faces=meta.get("faces")) if meta["pml"] else None
     precision = "float32" if case.dtype == np.float32 else "float64"
     sim = AcousticWave(Nx=meta["Nx"], dx=(1.0,) * ndim, N=meta["N"], dt=meta["dt"],
                        precision=precision, space_order=2 * case.R, boundary=boundary, pml=pml,
@@ -179,6 +182,24 @@ def test_blocked_uniform_step_matches_oracle(R, dirichlet, pml, damping):
     segments of rows a side, the last one short."""
     case, meta = _random_case(3, R, dirichlet=dirichlet, pml=pml, uniform=True, damping=damping,
                               seed=11 + R, nsrc=6, nsens=9, Nx=(45, 37, 139))
+    field, traces = _product(case, meta)
+    ref_field, ref_traces = case.forward(meta["N"])
+    np.testing.assert_array_equal(field, ref_field)
+    np.testing.assert_array_equal(traces, ref_traces)
+
+
+@pytest.mark.parametrize("R,faces,pml,dirichlet", [
+    (4, (1, 2, 5), 20, 0b000000), (4, (0, 3, 4), 9, 0b100001), (3, (2, 3), 17, 0b000100),
+    (2, (4, 5), 70, 0b000000), (1, (0, 1, 3, 4), 5, 0b110000),
+])
+def test_blocked_step_with_pml_on_some_faces(R, faces, pml, dirichlet):
+    """The blocked 3D step's pml on a subset of faces (a side lined, the other not), the
+    slabs of axes 1 and 2 taken inside the step's own tiles: tiles that meet a slab but no
+    wall, an axis-2 slab wider than a tile, Dirichlet faces beside a lined one."""
+    case, meta = _random_case(3, R, dirichlet=dirichlet, pml=pml, uniform=True, seed=200 + R,
+                              nsrc=4, nsens=9, Nx=(41, 53, 97), faces=faces)
+    meta["N"] = 24
+    case.signal = case.signal[:24]
     field, traces = _product(case, meta)
     ref_field, ref_traces = case.forward(meta["N"])
     np.testing.assert_array_equal(field, ref_field)
