@@ -579,7 +579,7 @@ def batch_problems(count: int, steps: int, seed: int = 3):
     return problems
 
 
-def batch_measure(count: int = 64, steps: int = 300) -> dict:
+def batch_measure(count: int = 64, steps: int = 1500) -> dict:
     """simulate_batch over the design population (batch_problems) against the same simulate calls in turn
     (device time, CUDA events; the second of two runs, the first tunes and loads)."""
     import torch

@@ -384,14 +384,14 @@ def _on_lanes(sim: Simulation, count: int, lanes: int, work: Callable) -> list:
 
 
 def _lanes(sim: Simulation, shots: int, solver: Callable) -> int:
-    """Shots to run side by side: up to four, as many as half the free device memory
+    """Shots to run side by side: up to eight, as many as half the free device memory
     holds the fields of (`sensitivity` keeps N + 2 fields a shot)."""
     if shots <= 1:
         return 1
     field = int(np.prod(sim.Nx_padded)) * torch.empty((), dtype=sim.dtype).element_size()
     per_shot = (sim.N + 8) * field if solver is sensitivity else 16 * field
     free, _ = torch.cuda.mem_get_info(device())
-    return int(max(1, min(4, shots, (free // 2) // max(per_shot, 1))))
+    return int(max(1, min(8, shots, (free // 2) // max(per_shot, 1))))
 
 
 def misfit_gradient(sim: Simulation, sources: Sequence[Source], indicator, sensors: Sensors,
@@ -407,7 +407,7 @@ def misfit_gradient(sim: Simulation, sources: Sequence[Source], indicator, senso
 
     The shots are independent, so `lanes` of them run side by side, each lane a CUDA
     stream with a plan of its own driven from its own host thread (by default as many
-    as the free memory holds, at most four); every shot's gradient is kept apart and the
+    as the free memory holds, at most eight); every shot's gradient is kept apart and the
     sum taken in shot order afterwards, so the result is the one-at-a-time result to the
     bit. `lanes=1` runs them in turn.
     """
