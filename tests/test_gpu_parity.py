@@ -288,6 +288,10 @@ def test_quad_2d_step_by_step_on_a_large_grid():
     (2, 3, 0b1001, 4, False, (67, 91)), (2, 4, 0b0110, 5, False, (75, 139)),
     (2, 4, 0b0000, 0, True, (67, 91)), (2, 4, 0b1111, 0, False, (59, 101)),
     (3, 2, 0b100110, 3, False, (23, 21, 27)),
+    # 3D: several chunks of planes and tiles, radius 1 to 4, walls, a pml, damping
+    (3, 1, 0b000000, 0, False, (37, 29, 71)), (3, 3, 0b011001, 4, False, (30, 41, 75)),
+    (3, 4, 0b000000, 5, False, (29, 35, 77)), (3, 4, 0b111111, 0, False, (27, 25, 45)),
+    (3, 4, 0b000000, 0, True, (27, 31, 53)), (3, 2, 0b010100, 6, False, (19, 33, 23)),
     # the narrowest grids a pml allows (its width + R on both sides leaves one interior
     # node): the transpose's gathered rows and columns leave one row or a few columns
     (2, 4, 0b0110, 6, False, (11, 13)), (2, 3, 0b1001, 5, False, (9, 61)),
