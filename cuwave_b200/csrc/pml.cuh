@@ -13,7 +13,9 @@
 //
 //   axis 1: a block per (plane, slab row), its threads along the row; the slab row's
 //           profile is one value per block; taps are the 2R rows of four around the row
-//   axis 2: a thread per (row, slab quad); taps are the quad's run of 4 + 2H values
+//   axis 2: a thread per (row, slab quad); taps are the quad's run of 4 + 2H values;
+//           the quad's memory is loaded for all its lanes before any is written back
+//           (four blocks an SM bound its registers, so the early loads cost no warps)
 //
 // Taps past a wall take their mirrors (cuwave common.cuh:50-54). The stiffness is
 // uniform (the blocked step's domain), so the harmonic means are one constant.
@@ -163,7 +165,7 @@ __global__ void __launch_bounds__(PML1_THREADS) pml_axis1_kernel(const __grid_co
 }
 
 template <typename T, int R>
-__global__ void __launch_bounds__(PML2_THREADS) pml_axis2_kernel(const __grid_constant__ Pml3Params<T> p) {
+__global__ void __launch_bounds__(PML2_THREADS, 4) pml_axis2_kernel(const __grid_constant__ Pml3Params<T> p) {
   constexpr int H = (R + 3) / 4 * 4;  // the run's halo, whole quads
   constexpr int XR = 4 + 2 * H;
   const Geometry &g = p.g;
@@ -223,9 +225,19 @@ __global__ void __launch_bounds__(PML2_THREADS) pml_axis2_kernel(const __grid_co
       } else {
         load4(mi, p.minv + idx);
       }
-      T *aux = p.aux;
       const long long sz = p.auxrow;
-      const long long row = ((long long)z * NM + y) * (lo + hi);
+      // the quad's slab nodes are consecutive slab indices of one side: the memory of
+      // lane i at m + i, loaded for every lane before the first is written back
+      const int f = __ffs(in) - 1;
+      T *m = p.aux + ((long long)z * NM + y) * (lo + hi) + (slab_row(xq + f, NF, lo, hi) - f);
+      T m0[4], m1[4], m2[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const bool on = (in >> i) & 1;
+        m0[i] = on ? m[i] : (T)0;
+        m1[i] = on ? m[sz + i] : (T)0;
+        m2[i] = on ? m[2 * sz + i] : (T)0;
+      }
       const T *prof = p.prof;
 #pragma unroll
       for (int i = 0; i < 4; ++i) {
@@ -235,11 +247,17 @@ __global__ void __launch_bounds__(PML2_THREADS) pml_axis2_kernel(const __grid_co
         const auto tap = [&](const int j) { return xr[H + i + j]; };
         T Dpu, Dmu;
         diffs_plain<T, R>(tap, xr[H + i], p.w, Dpu, Dmu);
-        const long long si = row + slab_row(x, NF, lo, hi);
         pml_node(p.f, p.gconst, prof[x], prof[NF + x], prof[2 * NF + x], prof[3 * NF + x],
-                 prof[2 * NF + x - 1], prof[3 * NF + x - 1], Dpu, Dmu, aux[si], aux[sz + si],
-                 aux[2 * sz + si], v[i], mi[i], (held >> i) & 1);
+                 prof[2 * NF + x - 1], prof[3 * NF + x - 1], Dpu, Dmu, m0[i], m1[i], m2[i],
+                 v[i], mi[i], (held >> i) & 1);
       }
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+        if ((in >> i) & 1) {
+          m[i] = m0[i];
+          m[sz + i] = m1[i];
+          m[2 * sz + i] = m2[i];
+        }
       // the face ghosts of axis 2 in this quad, refilled from their mirrors two nodes in
       // (homogeneous_neumann/dirichlet_kernel, scalar.cu:535-555), whose values are final
       // here: the host folds a face only when no source sits on its mirror column (the
