@@ -470,9 +470,19 @@ __global__ void __launch_bounds__(S2_THREADS) pml2d_kernel(const StepParams<T> p
         const int e_hi = NF - (xq - H);
         if (e_hi <= XR - 1)
           mirror_run_hi_at<T, XR, H + 2>(xr, (dirF & 2) ? (T)-1 : (T)1, e_hi);
-        T *aux = p.aux[1];
+        // the quad's slab nodes are consecutive slab indices of one side: the memory of
+        // lane i at m + i, loaded for every lane before the first is written back
         const long long sz = p.auxrow[1];
-        const long long base = (long long)z * (lo1 + hi1);
+        const int f = __ffs(xslab) - 1;
+        T *m = p.aux[1] + (long long)z * (lo1 + hi1) + (slab_row(xq + f, NF, lo1, hi1) - f);
+        T m0[4], m1[4], m2[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          const bool on = (xslab >> i) & 1;
+          m0[i] = on ? m[i] : (T)0;
+          m1[i] = on ? m[sz + i] : (T)0;
+          m2[i] = on ? m[2 * sz + i] : (T)0;
+        }
 #pragma unroll
         for (int i = 0; i < 4; ++i) {
           if (!((xslab >> i) & 1))
@@ -481,9 +491,15 @@ __global__ void __launch_bounds__(S2_THREADS) pml2d_kernel(const StepParams<T> p
           const auto tap = [&](const int j) { return xr[H + i + j]; };
           T Dpu, Dmu;
           diffs_plain<T, R>(tap, xr[H + i], p.w, Dpu, Dmu);
-          const long long si = base + slab_row(x, NF, lo1, hi1);
-          node(i, 1, x, NF, Dpu, Dmu, aux[si], aux[sz + si], aux[2 * sz + si]);
+          node(i, 1, x, NF, Dpu, Dmu, m0[i], m1[i], m2[i]);
         }
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+          if ((xslab >> i) & 1) {
+            m[i] = m0[i];
+            m[sz + i] = m1[i];
+            m[2 * sz + i] = m2[i];
+          }
       }
       // the face ghosts whose mirrors this thread holds, refilled from them (cuwave
       // scalar.cu:535-555): the host folds a face here only when no source sits on its
