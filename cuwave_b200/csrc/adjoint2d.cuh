@@ -194,6 +194,22 @@ __global__ void __launch_bounds__(A2_THREADS, A2_MIN_BLOCKS) adjoint2d_kernel(co
       for (int z = c0; z < c1; ++z) {
         const long long row = (long long)z * s0 + xq;
         const bool zheld = held_row(z);
+        // the row's point reads first, so their latency passes under the taps' arithmetic
+        // (issued later they wait behind the row's taps, and cannot pass the row before's
+        // stores)
+        T lov[4], miv[4], gm[4], gs4[4];
+        load4(lov, l0 + row);
+        if (flags & K_DERIVE) {
+  #pragma unroll
+          for (int i = 0; i < 4; ++i)
+            miv[i] = mi_derived;
+        } else {
+          load4(miv, p.minv + row);
+        }
+        if constexpr (GR) {
+          load4(gm, p.g_mass + row);
+          load4(gs4, p.g_stiff + row);
+        }
         // the row's own lambda and u, as stored (a held wall row's own value is not the
         // zero its taps read)
         T lcz[4], ucz[4];
@@ -269,20 +285,7 @@ __global__ void __launch_bounds__(A2_THREADS, A2_MIN_BLOCKS) adjoint2d_kernel(co
             dpx[j] = d;
           }
         }
-        T ln[4], gm[4], gs4[4];
-        T lov[4], miv[4], uc[4], lc[4];
-        load4(lov, l0 + row);
-        if (flags & K_DERIVE) {
-  #pragma unroll
-          for (int i = 0; i < 4; ++i)
-            miv[i] = mi_derived;
-        } else {
-          load4(miv, p.minv + row);
-        }
-        if constexpr (GR) {
-          load4(gm, p.g_mass + row);
-          load4(gs4, p.g_stiff + row);
-        }
+        T ln[4], uc[4], lc[4];
   #pragma unroll
         for (int i = 0; i < 4; ++i) {
           lc[i] = lcz[i];
