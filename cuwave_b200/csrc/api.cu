@@ -610,8 +610,8 @@ int pml_launch(const cwb_plan *p, const cwb::StepParams<T> &sp, const int fold,
     q1.aux = sp.aux[1];
     q1.auxrow = sp.auxrow[1];
     const int quads = (g.n[2] - 2) / 4 + 1;
-    const dim3 grid((quads + cwb::PML1_THREADS - 1) / cwb::PML1_THREADS, g.lo[1] + g.hi[1],
-                    g.n[0] - 2);
+    const dim3 grid((quads + cwb::PML1_QUADS - 1) / cwb::PML1_QUADS,
+                    (g.lo[1] + g.hi[1] + cwb::PML1_ROWS - 1) / cwb::PML1_ROWS, g.n[0] - 2);
     out.push_back([q1, R, grid](cudaStream_t s, bool adv) {
       cwb::Pml3Params<T> q = q1;
       if (adv)

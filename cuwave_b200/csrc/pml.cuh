@@ -11,8 +11,8 @@
 // A thread owns four consecutive axis-2 nodes (a quad, 16-byte aligned) of one row, so
 // the field, update and memory rows move as 16-byte vectors:
 //
-//   axis 1: a block per (plane, slab row), its threads along the row; the slab row's
-//           profile is one value per block; taps are the 2R rows of four around the row
+//   axis 1: a block per (plane, 4 slab rows, 32 quads), a warp along each row; taps are
+//           the 2R rows of four around the row (the block's rows share them in L1)
 //   axis 2: a thread per (row, slab quad); taps are the quad's run of 4 + 2H values;
 //           the quad's memory is loaded for all its lanes before any is written back
 //           (four blocks an SM bound its registers, so the early loads cost no warps)
@@ -25,7 +25,8 @@
 
 namespace cwb {
 
-constexpr int PML1_THREADS = 128;  // quads of one axis-1 slab row per block
+constexpr int PML1_THREADS = 128;
+constexpr int PML1_QUADS = 32, PML1_ROWS = PML1_THREADS / PML1_QUADS;  // an axis-1 block's tile
 constexpr int PML2_THREADS = 256;
 
 template <typename T>
@@ -91,11 +92,13 @@ __global__ void __launch_bounds__(PML1_THREADS) pml_axis1_kernel(const __grid_co
   const int t = step_index(p.ctr);
   const int N0 = g.n[0], NM = g.n[1], NF = g.n[2];
   const int lo = g.lo[1], hi = g.hi[1];
-  const int r = blockIdx.y;           // the slab row
-  const int z = 1 + blockIdx.z;       // the plane
+  // a warp a slab row, PML1_ROWS consecutive slab rows a block, so their taps' rows are
+  // shared in L1
+  const int r = blockIdx.y * PML1_ROWS + threadIdx.x / PML1_QUADS;  // the slab row
+  const int z = 1 + blockIdx.z;                                      // the plane
   const int y = r < lo ? 1 + r : NM - 1 - hi + (r - lo);
-  const int xq = 4 * (blockIdx.x * PML1_THREADS + threadIdx.x);
-  if (xq <= NF - 2) {
+  const int xq = 4 * (blockIdx.x * PML1_QUADS + threadIdx.x % PML1_QUADS);
+  if (r < lo + hi && xq <= NF - 2) {
     const T *__restrict__ u1 = level<T>(p.u1, t);
     T *u2 = level<T>(p.u2, t);
     int mask = 0, xheld = 0;
