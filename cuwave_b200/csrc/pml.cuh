@@ -242,17 +242,25 @@ __global__ void __launch_bounds__(PML2_THREADS, 4) pml_axis2_kernel(const __grid
         m2[i] = on ? m[2 * sz + i] : (T)0;
       }
       const T *prof = p.prof;
+      // the half-point profile one node down is the lane before's own: loaded once for
+      // the quad's first lane (xq >= 0: the slab nodes have x >= 1)
+      T ah_prev = xq >= 1 ? prof[2 * NF + xq - 1] : (T)0;
+      T bh_prev = xq >= 1 ? prof[3 * NF + xq - 1] : (T)0;
 #pragma unroll
       for (int i = 0; i < 4; ++i) {
-        if (!((in >> i) & 1))
-          continue;
         const int x = xq + i;
-        const auto tap = [&](const int j) { return xr[H + i + j]; };
-        T Dpu, Dmu;
-        diffs_plain<T, R>(tap, xr[H + i], p.w, Dpu, Dmu);
-        pml_node(p.f, p.gconst, prof[x], prof[NF + x], prof[2 * NF + x], prof[3 * NF + x],
-                 prof[2 * NF + x - 1], prof[3 * NF + x - 1], Dpu, Dmu, m0[i], m1[i], m2[i],
-                 v[i], mi[i], (held >> i) & 1);
+        // (the quad's last lanes may lie past the row's last node, NF - 1)
+        const T ah = x <= NF - 1 ? prof[2 * NF + x] : (T)0;
+        const T bh = x <= NF - 1 ? prof[3 * NF + x] : (T)0;
+        if ((in >> i) & 1) {
+          const auto tap = [&](const int j) { return xr[H + i + j]; };
+          T Dpu, Dmu;
+          diffs_plain<T, R>(tap, xr[H + i], p.w, Dpu, Dmu);
+          pml_node(p.f, p.gconst, prof[x], prof[NF + x], ah, bh, ah_prev, bh_prev, Dpu, Dmu,
+                   m0[i], m1[i], m2[i], v[i], mi[i], (held >> i) & 1);
+        }
+        ah_prev = ah;
+        bh_prev = bh;
       }
 #pragma unroll
       for (int i = 0; i < 4; ++i)
