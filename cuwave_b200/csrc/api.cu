@@ -64,6 +64,7 @@ struct cwb_plan {
   long long march3_bytes = 8LL << 20;
   int flow3 = 1;  // the 3D blocked step without a block barrier per plane (CWB_FLOW3D=0: with; 2: deeper ring)
   int pml2d = 1;  // the 2D quad step's pml terms by a launch of their own (CWB_PML2D=0: inside the update kernel)
+  int src2d = 1;  // that launch adds the step's sources too where none is on a slab node (CWB_SRC2D=0: a launch of their own)
   cudaStream_t lane = nullptr;
   cudaEvent_t fork = nullptr, join = nullptr;
   int sms = 148;
@@ -458,17 +459,17 @@ bool step2d_built_r(const int R) {
 }
 
 template <typename T>
-cudaError_t pml2d_r(const cwb::StepParams<T> &p, const cwb::Pml2Layout &lay, const int R,
-                    cudaStream_t s) {
+cudaError_t pml2d_r(const cwb::StepParams<T> &p, const cwb::Pml2Layout &lay,
+                    const cwb::TransferParams<T> &src, const int R, cudaStream_t s) {
   switch (R) {
-  case 1: return cwb::pml2d_unit<T, 1>(p, lay, s);
-  case 2: return cwb::pml2d_unit<T, 2>(p, lay, s);
-  case 3: return cwb::pml2d_unit<T, 3>(p, lay, s);
-  case 4: return cwb::pml2d_unit<T, 4>(p, lay, s);
-  case 5: return cwb::pml2d_unit<T, 5>(p, lay, s);
-  case 6: return cwb::pml2d_unit<T, 6>(p, lay, s);
-  case 7: return cwb::pml2d_unit<T, 7>(p, lay, s);
-  case 8: return cwb::pml2d_unit<T, 8>(p, lay, s);
+  case 1: return cwb::pml2d_unit<T, 1>(p, lay, src, s);
+  case 2: return cwb::pml2d_unit<T, 2>(p, lay, src, s);
+  case 3: return cwb::pml2d_unit<T, 3>(p, lay, src, s);
+  case 4: return cwb::pml2d_unit<T, 4>(p, lay, src, s);
+  case 5: return cwb::pml2d_unit<T, 5>(p, lay, src, s);
+  case 6: return cwb::pml2d_unit<T, 6>(p, lay, src, s);
+  case 7: return cwb::pml2d_unit<T, 7>(p, lay, src, s);
+  case 8: return cwb::pml2d_unit<T, 8>(p, lay, src, s);
   }
   return cudaErrorInvalidValue;
 }
@@ -828,6 +829,7 @@ int translate(cwb_plan *p, const cwb_op &op, const size_t slot, cudaStream_t str
                        aligned16(op.c.base, op.c.stride) && (derive || aligned16(sp.minv, 0)) &&
                        g.n[0] >= 3 * R && g.n[1] >= 3 * R;
     int refilled = 0;  // face ghosts a launch before the refill has written (face bits)
+    bool sources_done = false;  // the sources added by a launch before the excitation's
     if (quad2) {
       // enough quads x row chunks to give every SM a few blocks of 128 threads
       const long long rows = g.n[0] - 2, quads = (g.n[1] - 2) / 4 + 1;
@@ -867,12 +869,46 @@ int translate(cwb_plan *p, const cwb_op &op, const size_t slot, cudaStream_t str
         if (lay.total <= 0)
           lay.fold = 0;
         refilled = lay.fold;
+        // the sources ride on the pml launch where none sits on a node it writes (a slab
+        // node; its ghost folds are interior-free): the pml's share of a node comes
+        // before its source in cuwave's step, and no slab node holds one
+        cwb::TransferParams<T> src;
+        std::memset(&src, 0, sizeof src);
+        const cwb_points &pt = op.points;
+        if (lay.total > 0 && p->src2d && (op.flags & CWB_FOLD_SOURCES) && pt.num > 0 && pt.lin &&
+            pt.weight && pt.record && pt.store >= 0 && pt.store <= 1) {
+          std::vector<int> lin(pt.num);
+          CWB_CUDA(cudaMemcpyAsync(lin.data(), pt.lin, sizeof(int) * pt.num, cudaMemcpyDeviceToHost, stream));
+          CWB_CUDA(cudaStreamSynchronize(stream));
+          const int N0 = g.n[0], lo0 = g.lo[0], hi0 = g.hi[0];
+          bool clear = true;
+          for (const int l : lin) {
+            const int z = l / g.s[0], x = l % g.s[0];
+            const bool interior = z >= 1 && z <= N0 - 2 && x >= 1 && x <= NF - 2;
+            const bool slab = (lo0 && z <= lo0) || (hi0 && z >= N0 - 1 - hi0) || (lo1 && x <= lo1) ||
+                              (hi1 && x >= NF - 1 - hi1);
+            clear = clear && interior && !slab;
+          }
+          if (clear) {
+            src.g = g;
+            src.a = to_level(op.c, bytes);
+            src.lin = pt.lin;
+            src.weight = static_cast<const T *>(pt.weight);
+            src.record = pt.record;
+            src.num = pt.num;
+            src.row_mul = pt.row_mul;
+            src.row_add = pt.row_add;
+            src.store = pt.store;
+            src.ctr = p->ctr;
+            sources_done = true;
+          }
+        }
         if (lay.total > 0)
-          out.push_back([sp, lay, R](cudaStream_t s, bool adv) {
+          out.push_back([sp, lay, src, R](cudaStream_t s, bool adv) {
             cwb::StepParams<T> q = sp;
             if (adv)
               q.flags |= cwb::K_ADV;
-            return pml2d_r<T>(q, lay, R, s);
+            return pml2d_r<T>(q, lay, src, R, s);
           });
       }
     }
@@ -905,7 +941,7 @@ int translate(cwb_plan *p, const cwb_op &op, const size_t slot, cudaStream_t str
           refilled = fold << 4;
         }
       }
-      if ((op.flags & CWB_FOLD_SOURCES) && op.points.num > 0) {
+      if ((op.flags & CWB_FOLD_SOURCES) && op.points.num > 0 && !sources_done) {
         if (!op.points.weight || !op.points.record)
           return fail(CWB_ERR_ARG, "folded sources need weights and a signal");
         cwb_op ex;
@@ -1931,6 +1967,8 @@ int plan_geometry(const cwb_grid &G, cwb_plan &p) {
     p.march3 = std::atoi(env);
   if (const char *env = std::getenv("CWB_PML2D"))
     p.pml2d = std::atoi(env);
+  if (const char *env = std::getenv("CWB_SRC2D"))
+    p.src2d = std::atoi(env) != 0;
   if (const char *env = std::getenv("CWB_FLOW3D"))
     p.flow3 = std::atoi(env);
   if (const char *env = std::getenv("CWB_TBLOCK"))

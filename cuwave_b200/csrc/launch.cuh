@@ -47,7 +47,8 @@ bool step2d_built();
 // the pml terms of the 2D quad step when the update kernel leaves them out
 struct Pml2Layout;
 template <typename T, int R>
-cudaError_t pml2d_unit(const StepParams<T> &p, const Pml2Layout &lay, cudaStream_t stream);
+cudaError_t pml2d_unit(const StepParams<T> &p, const Pml2Layout &lay, const TransferParams<T> &src,
+                       cudaStream_t stream);
 
 // the 2D quad adjoint of a uniform stiffness (float, radius <= 4), MODE_STEP or
 // MODE_STEP_GRAD, 128 threads a block

@@ -343,8 +343,11 @@ struct Pml2Layout {
   int fold;          // face ghosts refilled here (1 row 0, 2 row N0-1, 4 column 0, 8 column NF-1)
 };
 
+// `src`: the step's sources when none sits on a node this launch writes (its num 0
+// otherwise): threads past the slab quads add them, as excite_kernel would after it
 template <typename T, int R, bool HOLD>
-__global__ void __launch_bounds__(S2_THREADS) pml2d_kernel(const StepParams<T> p, const Pml2Layout lay) {
+__global__ void __launch_bounds__(S2_THREADS) pml2d_kernel(const StepParams<T> p, const Pml2Layout lay,
+                                                           const TransferParams<T> src) {
   using S = Step2Shape<T, R>;
   constexpr int H = S::H, XR = S::XR;
   const long long k = (long long)blockIdx.x * S2_THREADS + threadIdx.x;
@@ -535,6 +538,13 @@ __global__ void __launch_bounds__(S2_THREADS) pml2d_kernel(const StepParams<T> p
             ghost[i] = sg * v[i];
       }
     }
+  } else if (k < lay.total + src.num) {
+    // a source (excite_kernel's add): its node is no slab node, so no thread above
+    // writes it, and no face this launch refills mirrors it
+    const int j = (int)(k - lay.total);
+    T *a = level<T>(src.a, t);
+    const long long srow = (long long)src.row_mul * t + src.row_add;
+    atomic_add_exact(&a[src.lin[j]], src.weight[j] * record_read(src, srow * src.num + j));
   }
   finish_step(p.ctr, p.flags & K_ADV);
 }

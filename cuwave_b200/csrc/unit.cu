@@ -150,15 +150,16 @@ cudaError_t step2d_unit(const StepParams<T> &p, const bool uniform, const dim3 g
 }
 
 template <typename T, int R>
-cudaError_t pml2d_unit(const StepParams<T> &p, const Pml2Layout &lay, cudaStream_t s) {
+cudaError_t pml2d_unit(const StepParams<T> &p, const Pml2Layout &lay, const TransferParams<T> &src,
+                       cudaStream_t s) {
   if constexpr (!Step2Shape<T, R>::SUPPORTED) {
     return cudaErrorInvalidValue;
   } else {
-    const dim3 grid((unsigned)((lay.total + S2_THREADS - 1) / S2_THREADS));
+    const dim3 grid((unsigned)((lay.total + src.num + S2_THREADS - 1) / S2_THREADS));
     if (p.g.dir)
-      pml2d_kernel<T, R, true><<<grid, S2_THREADS, 0, s>>>(p, lay);
+      pml2d_kernel<T, R, true><<<grid, S2_THREADS, 0, s>>>(p, lay, src);
     else
-      pml2d_kernel<T, R, false><<<grid, S2_THREADS, 0, s>>>(p, lay);
+      pml2d_kernel<T, R, false><<<grid, S2_THREADS, 0, s>>>(p, lay, src);
     return cudaGetLastError();
   }
 }
@@ -350,7 +351,7 @@ template cudaError_t step2d_unit<CWB_REAL, CWB_RADIUS>(const StepParams<CWB_REAL
                                                        cudaStream_t);
 template bool step2d_built<CWB_REAL, CWB_RADIUS>();
 template cudaError_t pml2d_unit<CWB_REAL, CWB_RADIUS>(const StepParams<CWB_REAL> &, const Pml2Layout &,
-                                                      cudaStream_t);
+                                                      const TransferParams<CWB_REAL> &, cudaStream_t);
 template cudaError_t batch2d_unit<CWB_REAL, CWB_RADIUS>(const Batch2Params<CWB_REAL> &, dim3,
                                                         cudaStream_t);
 template cudaError_t march2d_unit<CWB_REAL, CWB_RADIUS>(const March2Params<CWB_REAL> &, int,

@@ -233,6 +233,30 @@ def test_quad_2d_pml_step_ghosts_folded_or_not(dirichlet, on_mirrors):
     np.testing.assert_array_equal(traces, ref_traces)
 
 
+@pytest.mark.parametrize("inside,dirichlet", [(False, 0b0000), (False, 0b1001), (True, 0b0000)])
+def test_quad_2d_pml_launch_adds_the_sources(inside, dirichlet):
+    """The 2D quad step's pml launch adds the step's sources itself when none sits on a
+    slab node (two of them on one node here), and leaves them to a launch of their own
+    when one does: both equal to the oracle."""
+    pml = 6
+    case, meta = _random_case(2, 4, dirichlet=dirichlet, pml=pml, uniform=True, seed=63, nsrc=4,
+                              nsens=9, Nx=(611, 1090))
+    meta["N"] = 12
+    case.signal = case.signal[:12]
+    Nx = meta["Nx"]
+    src = np.array([[pml + 3, Nx[0] // 2, Nx[0] // 2, Nx[0] - pml - 4],
+                    [Nx[1] // 3, Nx[1] // 2, Nx[1] // 2, Nx[1] - pml - 4]], np.int32)
+    if inside:
+        src[:, 3] = (Nx[0] // 3, pml)  # a node of the axis-1 slab
+    meta["src"] = src
+    case.source_lin = cases.flat({"Nx": np.array(Nx)}, src)
+    case.source_weight = case.excitation_weights(case.source_lin)
+    field, traces = _product(case, meta)
+    ref_field, ref_traces = case.forward(meta["N"])
+    np.testing.assert_array_equal(field, ref_field)
+    np.testing.assert_array_equal(traces, ref_traces)
+
+
 @pytest.mark.parametrize("dirichlet", [0b000000, 0b110000])
 def test_blocked_step_with_sources_on_the_ghost_mirrors(dirichlet):
     """Sources on the columns whose values the fast axis' face ghosts copy (x = 2 and
