@@ -383,9 +383,13 @@ constexpr int A2P_THREADS = 256;
 // (pml_adjoint_kernel and pml_tap, scalar_sensitivity.cu:545-597, 237-251; the order of
 // adjoint_gradient_kernel's update and then pml_adjoint_kernel's, as cuwave launches
 // them).
+// `ld`: the adjoint load that follows the step, when none of its nodes is reached (its
+// num 0 otherwise): threads past the reached nodes apply it, as load_kernel would after
 template <typename T, int R, int MODE>
 __global__ void __launch_bounds__(A2P_THREADS) adjoint2d_pml_kernel(const AdjointParams<T> p,
-                                                                    const Adj2Reach reach) {
+                                                                    const Adj2Reach reach,
+                                                                    const TransferParams<T> ld,
+                                                                    T *ld_mass) {
   constexpr bool GR = MODE == MODE_STEP_GRAD;
   const Geometry &g = p.g;
   const int t = step_index(p.ctr);
@@ -469,6 +473,17 @@ __global__ void __launch_bounds__(A2P_THREADS) adjoint2d_pml_kernel(const Adjoin
     l0[row] = ln;
     if constexpr (GR)
       p.g_mass[row] = gm;
+  } else if (k >= nA + nB && k < nA + nB + ld.num) {
+    // a receiver's load (load_kernel's adds): no reached node, so no thread above
+    // writes its lambda or g_mass
+    const int j = (int)(k - nA - nB);
+    T *a = level<T>(ld.a, t);
+    const long long srow = (long long)ld.row_mul * t + ld.row_add;
+    const int n = ld.lin[j];
+    const T load = ld.weight[j] * record_read(ld, srow * ld.num + j);
+    atomic_add_exact(&a[n], load);
+    if (ld.flags & K_MASS)
+      atomic_add_exact(&ld_mass[n], -ld.scale * level<T>(ld.c, t)[n] * load);
   }
   finish_step(p.ctr, p.flags & K_ADV);
 }

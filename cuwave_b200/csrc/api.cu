@@ -65,6 +65,7 @@ struct cwb_plan {
   int flow3 = 1;  // the 3D blocked step without a block barrier per plane (CWB_FLOW3D=0: with; 2: deeper ring)
   int pml2d = 1;  // the 2D quad step's pml terms by a launch of their own (CWB_PML2D=0: inside the update kernel)
   int src2d = 1;  // that launch adds the step's sources too where none is on a slab node (CWB_SRC2D=0: a launch of their own)
+  int load2d = 1;  // the 2D adjoint's gather applies the load that follows where none of its nodes is reached (CWB_LOAD2D=0: its own launch)
   cudaStream_t lane = nullptr;
   cudaEvent_t fork = nullptr, join = nullptr;
   int sms = 148;
@@ -492,12 +493,13 @@ cudaError_t step2d_r(const cwb::StepParams<T> &p, const int R, const bool u, con
 
 template <typename T>
 cudaError_t adjoint2d_pml_r(const cwb::AdjointParams<T> &p, const cwb::Adj2Reach &reach,
-                            const int R, const int mode, const dim3 grid, cudaStream_t s) {
+                            const int R, const int mode, const cwb::TransferParams<T> &ld,
+                            T *ld_mass, const dim3 grid, cudaStream_t s) {
   switch (R) {
-  case 1: return cwb::adjoint2d_pml_unit<T, 1>(p, reach, mode, grid, s);
-  case 2: return cwb::adjoint2d_pml_unit<T, 2>(p, reach, mode, grid, s);
-  case 3: return cwb::adjoint2d_pml_unit<T, 3>(p, reach, mode, grid, s);
-  case 4: return cwb::adjoint2d_pml_unit<T, 4>(p, reach, mode, grid, s);
+  case 1: return cwb::adjoint2d_pml_unit<T, 1>(p, reach, mode, ld, ld_mass, grid, s);
+  case 2: return cwb::adjoint2d_pml_unit<T, 2>(p, reach, mode, ld, ld_mass, grid, s);
+  case 3: return cwb::adjoint2d_pml_unit<T, 3>(p, reach, mode, ld, ld_mass, grid, s);
+  case 4: return cwb::adjoint2d_pml_unit<T, 4>(p, reach, mode, ld, ld_mass, grid, s);
   }
   return cudaErrorInvalidValue;
 }
@@ -764,7 +766,7 @@ int x_ghost_fold(const cwb_plan *p, const cwb_op &op, cudaStream_t stream, int &
 // the launches of one op, each taking (stream, advance)
 template <typename T>
 int translate(cwb_plan *p, const cwb_op &op, const size_t slot, cudaStream_t stream,
-              std::vector<Launch> &out) {
+              std::vector<Launch> &out, const cwb_op *next = nullptr, bool *took_next = nullptr) {
   const Geometry &g = p->geo;
   const int ndim = g.ndim, R = p->grid.radius;
   const int bytes = sizeof(T);
@@ -1119,12 +1121,54 @@ int translate(cwb_plan *p, const cwb_op &op, const size_t slot, cudaStream_t str
         const long long nodes =
             (long long)(reach.za_lo + N0 - 1 - reach.za_hi) * (NF - 2) +
             (long long)(reach.za_hi - 1 - reach.za_lo) * (reach.xb_lo + NF - 1 - reach.xb_hi);
-        const dim3 pgrid((unsigned)std::max<long long>(1, (nodes + cwb::A2P_THREADS - 1) / cwb::A2P_THREADS));
-        out.push_back([ap, reach, R, mode, pgrid](cudaStream_t s, bool adv) {
+        // the adjoint load that follows this op rides on the gather where none of its nodes
+        // is reached: the gather adds nothing to them, so the load applied beside it is
+        // the load applied after it
+        cwb::TransferParams<T> ld;
+        std::memset(&ld, 0, sizeof ld);
+        T *ld_mass = nullptr;
+        if (next && took_next && p->load2d && next->kind == CWB_OP_LOAD && next->points.num > 0 &&
+            next->points.lin && next->points.weight && next->points.record &&
+            next->points.store >= 0 && next->points.store <= 1 && !check_level(next->a, "a") &&
+            (!next->g_mass || !check_level(next->c, "c"))) {
+          const cwb_points &pt = next->points;
+          std::vector<int> lin(pt.num);
+          CWB_CUDA(cudaMemcpyAsync(lin.data(), pt.lin, sizeof(int) * pt.num, cudaMemcpyDeviceToHost, stream));
+          CWB_CUDA(cudaStreamSynchronize(stream));
+          bool clear = true;
+          for (const int l : lin) {
+            const int z = l / g.s[0], x = l % g.s[0];
+            const bool interior = z >= 1 && z <= N0 - 2 && x >= 1 && x <= NF - 2;
+            const bool reached = z <= reach.za_lo || z >= reach.za_hi || x <= reach.xb_lo || x >= reach.xb_hi;
+            clear = clear && interior && !reached;
+          }
+          if (clear) {
+            ld.g = g;
+            ld.a = to_level(next->a, bytes);
+            ld.lin = pt.lin;
+            ld.weight = static_cast<const T *>(pt.weight);
+            ld.record = pt.record;
+            ld.num = pt.num;
+            ld.row_mul = pt.row_mul;
+            ld.row_add = pt.row_add;
+            ld.store = pt.store;
+            ld.ctr = p->ctr;
+            if (next->g_mass) {
+              ld.flags |= cwb::K_MASS;
+              ld.c = to_level(next->c, bytes);
+              ld.scale = (T)next->scale;
+              ld_mass = static_cast<T *>(next->g_mass);
+            }
+            *took_next = true;
+          }
+        }
+        const long long threads = nodes + ld.num;
+        const dim3 pgrid((unsigned)std::max<long long>(1, (threads + cwb::A2P_THREADS - 1) / cwb::A2P_THREADS));
+        out.push_back([ap, reach, R, mode, ld, ld_mass, pgrid](cudaStream_t s, bool adv) {
           cwb::AdjointParams<T> q = ap;
           if (adv)
             q.flags |= cwb::K_ADV;
-          return adjoint2d_pml_r<T>(q, reach, R, mode, pgrid, s);
+          return adjoint2d_pml_r<T>(q, reach, R, mode, ld, ld_mass, pgrid, s);
         });
       }
       return CWB_OK;
@@ -1853,9 +1897,14 @@ int march(cwb_plan *p, const cwb_op *ops, const int nops, const int t0, const in
   }
   std::vector<Launch> launches;
   for (int i = 0; i < nops; ++i) {
-    const int rc = translate<T>(p, ops[i], (size_t)i, user, launches);
+    // an op may take the one after it into its own launches (the 2D adjoint its load)
+    bool took = false;
+    const int rc = translate<T>(p, ops[i], (size_t)i, user, launches, i + 1 < nops ? &ops[i + 1] : nullptr,
+                                &took);
     if (rc)
       return rc;
+    if (took)
+      ++i;
   }
   if (launches.empty() || steps <= 0)
     return CWB_OK;
@@ -1969,6 +2018,8 @@ int plan_geometry(const cwb_grid &G, cwb_plan &p) {
     p.pml2d = std::atoi(env);
   if (const char *env = std::getenv("CWB_SRC2D"))
     p.src2d = std::atoi(env) != 0;
+  if (const char *env = std::getenv("CWB_LOAD2D"))
+    p.load2d = std::atoi(env) != 0;
   if (const char *env = std::getenv("CWB_FLOW3D"))
     p.flow3 = std::atoi(env);
   if (const char *env = std::getenv("CWB_TBLOCK"))

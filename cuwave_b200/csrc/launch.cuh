@@ -58,7 +58,8 @@ struct Adj2Reach;
 // its pml transpose, a launch after it over the nodes within R of a slab
 template <typename T, int R>
 cudaError_t adjoint2d_pml_unit(const AdjointParams<T> &p, const Adj2Reach &reach, int mode,
-                               dim3 grid, cudaStream_t stream);
+                               const TransferParams<T> &ld, T *ld_mass, dim3 grid,
+                               cudaStream_t stream);
 
 template <typename T>
 struct March3Params;

@@ -252,14 +252,15 @@ cudaError_t adjoint2d_unit(const AdjointParams<T> &p, const int mode, const dim3
 
 template <typename T, int R>
 cudaError_t adjoint2d_pml_unit(const AdjointParams<T> &p, const Adj2Reach &reach, const int mode,
-                               const dim3 grid, cudaStream_t s) {
+                               const TransferParams<T> &ld, T *ld_mass, const dim3 grid,
+                               cudaStream_t s) {
   if constexpr (!Adj2Shape<T, R>::SUPPORTED) {
     return cudaErrorInvalidValue;
   } else {
     if (mode == MODE_STEP_GRAD)
-      adjoint2d_pml_kernel<T, R, MODE_STEP_GRAD><<<grid, A2P_THREADS, 0, s>>>(p, reach);
+      adjoint2d_pml_kernel<T, R, MODE_STEP_GRAD><<<grid, A2P_THREADS, 0, s>>>(p, reach, ld, ld_mass);
     else if (mode == MODE_STEP)
-      adjoint2d_pml_kernel<T, R, MODE_STEP><<<grid, A2P_THREADS, 0, s>>>(p, reach);
+      adjoint2d_pml_kernel<T, R, MODE_STEP><<<grid, A2P_THREADS, 0, s>>>(p, reach, ld, ld_mass);
     else
       return cudaErrorInvalidValue;
     return cudaGetLastError();
@@ -361,8 +362,9 @@ template cudaError_t tblock2d_unit<CWB_REAL, CWB_RADIUS>(const TBlock2Params<flo
 template cudaError_t adjoint2d_unit<CWB_REAL, CWB_RADIUS>(const AdjointParams<CWB_REAL> &, int,
                                                           dim3, cudaStream_t);
 template cudaError_t adjoint2d_pml_unit<CWB_REAL, CWB_RADIUS>(const AdjointParams<CWB_REAL> &,
-                                                              const Adj2Reach &, int, dim3,
-                                                              cudaStream_t);
+                                                              const Adj2Reach &, int,
+                                                              const TransferParams<CWB_REAL> &,
+                                                              CWB_REAL *, dim3, cudaStream_t);
 #endif
 #if CWB_NDIM == 3
 template cudaError_t step3d_unit<CWB_REAL, CWB_RADIUS>(const Step3Params<CWB_REAL> &, bool, dim3,

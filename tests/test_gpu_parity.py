@@ -353,6 +353,44 @@ def test_uniform_sensitivity_matches_oracle(ndim, R, dirichlet, pml, damping, Nx
         np.testing.assert_array_equal(grads[key].cpu().numpy(), ref[key])
 
 
+@pytest.mark.parametrize("inside", [False, True])
+def test_quad_adjoint_gather_applies_the_load(inside):
+    """The 2D quad adjoint's pml gather applies the adjoint load that follows it when no
+    receiver sits on a node the gather reaches (two receivers on one node here), and
+    leaves it to a launch of its own when one does: the gradients and traces equal the
+    oracle's to the bit either way."""
+    from cuwave_b200 import AcousticWave, Neumann, Pml, Source
+    from cuwave_b200.sensitivity import l2_misfit, sensitivity
+
+    R, pml = 4, 5
+    case, meta = _random_case(2, R, pml=pml, uniform=True, seed=71, nsrc=2, nsens=6, Nx=(75, 139))
+    Nx = meta["Nx"]
+    reach = pml + R
+    sens = np.array([[reach + 2, Nx[0] // 2, Nx[0] // 2, Nx[0] - reach - 3, 30, 40],
+                     [reach + 2, Nx[1] // 2, Nx[1] // 2, Nx[1] - reach - 3, 60, 90]], np.int32)
+    if inside:
+        sens[:, 5] = (Nx[0] // 2, reach - 1)  # within R of the axis-1 slab
+    meta["sens"] = sens
+    case.sensor_lin = cases.flat({"Nx": np.array(Nx)}, sens)
+    rng = np.random.default_rng(9)
+    observed = rng.standard_normal((meta["N"], sens.shape[1])).astype(case.dtype) * 1e-3
+    _, ref, ref_traces = case.sensitivity(meta["N"], o.l2(observed))
+    sim = AcousticWave(Nx=Nx, dx=(1.0, 1.0), N=meta["N"], dt=meta["dt"], precision="float32",
+                       space_order=2 * R, boundary=((Neumann, Neumann), (Neumann, Neumann)),
+                       pml=Pml(width=pml, wavespeed=1.6), rho1=1.0, rho2=1.0, kappa1=1.0,
+                       kappa2=2.0)
+    dev = torch.device("cuda")
+    t = lambda a: torch.as_tensor(a, device=dev)  # noqa: E731
+    mat = {"stiff": t(case.stiff), "minv": t(case.minv), "damping": None,
+           "profiles": [t(p) for p in case.profiles] + [None],
+           "uniform": True, "stiff_value": float(case.stiff.flat[0])}
+    source = Source(meta["src"], case.signal)
+    _, grads, traces, _ = sensitivity(sim, source, None, sens, l2_misfit(t(observed)), _mat=mat)
+    np.testing.assert_array_equal(traces.cpu().numpy(), ref_traces)
+    for key in ("mass", "stiff"):
+        np.testing.assert_array_equal(grads[key].cpu().numpy(), ref[key])
+
+
 @pytest.mark.parametrize("name", cases.GRADIENT)
 def test_reconstruction_matches_reference(name):
     """The strip-replay adjoint with two checkpoints against the reference's own run."""
