@@ -65,6 +65,7 @@ struct cwb_plan {
   int flow3 = 1;  // the 3D blocked step without a block barrier per plane (CWB_FLOW3D=0: with; 2: deeper ring)
   int pml2d = 1;  // the 2D quad step's pml terms by a launch of their own (CWB_PML2D=0: inside the update kernel)
   int src2d = 1;  // that launch adds the step's sources too where none is on a slab node (CWB_SRC2D=0: a launch of their own)
+  int rec2d = 1;  // that launch also reads the record op that follows where its nodes are final (CWB_REC2D=0: its own launch)
   int load2d = 1;  // the 2D adjoint's gather applies the load that follows where none of its nodes is reached (CWB_LOAD2D=0: its own launch)
   cudaStream_t lane = nullptr;
   cudaEvent_t fork = nullptr, join = nullptr;
@@ -461,16 +462,17 @@ bool step2d_built_r(const int R) {
 
 template <typename T>
 cudaError_t pml2d_r(const cwb::StepParams<T> &p, const cwb::Pml2Layout &lay,
-                    const cwb::TransferParams<T> &src, const int R, cudaStream_t s) {
+                    const cwb::TransferParams<T> &src, const cwb::TransferParams<T> &rec, const int R,
+                    cudaStream_t s) {
   switch (R) {
-  case 1: return cwb::pml2d_unit<T, 1>(p, lay, src, s);
-  case 2: return cwb::pml2d_unit<T, 2>(p, lay, src, s);
-  case 3: return cwb::pml2d_unit<T, 3>(p, lay, src, s);
-  case 4: return cwb::pml2d_unit<T, 4>(p, lay, src, s);
-  case 5: return cwb::pml2d_unit<T, 5>(p, lay, src, s);
-  case 6: return cwb::pml2d_unit<T, 6>(p, lay, src, s);
-  case 7: return cwb::pml2d_unit<T, 7>(p, lay, src, s);
-  case 8: return cwb::pml2d_unit<T, 8>(p, lay, src, s);
+  case 1: return cwb::pml2d_unit<T, 1>(p, lay, src, rec, s);
+  case 2: return cwb::pml2d_unit<T, 2>(p, lay, src, rec, s);
+  case 3: return cwb::pml2d_unit<T, 3>(p, lay, src, rec, s);
+  case 4: return cwb::pml2d_unit<T, 4>(p, lay, src, rec, s);
+  case 5: return cwb::pml2d_unit<T, 5>(p, lay, src, rec, s);
+  case 6: return cwb::pml2d_unit<T, 6>(p, lay, src, rec, s);
+  case 7: return cwb::pml2d_unit<T, 7>(p, lay, src, rec, s);
+  case 8: return cwb::pml2d_unit<T, 8>(p, lay, src, rec, s);
   }
   return cudaErrorInvalidValue;
 }
@@ -905,12 +907,51 @@ int translate(cwb_plan *p, const cwb_op &op, const size_t slot, cudaStream_t str
             sources_done = true;
           }
         }
+        // the record op that follows rides on the launch too where its nodes are final
+        // after the update: interior, no slab node (the pml's), no source's node
+        cwb::TransferParams<T> rec;
+        std::memset(&rec, 0, sizeof rec);
+        if (lay.total > 0 && p->rec2d && next && took_next && next->kind == CWB_OP_RECORD &&
+            next->points.num > 0 && next->points.num <= 65536 && next->points.lin && next->points.record &&
+            next->points.store >= 0 && next->points.store <= 2 &&
+            !(next->points.store == 2 && sizeof(T) == 4) && !check_level(next->a, "a")) {
+          const cwb_points &rp = next->points;
+          std::vector<int> rlin(rp.num), slin;
+          CWB_CUDA(cudaMemcpyAsync(rlin.data(), rp.lin, sizeof(int) * rp.num, cudaMemcpyDeviceToHost, stream));
+          if ((op.flags & CWB_FOLD_SOURCES) && pt.num > 0 && pt.lin) {
+            slin.resize(pt.num);
+            CWB_CUDA(cudaMemcpyAsync(slin.data(), pt.lin, sizeof(int) * pt.num, cudaMemcpyDeviceToHost, stream));
+          }
+          CWB_CUDA(cudaStreamSynchronize(stream));
+          std::sort(slin.begin(), slin.end());
+          const int N0 = g.n[0], lo0 = g.lo[0], hi0 = g.hi[0];
+          bool clear = true;
+          for (const int l : rlin) {
+            const int z = l / g.s[0], x = l % g.s[0];
+            const bool interior = z >= 1 && z <= N0 - 2 && x >= 1 && x <= NF - 2;
+            const bool slab = (lo0 && z <= lo0) || (hi0 && z >= N0 - 1 - hi0) || (lo1 && x <= lo1) ||
+                              (hi1 && x >= NF - 1 - hi1);
+            clear = clear && interior && !slab && !std::binary_search(slin.begin(), slin.end(), l);
+          }
+          if (clear) {
+            rec.g = g;
+            rec.a = to_level(next->a, bytes);
+            rec.lin = rp.lin;
+            rec.record = rp.record;
+            rec.num = rp.num;
+            rec.row_mul = rp.row_mul;
+            rec.row_add = rp.row_add;
+            rec.store = rp.store;
+            rec.ctr = p->ctr;
+            *took_next = true;
+          }
+        }
         if (lay.total > 0)
-          out.push_back([sp, lay, src, R](cudaStream_t s, bool adv) {
+          out.push_back([sp, lay, src, rec, R](cudaStream_t s, bool adv) {
             cwb::StepParams<T> q = sp;
             if (adv)
               q.flags |= cwb::K_ADV;
-            return pml2d_r<T>(q, lay, src, R, s);
+            return pml2d_r<T>(q, lay, src, rec, R, s);
           });
       }
     }
@@ -1128,6 +1169,7 @@ int translate(cwb_plan *p, const cwb_op &op, const size_t slot, cudaStream_t str
         std::memset(&ld, 0, sizeof ld);
         T *ld_mass = nullptr;
         if (next && took_next && p->load2d && next->kind == CWB_OP_LOAD && next->points.num > 0 &&
+            next->points.num <= 65536 &&
             next->points.lin && next->points.weight && next->points.record &&
             next->points.store >= 0 && next->points.store <= 1 && !check_level(next->a, "a") &&
             (!next->g_mass || !check_level(next->c, "c"))) {
@@ -2020,6 +2062,8 @@ int plan_geometry(const cwb_grid &G, cwb_plan &p) {
     p.src2d = std::atoi(env) != 0;
   if (const char *env = std::getenv("CWB_LOAD2D"))
     p.load2d = std::atoi(env) != 0;
+  if (const char *env = std::getenv("CWB_REC2D"))
+    p.rec2d = std::atoi(env) != 0;
   if (const char *env = std::getenv("CWB_FLOW3D"))
     p.flow3 = std::atoi(env);
   if (const char *env = std::getenv("CWB_TBLOCK"))

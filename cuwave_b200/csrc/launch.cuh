@@ -48,7 +48,7 @@ bool step2d_built();
 struct Pml2Layout;
 template <typename T, int R>
 cudaError_t pml2d_unit(const StepParams<T> &p, const Pml2Layout &lay, const TransferParams<T> &src,
-                       cudaStream_t stream);
+                       const TransferParams<T> &rec, cudaStream_t stream);
 
 // the 2D quad adjoint of a uniform stiffness (float, radius <= 4), MODE_STEP or
 // MODE_STEP_GRAD, 128 threads a block

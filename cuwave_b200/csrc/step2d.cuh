@@ -344,10 +344,13 @@ struct Pml2Layout {
 };
 
 // `src`: the step's sources when none sits on a node this launch writes (its num 0
-// otherwise): threads past the slab quads add them, as excite_kernel would after it
+// otherwise): threads past the slab quads add them, as excite_kernel would after it.
+// `rec`: the record op that follows the step, when its nodes are final before this launch
+// (interior, no slab node, no source): threads past those read them, as record_kernel would
 template <typename T, int R, bool HOLD>
 __global__ void __launch_bounds__(S2_THREADS) pml2d_kernel(const StepParams<T> p, const Pml2Layout lay,
-                                                           const TransferParams<T> src) {
+                                                           const TransferParams<T> src,
+                                                           const TransferParams<T> rec) {
   using S = Step2Shape<T, R>;
   constexpr int H = S::H, XR = S::XR;
   const long long k = (long long)blockIdx.x * S2_THREADS + threadIdx.x;
@@ -545,6 +548,13 @@ __global__ void __launch_bounds__(S2_THREADS) pml2d_kernel(const StepParams<T> p
     T *a = level<T>(src.a, t);
     const long long srow = (long long)src.row_mul * t + src.row_add;
     atomic_add_exact(&a[src.lin[j]], src.weight[j] * record_read(src, srow * src.num + j));
+  } else if (k < lay.total + src.num + rec.num) {
+    // a receiver (record_kernel's read) of a node no launch of the step writes after the
+    // update
+    const int j = (int)(k - lay.total - src.num);
+    const T *a = level<T>(rec.a, t);
+    const long long rrow = (long long)rec.row_mul * t + rec.row_add;
+    record_write(rec, rrow * rec.num + j, a[rec.lin[j]]);
   }
   finish_step(p.ctr, p.flags & K_ADV);
 }

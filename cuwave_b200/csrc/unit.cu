@@ -151,15 +151,15 @@ cudaError_t step2d_unit(const StepParams<T> &p, const bool uniform, const dim3 g
 
 template <typename T, int R>
 cudaError_t pml2d_unit(const StepParams<T> &p, const Pml2Layout &lay, const TransferParams<T> &src,
-                       cudaStream_t s) {
+                       const TransferParams<T> &rec, cudaStream_t s) {
   if constexpr (!Step2Shape<T, R>::SUPPORTED) {
     return cudaErrorInvalidValue;
   } else {
-    const dim3 grid((unsigned)((lay.total + src.num + S2_THREADS - 1) / S2_THREADS));
+    const dim3 grid((unsigned)((lay.total + src.num + rec.num + S2_THREADS - 1) / S2_THREADS));
     if (p.g.dir)
-      pml2d_kernel<T, R, true><<<grid, S2_THREADS, 0, s>>>(p, lay, src);
+      pml2d_kernel<T, R, true><<<grid, S2_THREADS, 0, s>>>(p, lay, src, rec);
     else
-      pml2d_kernel<T, R, false><<<grid, S2_THREADS, 0, s>>>(p, lay, src);
+      pml2d_kernel<T, R, false><<<grid, S2_THREADS, 0, s>>>(p, lay, src, rec);
     return cudaGetLastError();
   }
 }
@@ -352,6 +352,7 @@ template cudaError_t step2d_unit<CWB_REAL, CWB_RADIUS>(const StepParams<CWB_REAL
                                                        cudaStream_t);
 template bool step2d_built<CWB_REAL, CWB_RADIUS>();
 template cudaError_t pml2d_unit<CWB_REAL, CWB_RADIUS>(const StepParams<CWB_REAL> &, const Pml2Layout &,
+                                                      const TransferParams<CWB_REAL> &,
                                                       const TransferParams<CWB_REAL> &, cudaStream_t);
 template cudaError_t batch2d_unit<CWB_REAL, CWB_RADIUS>(const Batch2Params<CWB_REAL> &, dim3,
                                                         cudaStream_t);

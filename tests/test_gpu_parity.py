@@ -233,11 +233,16 @@ def test_quad_2d_pml_step_ghosts_folded_or_not(dirichlet, on_mirrors):
     np.testing.assert_array_equal(traces, ref_traces)
 
 
-@pytest.mark.parametrize("inside,dirichlet", [(False, 0b0000), (False, 0b1001), (True, 0b0000)])
-def test_quad_2d_pml_launch_adds_the_sources(inside, dirichlet):
+@pytest.mark.parametrize("inside,dirichlet,receivers", [
+    (False, 0b0000, "clear"), (False, 0b1001, "clear"), (True, 0b0000, "clear"),
+    (False, 0b0000, "on a source"), (False, 0b0000, "in a slab"),
+])
+def test_quad_2d_pml_launch_adds_the_sources(inside, dirichlet, receivers):
     """The 2D quad step's pml launch adds the step's sources itself when none sits on a
     slab node (two of them on one node here), and leaves them to a launch of their own
-    when one does: both equal to the oracle."""
+    when one does; it reads the receivers that follow when they are final after the update
+    (clear of the slabs and the sources), and leaves them to the record launch when one
+    sits on a source or a slab node: all equal to the oracle."""
     pml = 6
     case, meta = _random_case(2, 4, dirichlet=dirichlet, pml=pml, uniform=True, seed=63, nsrc=4,
                               nsens=9, Nx=(611, 1090))
@@ -251,6 +256,13 @@ def test_quad_2d_pml_launch_adds_the_sources(inside, dirichlet):
     meta["src"] = src
     case.source_lin = cases.flat({"Nx": np.array(Nx)}, src)
     case.source_weight = case.excitation_weights(case.source_lin)
+    sens = np.stack([np.full(9, Nx[0] // 4), np.linspace(pml + 2, Nx[1] - pml - 3, 9).astype(int)]).astype(np.int32)
+    if receivers == "on a source":
+        sens[:, 4] = src[:, 1]
+    elif receivers == "in a slab":
+        sens[:, 4] = (pml - 1, Nx[1] // 2)
+    meta["sens"] = sens
+    case.sensor_lin = cases.flat({"Nx": np.array(Nx)}, sens)
     field, traces = _product(case, meta)
     ref_field, ref_traces = case.forward(meta["N"])
     np.testing.assert_array_equal(field, ref_field)
