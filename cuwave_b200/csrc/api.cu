@@ -69,6 +69,10 @@ struct cwb_plan {
   int load2d = 1;  // the 2D adjoint's gather applies the load that follows where none of its nodes is reached (CWB_LOAD2D=0: its own launch)
   cudaStream_t lane = nullptr;
   cudaEvent_t fork = nullptr, join = nullptr;
+  // the adjoint's pml memory beside its march (CWB_AUXPAR=0: before it), on this stream
+  int aux_par = 1;
+  cudaStream_t side = nullptr;
+  cudaEvent_t side_fork = nullptr, side_join = nullptr;
   int sms = 148;
   int chunk_override = 0;
   std::vector<Scratch> scratch;
@@ -1939,6 +1943,44 @@ int march(cwb_plan *p, const cwb_op *ops, const int nops, const int t0, const in
   }
   std::vector<Launch> launches;
   for (int i = 0; i < nops; ++i) {
+    // the adjoint's pml memory [PML_AUX, ADJOINT with its gather apart]: the memory launch
+    // reads lambda^(n+1) and writes only the memory, which the march neither reads nor
+    // writes; it runs beside the march on the side stream and the gather, which reads the
+    // memory, waits for it
+    if (p->aux_par && p->side && ops[i].kind == CWB_OP_PML_AUX && i + 1 < nops &&
+        ops[i + 1].kind == CWB_OP_ADJOINT) {
+      std::vector<Launch> aux, adj;
+      bool took = false;
+      int rc = translate<T>(p, ops[i], (size_t)i, user, aux);
+      if (!rc)
+        rc = translate<T>(p, ops[i + 1], (size_t)(i + 1), user, adj, i + 2 < nops ? &ops[i + 2] : nullptr,
+                          &took);
+      if (rc)
+        return rc;
+      if (aux.size() == 1 && adj.size() == 2) {
+        const Launch mem = aux[0], gather = adj[1];
+        cudaStream_t side = p->side;
+        cudaEvent_t sf = p->side_fork, sj = p->side_join;
+        launches.push_back([mem, side, sf](cudaStream_t s, bool) {
+          cudaError_t e = cudaEventRecord(sf, s);
+          if (e == cudaSuccess)
+            e = cudaStreamWaitEvent(side, sf, 0);
+          return e == cudaSuccess ? mem(side, false) : e;  // never a step's last launch
+        });
+        launches.push_back(adj[0]);
+        launches.push_back([gather, side, sj](cudaStream_t s, bool adv) {
+          cudaError_t e = cudaEventRecord(sj, side);
+          if (e == cudaSuccess)
+            e = cudaStreamWaitEvent(s, sj, 0);
+          return e == cudaSuccess ? gather(s, adv) : e;
+        });
+      } else {
+        launches.insert(launches.end(), aux.begin(), aux.end());
+        launches.insert(launches.end(), adj.begin(), adj.end());
+      }
+      i += took ? 2 : 1;
+      continue;
+    }
     // an op may take the one after it into its own launches (the 2D adjoint its load)
     bool took = false;
     const int rc = translate<T>(p, ops[i], (size_t)i, user, launches, i + 1 < nops ? &ops[i + 1] : nullptr,
@@ -2066,6 +2108,8 @@ int plan_geometry(const cwb_grid &G, cwb_plan &p) {
     p.rec2d = std::atoi(env) != 0;
   if (const char *env = std::getenv("CWB_FLOW3D"))
     p.flow3 = std::atoi(env);
+  if (const char *env = std::getenv("CWB_AUXPAR"))
+    p.aux_par = std::atoi(env) != 0;
   if (const char *env = std::getenv("CWB_TBLOCK"))
     p.tblock = std::atoi(env);
   if (const char *env = std::getenv("CWB_ADJSPLIT"))
@@ -2566,7 +2610,10 @@ int cwb_plan_create(const cwb_grid *grid, cwb_plan **out) {
       cudaMalloc(&p->err, sizeof(int)) != cudaSuccess ||
       cudaStreamCreateWithFlags(&p->lane, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreateWithFlags(&p->fork, cudaEventDisableTiming) != cudaSuccess ||
-      cudaEventCreateWithFlags(&p->join, cudaEventDisableTiming) != cudaSuccess) {
+      cudaEventCreateWithFlags(&p->join, cudaEventDisableTiming) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&p->side, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&p->side_fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&p->side_join, cudaEventDisableTiming) != cudaSuccess) {
     cwb_plan_destroy(p);
     return fail(CWB_ERR_ALLOC, std::string("plan resources: ") +
                                    cudaGetErrorString(cudaGetLastError()));
@@ -2602,6 +2649,14 @@ int cwb_plan_destroy(cwb_plan *p) {
     cudaEventDestroy(p->fork);
   if (p->join)
     cudaEventDestroy(p->join);
+  if (p->side) {
+    cudaStreamSynchronize(p->side);
+    cudaStreamDestroy(p->side);
+  }
+  if (p->side_fork)
+    cudaEventDestroy(p->side_fork);
+  if (p->side_join)
+    cudaEventDestroy(p->side_join);
   if (p->lane)
     cudaStreamDestroy(p->lane);
   delete p;
