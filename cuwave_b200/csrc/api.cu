@@ -65,6 +65,7 @@ struct cwb_plan {
   int flow3 = 1;  // the 3D blocked step without a block barrier per plane (CWB_FLOW3D=0: with; 2: deeper ring)
   int pml2d = 1;  // the 2D quad step's pml terms by a launch of their own (CWB_PML2D=0: inside the update kernel)
   int src2d = 1;  // that launch adds the step's sources too where none is on a slab node (CWB_SRC2D=0: a launch of their own)
+  int fold3d = 1;  // the 3D refill launch adds the sources and reads the next record op where they touch no refilled node (CWB_FOLD3D=0: their own launches)
   int rec2d = 1;  // that launch also reads the record op that follows where its nodes are final (CWB_REC2D=0: its own launch)
   int load2d = 1;  // the 2D adjoint's gather applies the load that follows where none of its nodes is reached (CWB_LOAD2D=0: its own launch)
   cudaStream_t lane = nullptr;
@@ -988,6 +989,95 @@ int translate(cwb_plan *p, const cwb_op &op, const size_t slot, cudaStream_t str
           refilled = fold << 4;
         }
       }
+      // 3D: the refill launch adds the sources and reads the record op that follows where
+      // neither touches a node the refill reads or writes (a refilled face's mirror, a ghost,
+      // a held wall node) and no receiver sits on a source
+      cwb::TransferParams<T> src3, rec3;
+      std::memset(&src3, 0, sizeof src3);
+      std::memset(&rec3, 0, sizeof rec3);
+      const int faces3 = (p->grid.neumann | p->grid.dirichlet) & ~refilled;
+      if (blocked && p->fold3d && (op.flags & CWB_FOLD_REFILL)) {
+        const auto place = [&](const int l, int A[3]) {
+          A[0] = l / g.s[0];
+          A[1] = (l % g.s[0]) / g.s[1];
+          A[2] = l % g.s[1];
+        };
+        // along axis d: whether index a is a refilled face's mirror, a ghost or a held wall
+        const auto touched = [&](const int d, const int a, const bool reads) {
+          const int N = g.n[d];
+          bool hit = a <= 0 || a >= N - 1;
+          for (int side = 0; side < 2; ++side) {
+            if (!((faces3 >> (2 * d + side)) & 1))
+              continue;
+            if (reads && a == (side ? N - 3 : 2))
+              hit = true;
+            if (((p->grid.dirichlet >> (2 * d + side)) & 1) && a == (side ? N - 2 : 1))
+              hit = true;
+          }
+          return hit;
+        };
+        const cwb_points &sp3 = op.points;
+        std::vector<int> slin;
+        if ((op.flags & CWB_FOLD_SOURCES) && sp3.num > 0 && sp3.num <= 65536 && sp3.lin && sp3.weight &&
+            sp3.record && sp3.store >= 0 && sp3.store <= 1) {
+          slin.resize(sp3.num);
+          CWB_CUDA(cudaMemcpyAsync(slin.data(), sp3.lin, sizeof(int) * sp3.num, cudaMemcpyDeviceToHost, stream));
+          CWB_CUDA(cudaStreamSynchronize(stream));
+          bool clear = true;
+          for (const int l : slin) {
+            int A[3];
+            place(l, A);
+            for (int d = 0; d < 3; ++d)
+              clear = clear && !touched(d, A[d], true);
+          }
+          if (clear) {
+            src3.g = g;
+            src3.a = to_level(op.c, bytes);
+            src3.lin = sp3.lin;
+            src3.weight = static_cast<const T *>(sp3.weight);
+            src3.record = sp3.record;
+            src3.num = sp3.num;
+            src3.row_mul = sp3.row_mul;
+            src3.row_add = sp3.row_add;
+            src3.store = sp3.store;
+            src3.ctr = p->ctr;
+            sources_done = true;
+          }
+        }
+        if (next && took_next && next->kind == CWB_OP_RECORD && next->points.num > 0 &&
+            next->points.num <= 65536 && next->points.lin && next->points.record &&
+            next->points.store >= 0 && next->points.store <= 2 &&
+            !(next->points.store == 2 && sizeof(T) == 4) && !check_level(next->a, "a")) {
+          const cwb_points &rp = next->points;
+          std::vector<int> rlin(rp.num);
+          CWB_CUDA(cudaMemcpyAsync(rlin.data(), rp.lin, sizeof(int) * rp.num, cudaMemcpyDeviceToHost, stream));
+          CWB_CUDA(cudaStreamSynchronize(stream));
+          std::vector<int> sorted;
+          if (src3.num)
+            sorted = slin;
+          std::sort(sorted.begin(), sorted.end());
+          bool clear = true;
+          for (const int l : rlin) {
+            int A[3];
+            place(l, A);
+            for (int d = 0; d < 3; ++d)
+              clear = clear && !touched(d, A[d], false);
+            clear = clear && !std::binary_search(sorted.begin(), sorted.end(), l);
+          }
+          if (clear) {
+            rec3.g = g;
+            rec3.a = to_level(next->a, bytes);
+            rec3.lin = rp.lin;
+            rec3.record = rp.record;
+            rec3.num = rp.num;
+            rec3.row_mul = rp.row_mul;
+            rec3.row_add = rp.row_add;
+            rec3.store = rp.store;
+            rec3.ctr = p->ctr;
+            *took_next = true;
+          }
+        }
+      }
       if ((op.flags & CWB_FOLD_SOURCES) && op.points.num > 0 && !sources_done) {
         if (!op.points.weight || !op.points.record)
           return fail(CWB_ERR_ARG, "folded sources need weights and a signal");
@@ -999,7 +1089,20 @@ int translate(cwb_plan *p, const cwb_op &op, const size_t slot, cudaStream_t str
         if ((rc = translate<T>(p, ex, slot, stream, out)))
           return rc;
       }
-      if (op.flags & CWB_FOLD_REFILL) {
+      if (src3.num || rec3.num) {
+        cwb::TransferParams<T> tp;
+        std::memset(&tp, 0, sizeof tp);
+        tp.g = g;
+        tp.a = to_level(op.c, bytes);
+        tp.ctr = p->ctr;
+        out.push_back([tp, faces3, src3, rec3](cudaStream_t s, bool adv) {
+          cwb::TransferParams<T> q = tp;
+          if (adv)
+            q.flags |= cwb::K_ADV;
+          return cwb::launch_refill3d<T>(q, faces3, src3.num ? &src3 : nullptr,
+                                         rec3.num ? &rec3 : nullptr, s);
+        });
+      } else if (op.flags & CWB_FOLD_REFILL) {
         cwb_op rf;
         std::memset(&rf, 0, sizeof rf);
         rf.kind = CWB_OP_REFILL;
@@ -2106,6 +2209,8 @@ int plan_geometry(const cwb_grid &G, cwb_plan &p) {
     p.load2d = std::atoi(env) != 0;
   if (const char *env = std::getenv("CWB_REC2D"))
     p.rec2d = std::atoi(env) != 0;
+  if (const char *env = std::getenv("CWB_FOLD3D"))
+    p.fold3d = std::atoi(env) != 0;
   if (const char *env = std::getenv("CWB_FLOW3D"))
     p.flow3 = std::atoi(env);
   if (const char *env = std::getenv("CWB_AUXPAR"))

@@ -100,6 +100,12 @@ cudaError_t adjoint3d_pml_unit(const AdjointParams<T> &p, const Adj3Reach &reach
 template <typename T>
 cudaError_t launch_transfer(int kind, const TransferParams<T> &p, T *g_mass, int faces,
                             int threads_total, cudaStream_t stream);
+
+// the 3D ghost refill, with the step's sources and the following record folded in where
+// they touch no node the refill reads or writes (null: none)
+template <typename T>
+cudaError_t launch_refill3d(const TransferParams<T> &p, int faces, const TransferParams<T> *src,
+                            const TransferParams<T> *rec, cudaStream_t stream);
 template <typename T>
 cudaError_t launch_pml_aux(const PmlAuxSet<T> &set, cudaStream_t stream);
 template <typename T>

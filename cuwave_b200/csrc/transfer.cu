@@ -1,4 +1,6 @@
 // The transfer, refill and adjoint pml memory kernels of both precisions.
+#include <cstring>
+
 #include "launch.cuh"
 #include "transfer.cuh"
 #include "batch.cuh"
@@ -6,7 +8,8 @@
 namespace cwb {
 
 template <typename T>
-cudaError_t launch_refill3d(const TransferParams<T> &p, int faces, cudaStream_t stream);
+cudaError_t launch_refill3d(const TransferParams<T> &p, int faces, const TransferParams<T> *src,
+                            const TransferParams<T> *rec, cudaStream_t stream);
 
 template <typename T>
 cudaError_t launch_transfer(const int kind, const TransferParams<T> &p, T *g_mass,
@@ -21,7 +24,7 @@ cudaError_t launch_transfer(const int kind, const TransferParams<T> &p, T *g_mas
   case TR_REPLAY: replay_kernel<T><<<blocks, TRANSFER_THREADS, 0, stream>>>(p); break;
   case TR_REFILL:
     if (p.g.ndim == 3)
-      return launch_refill3d<T>(p, faces, stream);
+      return launch_refill3d<T>(p, faces, nullptr, nullptr, stream);
     refill_kernel<T><<<blocks, TRANSFER_THREADS, 0, stream>>>(p, faces);
     break;
   case TR_DFT: dft_kernel<T><<<blocks, TRANSFER_THREADS, 0, stream>>>(p, g_mass); break;
@@ -31,7 +34,8 @@ cudaError_t launch_transfer(const int kind, const TransferParams<T> &p, T *g_mas
 }
 
 template <typename T>
-cudaError_t launch_refill3d(const TransferParams<T> &p, const int faces, cudaStream_t stream) {
+cudaError_t launch_refill3d(const TransferParams<T> &p, const int faces, const TransferParams<T> *src,
+                            const TransferParams<T> *rec, cudaStream_t stream) {
   const Geometry &g = p.g;
   Refill3Layout lay;
   lay.faces = faces;
@@ -40,10 +44,14 @@ cudaError_t launch_refill3d(const TransferParams<T> &p, const int faces, cudaStr
   lay.n1 = (faces & 12) ? 2LL * (g.n[0] - 2) * lay.nq : 0;
   const long long n2 = (faces & 48) ? (long long)(g.n[0] - 2) * (g.n[1] - 2) : 0;
   lay.total = lay.n0 + lay.n1 + n2;
-  if (lay.total <= 0)
+  TransferParams<T> none;
+  std::memset(&none, 0, sizeof none);
+  const TransferParams<T> &sp = src ? *src : none, &rp = rec ? *rec : none;
+  const long long threads = lay.total + sp.num + rp.num;
+  if (threads <= 0)
     return cudaSuccess;
-  const long long blocks = (lay.total + TRANSFER_THREADS - 1) / TRANSFER_THREADS;
-  refill3d_kernel<T><<<(unsigned)blocks, TRANSFER_THREADS, 0, stream>>>(p, lay);
+  const long long blocks = (threads + TRANSFER_THREADS - 1) / TRANSFER_THREADS;
+  refill3d_kernel<T><<<(unsigned)blocks, TRANSFER_THREADS, 0, stream>>>(p, lay, sp, rp);
   return cudaGetLastError();
 }
 
@@ -89,6 +97,12 @@ template cudaError_t launch_transfer<float>(int, const TransferParams<float> &, 
                                             int, cudaStream_t);
 template cudaError_t launch_transfer<double>(int, const TransferParams<double> &, double *,
                                              int, int, cudaStream_t);
+template cudaError_t launch_refill3d<float>(const TransferParams<float> &, int,
+                                            const TransferParams<float> *,
+                                            const TransferParams<float> *, cudaStream_t);
+template cudaError_t launch_refill3d<double>(const TransferParams<double> &, int,
+                                             const TransferParams<double> *,
+                                             const TransferParams<double> *, cudaStream_t);
 template cudaError_t launch_frechet<float>(const FrechetParams<float> &, cudaStream_t);
 template cudaError_t launch_frechet<double>(const FrechetParams<double> &, cudaStream_t);
 template cudaError_t launch_batch_record<float>(const BatchRecordParams<float> &, cudaStream_t);

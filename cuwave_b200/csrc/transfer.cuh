@@ -146,12 +146,30 @@ struct Refill3Layout {
   long long total;
 };
 
+// `src`, `rec`: the step's sources and the record op that follows, when neither touches a
+// node another thread of the launch reads or writes (no source on a refilled face's
+// mirror, no receiver on a ghost, a held wall node or a source): threads past the faces'
+// add the sources as excite_kernel would before the refill and read the receivers as
+// record_kernel would after it (num 0 where they run as launches of their own)
 template <typename T>
-__global__ void refill3d_kernel(const TransferParams<T> p, const Refill3Layout lay) {
+__global__ void refill3d_kernel(const TransferParams<T> p, const Refill3Layout lay,
+                                const TransferParams<T> src, const TransferParams<T> rec) {
   const int t = step_index(p.ctr);
   const Geometry &g = p.g;
   long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (k < lay.total) {
+  if (k >= lay.total) {
+    k -= lay.total;
+    if (k < src.num) {
+      T *a = level<T>(src.a, t);
+      const long long srow = (long long)src.row_mul * t + src.row_add;
+      atomic_add_exact(&a[src.lin[k]], src.weight[k] * record_read(src, srow * src.num + k));
+    } else if (k - src.num < rec.num) {
+      const int j = (int)(k - src.num);
+      const T *a = level<T>(rec.a, t);
+      const long long rrow = (long long)rec.row_mul * t + rec.row_add;
+      record_write(rec, rrow * rec.num + j, a[rec.lin[j]]);
+    }
+  } else {
     T *u = level<T>(p.a, t);
     const int N0 = g.n[0], NM = g.n[1], NF = g.n[2];
     const long long s0 = g.s[0], s1 = g.s[1];
