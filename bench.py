@@ -886,8 +886,10 @@ def step_kernel_name() -> str:
     if os.environ.get("CWB_STEP3D", "1") != "0" and os.environ.get("CWB_NO_TMA", "0") == "0":
         step = ("step3d_flow_kernel<float,4>" if os.environ.get("CWB_FLOW3D", "1") != "0"
                 else "step3d_kernel<float,4,uniform>")
+        tail = ("refill3d_kernel (refill, sources, receivers)" if os.environ.get("CWB_FOLD3D", "1") != "0"
+                else "excite_kernel + refill3d_kernel + record_kernel")
         return (f"one march step: {step} (fd + axis-0 pml) + "
-                "pml_axis1_kernel + pml_axis2_kernel (axes 1-2) + excite_kernel + refill_kernel")
+                f"pml_axis1_kernel + pml_axis2_kernel (axes 1-2) + {tail}")
     return "step_tma_kernel<float,3,4,uniform> (row step: fd + pml + sources + refill)"
 
 
