@@ -3,7 +3,7 @@
 Fixture cases come from the reference itself (tests/golden); the larger cases are
 seeded and checked against the oracle. The kernels keep the reference's order of
 operations and are built without fused multiply-adds the source does not ask for, so
-the bar is equality; the north-star tolerance (1e-5 relative L2) is checked as well so
+the bar is equality; a 1e-5 relative L2 tolerance is checked as well so
 a failure says how far off it is.
 """
 
