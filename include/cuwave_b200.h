@@ -10,7 +10,8 @@
  * C-contiguous over the padded grid (nx[0], .., ceil32(nx[ndim-1])); a flat node index
  * is sum_d i_d * stride_d over that grid, int32. Every call returns CWB_OK (0) or a
  * negative CWB_ERR_* code, and cwb_last_error() then holds one line of text. Nothing is
- * allocated outside a plan: a plan owns its scratch (counters, source lists, graphs).
+ * allocated outside a plan: a plan owns its scratch (counters, source lists, graphs)
+ * and its two streams (the march's, and a side stream the adjoint's pml memory runs on).
  * The one entry point that runs without a plan, cwb_march_static, allocates nothing at
  * all: its scratch is a fixed static device array.
  *
